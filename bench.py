@@ -1,0 +1,354 @@
+"""Benchmark: SIMPLEC outer iterations of an Euler nozzle on B200.
+
+Workload (one step = one outer iteration `it` of src/mach2d_main.f90:94-445):
+the C01 cosine nozzle (Lc = 2, Ld = 4, throat r = 1 m) at 512 x 256 real
+volumes (514 x 258 with the ghost ring), Euler, constant properties
+(gamma = 1.4, R = 287), p0 = 1e6 Pa, T0 = 1000 K, MSI for u, v and p'
+(nitm_u = 5, nitm_p = 20, tol 1e-2), itpmax = 20, SCARBOROUGH time stepper,
+FP64.  Metric: cell-updates/s = real cells x outer iterations / time.
+
+Each rank runs its own nozzle instance (replicas: a single grid does not
+shard, see the MSI factorisation); value = total cell-updates of all ranks /
+max-over-ranks time.  The per-iteration working set (~140 MB of fields,
+coefficients and solver factors) exceeds the 126 MB L2, so no explicit L2
+flush is inserted between iterations.
+
+--impl reference times the CPU restatement of the reference (the reference
+itself is Fortran and no Fortran compiler exists on this image) on the
+host, serially like the reference build, on a bounded sample of the same
+workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NXR, NYR = 512, 256
+HBM_FALLBACK_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nxr", type=int, default=NXR)
+    ap.add_argument("--nyr", type=int, default=NYR)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+def make_case(nxr, nyr):
+    from mach2d_b200.simplec import euler_cosine_case
+    return euler_cosine_case(nxr, nyr)
+
+
+def workload_config(args, extra=None):
+    cfg = {"workload": f"simplec-outer-iteration euler c01-cosine-nozzle {args.nxr}x{args.nyr}",
+           "real_cells": args.nxr * args.nyr, "grid_with_ghosts": [args.nxr + 2, args.nyr + 2],
+           "solver": "MSI (nitm_u=5, nitm_p=20, tol 1e-2), itpmax=20, SCARBOROUGH dt",
+           "precision": "fp64", "parallelism": "replicas (one instance per rank)",
+           "l2": "working set per iteration ~140 MB > 126 MB L2; no flush"}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self._stop = threading.Event()
+        self._proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self._proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "100",
+                 "-i", str(self.gpu)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except Exception:
+            self._proc = None
+        return self
+
+    def _read(self):
+        for line in self._proc.stdout:
+            self.rows.append([s.strip() for s in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self._proc:
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=5)
+            except Exception:
+                self._proc.kill()
+
+    def summary(self):
+        sm = []
+        mx = None
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[0]))
+                mx = float(r[1])
+                for k, nm in enumerate(names):
+                    if r[4 + k].lower().startswith("active"):
+                        reasons.add(nm)
+            except Exception:
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- reference arm
+def cpu_sample(args, seconds):
+    """Times the CPU restatement of the reference (serial, like the shipped
+    reference build) on the first outer iterations of the same workload."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from _oracle import OracleCase
+    o = OracleCase(make_case(args.nxr, args.nyr))
+    t0 = time.perf_counter()
+    n = 0
+    while True:
+        rc, _ = o.iterate()
+        n += 1
+        if rc or time.perf_counter() - t0 > seconds:
+            break
+    dt = time.perf_counter() - t0
+    return args.nxr * args.nyr * n / dt, n, dt
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    total_s = 0.0
+    total_n = 0
+    for _ in range(max(1, args.warmup)):
+        pass
+    per_step = max(5.0, min(20.0, 120.0 / max(1, args.steps)))
+    vals = []
+    for _ in range(args.steps):
+        v, n, dt = cpu_sample(args, per_step / 5.0)
+        vals.append(v)
+        total_s += dt
+        total_n += n
+    value = args.nxr * args.nyr * total_n / total_s
+    line = {
+        "impl": "reference", "metric": "cell-updates/s (SIMPLEC outer iterations)", "value": value,
+        "unit": "cell-updates/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total_s / total_n, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded nozzle geometry, isentropic initial guess)",
+        "config": workload_config(args),
+        "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": 1, "kind": "port",
+                         "sample": f"{total_n} outer iterations from the initial guess, serial C restatement "
+                                   "(reference is Fortran, no compiler on the image)"},
+        "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- our arm
+def msi_algorithmic_bytes(nd, N, nit):
+    """FP64 compulsory traffic of one MSI solve launch: factorisation (A in,
+    dl + du out), initial residual (A, x, b in; r out), and per iteration the
+    forward sweep (r, dl in; w out), the backward sweep (w, du, x in; x out)
+    and the residual (A, x, b in; r out)."""
+    nl, nu = (5, 4) if nd == 9 else (4, 3)
+    lu = nd + nl + nu
+    res = nd + 3
+    it = (1 + nl + 1) + (1 + nu + 2) + res
+    return 8 * N * (lu + res + nit * it)
+
+
+def run_ours(args):
+    import ctypes
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from mach2d_b200._lib import check, lib
+    from mach2d_b200.simplec import Simplec
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    sim = Simplec(make_case(args.nxr, args.nyr), device=local)
+    L = lib()
+    stream_ptr = ctypes.c_void_p()
+    L.m2d_ctx_stream.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
+    check(L.m2d_ctx_stream(sim._ctx, ctypes.byref(stream_ptr)))
+    st = torch.cuda.ExternalStream(stream_ptr.value, device=local)
+
+    for _ in range(args.warmup):
+        sim.iterate()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = sim.scalar("launches")
+    itp = []
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(st)
+        for _ in range(args.steps):
+            r = sim.iterate()
+            itp.append(r.itp_used)
+        e1.record(st)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    launches = int(sim.scalar("launches") - l0)
+    if world > 1:
+        t = torch.tensor([ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    cells = args.nxr * args.nyr
+    value = cells * args.steps * world / (ms / 1e3)
+
+    # ---- end to end through the public API with host buffers: every step
+    # uploads the state a host driver owns from pinned memory, iterates, and
+    # reads the state back
+    state = ("u", "v", "p", "T", "ro", "ue", "ve", "un", "vn", "Uce", "Vcn", "roe", "ron")
+    pinned = {}
+    for f in state:
+        t = torch.empty(sim.nx * sim.ny, dtype=torch.float64, pin_memory=True)
+        a = t.numpy()
+        a[:] = sim.field(f)
+        pinned[f] = (t, a)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for f in state:
+            sim.set_field(f, pinned[f][1])
+        sim.iterate()
+        for f in state:
+            src = sim.field(f)
+            pinned[f][1][:] = src
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = cells * args.steps * world / e2e_s
+    nbytes = len(state) * sim.nx * sim.ny * 8
+
+    # ---- roofline of the dominant kernel: the MSI5 p' solve, re-run on the
+    # instance's last p' system with CUDA events on the launching stream
+    N = sim.nx * sim.ny
+    dptr = ctypes.POINTER(ctypes.c_double)()
+    n = ctypes.c_long()
+    L.m2d_ctx_field_device.argtypes = [ctypes.c_void_p, ctypes.c_char_p,
+                                       ctypes.POINTER(ctypes.POINTER(ctypes.c_double)), ctypes.POINTER(ctypes.c_long)]
+    check(L.m2d_ctx_field_device(sim._ctx, b"ap", ctypes.byref(dptr), ctypes.byref(n)))
+    d_ap = ctypes.cast(dptr, ctypes.c_void_p).value
+    check(L.m2d_ctx_field_device(sim._ctx, b"bp", ctypes.byref(dptr), ctypes.byref(n)))
+    d_bp = ctypes.cast(dptr, ctypes.c_void_p).value
+    L.m2d_msi_workspace_doubles.restype = ctypes.c_long
+    wsz = L.m2d_msi_workspace_doubles(5, sim.nx, sim.ny)
+    work = torch.empty(wsz, dtype=torch.float64, device=f"cuda:{local}")
+    xk = torch.zeros(N, dtype=torch.float64, device=f"cuda:{local}")
+    nit_d = torch.zeros(1, dtype=torch.int32, device=f"cuda:{local}")
+    L.m2d_msi_solve_device.argtypes = [ctypes.c_int] * 4 + [ctypes.c_double] + [ctypes.c_void_p] * 6
+    ks = torch.cuda.Stream(device=f"cuda:{local}")
+    reps = 20
+    durs = []
+    with torch.cuda.stream(ks):
+        for k in range(reps + 3):
+            xk.zero_()
+            a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a0.record(ks)
+            check(L.m2d_msi_solve_device(5, sim.nx, sim.ny, 20, 1e-2, d_ap, d_bp, xk.data_ptr(),
+                                         work.data_ptr(), ks.cuda_stream, nit_d.data_ptr()))
+            a1.record(ks)
+            if k >= 3:
+                durs.append((a0, a1))
+    torch.cuda.synchronize()
+    avg_ms = sum(a.elapsed_time(b) for a, b in durs) / len(durs)
+    nit = int(nit_d.item())
+    alg = msi_algorithmic_bytes(5, N, nit)
+    achieved = alg / (avg_ms / 1e3) / 1e9
+    peak, peak_kind = peaks()
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "msi5_traffic.json")
+    if os.path.exists(prof):
+        try:
+            traffic = json.load(open(prof)).get("bytes_per_launch")
+        except Exception:
+            traffic = None
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, nsamp, secs = cpu_sample(args, args.cpu_seconds)
+        cpu = {"value": v, "unit": "cell-updates/s", "cores": 1, "kind": "port",
+               "sample": f"{nsamp} outer iterations ({secs:.1f} s) of the same 512x256 case from the initial "
+                         "guess, serial C restatement of the reference"}
+
+    if rank == 0:
+        line = {
+            "metric": "cell-updates/s (SIMPLEC outer iterations)", "value": value, "unit": "cell-updates/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded nozzle geometry, isentropic initial guess)",
+            "config": workload_config(args, {"p_cycles_per_iteration": sum(itp) / len(itp)}),
+            "e2e": {"value": e2e, "unit": "cell-updates/s", "h2d_bytes_per_step": nbytes,
+                    "d2h_bytes_per_step": nbytes},
+            "gpu_launches": launches,
+            "roofline": {"kernel": "k_msi<5> (MSI5 factorisation + fb2d5 iterations, one CTA)",
+                         "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_kind,
+                         "traffic": traffic, "algorithmic_bytes_per_launch": alg,
+                         "launch_ms": avg_ms, "iterations_per_launch": nit},
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

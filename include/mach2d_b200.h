@@ -1,0 +1,283 @@
+/*
+ * mach2d_b200.h -- C ABI of the B200 (sm_100a) implementation of MACH-2D's
+ * SIMPLEC outer iteration.
+ *
+ * Two layers:
+ *
+ *  1. Drop-ins for the reference's routines.  Each entry point takes the
+ *     reference routine's argument list in the reference's order, with HOST
+ *     pointers and every argument by reference, exactly what a Fortran
+ *     `bind(C)` interface passes.  Arrays use the
+ *     reference layout: nx, ny count the ghost ring, cell (i,j) 1-based sits
+ *     at offset nx*(j-1)+i-1, a coefficient matrix a(nx*ny,k) is stored
+ *     diagonal after diagonal (9-diagonal order SW,S,SE,W,P,E,NW,N,NE;
+ *     5-diagonal order S,W,P,E,N).  Each call copies its inputs to the GPU,
+ *     runs the kernel and copies its outputs back; it is meant for swapping
+ *     one routine at a time.
+ *
+ *  2. A device-resident context (m2d_ctx) that holds every field of one
+ *     nozzle instance in HBM and runs whole outer iterations; host copies are
+ *     made only on request.  This is the fast path.
+ *
+ * Every function returns 0 on success or an M2D_ERR_* code; m2d_last_error()
+ * describes the last failure of the calling thread.  Nothing in the library
+ * calls exit() or stop.  Errors of the solver kernels (non-finite pivots, an
+ * unbounded MSI iteration that reached its cap) are reported through the
+ * status code, never by trapping the GPU.
+ */
+#ifndef MACH2D_B200_H
+#define MACH2D_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define M2D_OK 0
+#define M2D_ERR_CUDA 1         /* a CUDA call failed (m2d_last_error has it) */
+#define M2D_ERR_ARG 2          /* invalid argument (sizes, null pointer, ...) */
+#define M2D_ERR_NAN 3          /* NaN in the iteration norm (src/mach2d_main.f90:424-436) */
+#define M2D_ERR_TIMEOUT 4      /* bounded iteration / wait reached its limit */
+#define M2D_ERR_NOMEM 5        /* device allocation failed */
+#define M2D_ERR_TOO_LARGE 6    /* grid larger than the kernel supports */
+#define M2D_ERR_PIVOT 7        /* zero or non-finite pivot in the MSI factorisation */
+
+const char *m2d_last_error(void);
+int m2d_version(void);
+
+/* ===================== 1. drop-ins for reference routines ================ */
+
+/* ---- linear solvers ------------------------------------------------------
+ * m2d_msi9_solve / m2d_msi5_solve replace class_solver_msi9d%solve and
+ * class_solver_msi5d%solve (src/solvers/mod_solver_msi.f90:79-93,119-133):
+ * incomplete LU (lu2d9 src/solvers/msi2d9-v03.f90:277-432, lu2d5
+ * src/solvers/msi2d5-v03.f90:247-330) recomputed on every call, then the
+ * fb2d9 / fb2d5 iteration (msi2d9-v03.f90:42-262, msi2d5-v03.f90:42-233) to
+ * |r| < tol |r0| or nitm iterations (nitm <= 0: until converged, capped at
+ * 10000 iterations with M2D_ERR_TIMEOUT).  x is the initial guess on entry.
+ * Precondition of the reference (msi2d9-v03.f90:16-17): no coefficient couples
+ * a cell to a neighbour outside the nx x ny grid.  ny <= m2d_msi_max_ny(). */
+int m2d_msi9_solve(const int *nx, const int *ny, const int *nitm, const double *tol,
+                   const double *a, const double *b, double *x);
+int m2d_msi5_solve(const int *nx, const int *ny, const int *nitm, const double *tol,
+                   const double *a, const double *b, double *x);
+int m2d_msi_max_ny(void);
+/* same, also returning the iterations performed */
+int m2d_msi9_solve_it(const int *nx, const int *ny, const int *nitm, const double *tol,
+                      const double *a, const double *b, double *x, int *nit);
+int m2d_msi5_solve_it(const int *nx, const int *ny, const int *nitm, const double *tol,
+                      const double *a, const double *b, double *x, int *nit);
+
+/* Device-resident variant of the same solve for callers whose arrays already
+ * live in GPU memory (CUDA Fortran / OpenACC data, or another library):
+ * nd = 9 or 5; d_a, d_b, d_x device pointers in the layout above; d_work a
+ * caller-allocated device buffer of m2d_msi_workspace_doubles(nd,nx,ny)
+ * doubles; `stream` a cudaStream_t (NULL: the default stream).  The call is
+ * asynchronous: the iteration count is written to the device int *d_nit
+ * (may be NULL) when the solve completes on `stream`. */
+long m2d_msi_workspace_doubles(int nd, int nx, int ny);
+int m2d_msi_solve_device(int nd, int nx, int ny, int nitm, double tol, const double *d_a,
+                         const double *d_b, double *d_x, double *d_work, void *stream,
+                         int *d_nit);
+
+/* class_solver_tdma9d%solve / class_solver_tdma5d%solve
+ * (src/solvers/mod_solver_tdma.f90:63-100): tdma2d9 src/solvers/tdma2d9.f90:38-322,
+ * tdma2d5 src/solvers/tdma2d5.f90:38-241 */
+int m2d_tdma9_solve(const int *nx, const int *ny, const int *nitm, const double *a,
+                    const double *b, double *x);
+int m2d_tdma5_solve(const int *nx, const int *ny, const int *nitm, const double *a,
+                    const double *b, double *x);
+
+/* A batch of independent tridiagonal lines (the x-line kernel of tdma2d9,
+ * src/solvers/tdma2d9.f90:80-192, on caller-supplied lines): line l element
+ * i at offset l*n + i; aw, ap, ae the W, P, E coefficients, d the rhs. */
+int m2d_tdma_lines(const int *n, const int *nlines, const double *aw, const double *ap,
+                   const double *ae, const double *d, double *x);
+
+/* norms: src/solvers/mod_solvers.f90:91-277.  `norm` is in/out (the routines
+ * add to it); the sums run in a fixed tree order on the GPU. */
+int m2d_norm_l1_5d(const int *nx, const int *ny, const double *var, const double *b,
+                   const double *a, double *norm);
+int m2d_norm_l1_9d(const int *nx, const int *ny, const double *var, const double *b,
+                   const double *a, double *norm);
+int m2d_norm_l1_9d_relative(const int *nx, const int *ny, const double *var,
+                            const double *b, const double *a, double *norm);
+
+/* ---- coefficient assembly and corrections: src/equations/mach2d_coef.f90 */
+int m2d_get_density_at_nodes(const int *nx, const int *ny, const double *Rg, const double *p,
+                             const double *T, double *ro);                          /* :6-17 */
+int m2d_get_density_at_faces(const int *nx, const int *ny, const double *beta,
+                             const double *ro, const double *Uce, const double *Vcn,
+                             double *roe, double *ron);                             /* :20-60 */
+int m2d_get_u_coefficients(const int *nx, const int *ny, const int *modvis, const double *dt,
+    const double *rp, const double *re, const double *rn, const double *Jp, const double *Je,
+    const double *Jn, const double *ye, const double *yk, const double *alphae,
+    const double *betae, const double *betan, const double *gamman, const double *vle,
+    const double *vln, const double *roe, const double *ron, const double *roa,
+    const double *Uce, const double *Vcn, double *a);                              /* :63-218 */
+int m2d_get_u_source(const int *nx, const int *ny, const int *modvis, const double *beta,
+    const double *dt, const double *rp, const double *re, const double *rn, const double *xe,
+    const double *ye, const double *xk, const double *yk, const double *xke, const double *yke,
+    const double *xen, const double *yen, const double *Jp, const double *Je, const double *Jn,
+    const double *roe, const double *ron, const double *roa, const double *p, const double *vle,
+    const double *vln, const double *Uce, const double *Vcn, const double *ua, const double *u,
+    const double *v, double *cup, double *sup, double *b);                         /* :221-451 */
+int m2d_get_v_coefficients(const int *nx, const int *ny, const int *coord, const int *modvis,
+    const double *dt, const double *rp, const double *re, const double *rn, const double *Jp,
+    const double *Je, const double *Jn, const double *xe, const double *xk,
+    const double *alphae, const double *betae, const double *betan, const double *gamman,
+    const double *vle, const double *vln, const double *vlp, const double *roe,
+    const double *ron, const double *roa, const double *Uce, const double *Vcn,
+    double *a);                                                                    /* :454-613 */
+int m2d_get_v_source(const int *nx, const int *ny, const int *coord, const int *modvis,
+    const double *beta, const double *dt, const double *rp, const double *re, const double *rn,
+    const double *xe, const double *ye, const double *xk, const double *yk, const double *xke,
+    const double *yke, const double *xen, const double *yen, const double *Jp, const double *Je,
+    const double *Jn, const double *roe, const double *ron, const double *roa, const double *p,
+    const double *vle, const double *vln, const double *Uce, const double *Vcn,
+    const double *va, const double *u, const double *v, double *cvp, double *svp,
+    double *b);                                                                    /* :616-783 */
+int m2d_get_T_coefficients_and_source(const int *nx, const int *ny, const int *modvis,
+    const double *beta, const double *dt, const double *rp, const double *re, const double *rn,
+    const double *xe, const double *ye, const double *xk, const double *yk, const double *xke,
+    const double *yke, const double *xen, const double *yen, const double *alphae,
+    const double *betae, const double *betan, const double *gamman, const double *Jp,
+    const double *Je, const double *Jn, const double *roe, const double *ron, const double *ro,
+    const double *roa, const double *p, const double *pa, const double *cp, const double *vle,
+    const double *vln, const double *ke, const double *kn, const double *Uce, const double *Vcn,
+    const double *u, const double *v, const double *ue, const double *ve, const double *un,
+    const double *vn, const double *ua, const double *va, const double *T, const double *Ta,
+    const double *fbe, const double *fbn, double *a, double *b);                   /* :787-1203 */
+int m2d_get_p_coefficients(const int *nx, const int *ny, const double *dt, const double *rp,
+    const double *re, const double *rn, const double *Jp, const double *Uce, const double *Vcn,
+    const double *roe, const double *ron, const double *g, const double *de, const double *dn,
+    double *a);                                                                    /* :1207-1278 */
+int m2d_get_p_source(const int *nx, const int *ny, const double *dt, const double *rp,
+    const double *re, const double *rn, const double *Jp, const double *roe, const double *ron,
+    const double *ro, const double *roa, const double *Uce, const double *Vcn, const double *de,
+    const double *dn, const double *g, const double *pl, double *b);               /* :1281-1348 */
+int m2d_get_velocities_at_internal_faces(const int *nx, const int *ny, const double *dt,
+    const double *rp, const double *re, const double *rn, const double *xe, const double *ye,
+    const double *xk, const double *yk, const double *xen, const double *yen, const double *xke,
+    const double *yke, const double *Jp, const double *cup, const double *cvp, const double *sup,
+    const double *svp, const double *au, const double *av, const double *roa, const double *p,
+    const double *u, const double *v, const double *uea, const double *vea, const double *una,
+    const double *vna, double *ue, double *ve, double *un, double *vn, double *Uce,
+    double *Vcn);                                                                  /* :1350-1501 */
+int m2d_get_internal_simplec_coefficients(const int *nx, const int *ny, const double *re,
+    const double *rn, const double *xe, const double *ye, const double *xk, const double *yk,
+    const double *au, const double *av, double *due, double *dve, double *dun, double *dvn,
+    double *de, double *dn);                                                       /* :1504-1600 */
+int m2d_get_pressure_correction_with_pl(const int *nx, const int *ny, const double *pl,
+                                        double *p);                               /* :1602-1611 */
+int m2d_get_density_correction_with_pl(const int *nx, const int *ny, const double *pl,
+                                       const double *g, double *ro);              /* :1614-1624 */
+int m2d_get_u_v_at_real_nodes_with_pl(const int *nx, const int *ny, const double *xe,
+    const double *ye, const double *xk, const double *yk, const double *rp, const double *pl,
+    const double *au, const double *av, double *u, double *v);                     /* :1626-1675 */
+int m2d_get_velocity_correction_at_faces_with_pl(const int *nx, const int *ny,
+    const double *xe, const double *ye, const double *xk, const double *yk, const double *due,
+    const double *dve, const double *dun, const double *dvn, const double *de, const double *dn,
+    const double *pl, double *ue, double *ve, double *un, double *vn, double *Uce,
+    double *Vcn);                                                                  /* :1679-1758 */
+int m2d_initialize_boundary_faces_flags(const int *nx, const int *ny, double *fbe,
+                                        double *fbn);                             /* :1764-1828 */
+int m2d_check_mass_conservation(const int *nx, const int *ny, const double *dt,
+    const double *rp, const double *re, const double *rn, const double *Jp, const double *ro,
+    const double *roa, const double *ron, const double *roe, const double *Uce,
+    const double *Vcn, double *res);                                               /* :1833-1880 */
+
+/* ---- internal-flow plug-in: src/user/internal_flow/mod_intflow.f90 ------- */
+int m2d_intflow_set_bcu(const int *nx, const int *ny, const int *modvis, const double *x,
+    const double *xp, const double *xk, const double *yk, const double *u, const double *v,
+    double *au, double *b);                                                        /* :214-301 */
+int m2d_intflow_set_bcv(const int *nx, const int *ny, const int *modvis, const double *x,
+    const double *xp, const double *xk, const double *yk, const double *u, const double *v,
+    double *av, double *b);                                                        /* :305-392 */
+/* plin(ny) stands for iflow%plin of the derived-type argument */
+int m2d_intflow_set_bcpl(const int *nx, const int *ny, const double *x, const double *xp,
+    const double *pl, const double *plin, double *ap, double *bp);                 /* :396-459 */
+/* Twall and Tin(ny) stand for iflow%Twall and iflow%Tin */
+int m2d_intflow_set_bcT(const int *nx, const int *ny, const double *x, const double *xp,
+    const double *T, const double *Twall, const double *Tin, double *at, double *bt); /* :464-550 */
+int m2d_intflow_boundary_T_from_H_conservation(const int *nx, const int *ny,
+    const double *Cpref, const double *Href, const double *Tin, const double *u,
+    const double *ue, const double *un, const double *v, const double *ve, const double *vn,
+    double *T, double *Tbe, double *Tbw, double *Tbn, double *Tbs);               /* :557-688 */
+int m2d_intflow_velocities_at_boundary_faces(const int *nx, const int *ny, const int *modvis,
+    const double *x, const double *xp, const double *xe, const double *ye, const double *xk,
+    const double *yk, const double *u, const double *v, double *ue, double *ve, double *un,
+    double *vn, double *Uce, double *Vcn);                                         /* :692-787 */
+int m2d_intflow_boundary_simplec(const int *nx, const int *ny, const int *modvis, double *due,
+    double *dve, double *dun, double *dvn, double *de, double *dn);                /* :791-877 */
+int m2d_intflow_extrapolate_u_v_to_fictitious(const int *nx, const int *ny, const int *modvis,
+    const double *x, const double *xp, const double *xk, const double *yk, double *u,
+    double *v);                                                                    /* :881-964 */
+/* intflow_time_cycle_update (:1106-1134): gamma, Rg, P0, T0 and the inlet
+ * arrays (ny each) stand for the thermophysical model and iflow members */
+int m2d_intflow_time_cycle_update(const int *nx, const int *ny, const double *x,
+    const double *xp, const double *u, const double *gamma, const double *Rg,
+    const double *P0, const double *T0, double *uin, double *vin, double *pin, double *Tin,
+    double *Mw, double *plin, double *pina, double *p);
+
+/* ===================== 2. device-resident SIMPLEC context =================
+ * Mirrors the set-up and the `it` loop body of src/mach2d_main.f90:25-445 for
+ * internal flow with constant thermophysical properties. */
+
+typedef struct m2d_case {
+    int geom;                               /* 0: C01 cosine nozzle, 1: N01 nozzle */
+    double Lc, Ld, Rin, Rout;               /* C01 (Rin, Rout also N01) */
+    double Rth, Rc1, Rc2, Rc3, alf, bet, Lchamb;  /* N01, geometry_n01.txt */
+    int nxr, nyr;                           /* real volumes (nxi-2, nyi-2 at nmd = nmf) */
+    int kg, kcm;                            /* grid kind 1 uniform / 2 geometric; centroid mean */
+    double a1;                              /* first wall-cell width for kg = 2 */
+    int coord, modvis;
+    double beta;
+    double p0, T0, Twall;                   /* Tnbc: Twall <= 0 means adiabatic */
+    double Rg, gamma, mu, kappa;            /* CONSTANT thermophysical model */
+    int itmmax, itpmax;
+    double tolm, tolt;
+    int solver;                             /* 0 MSI, 1 TDMA */
+    int nitm_u, nitm_p;
+    double tol_u, tol_p;
+    int dtmodel;                            /* 0 RAMP, 1 SCARBOROUGH */
+    double dt1, dt2; int it1, it2;
+    double h0, mincc, maxcc;
+    int nan_policy;                         /* max() with the NaN of at = 0: 0 drop, 1 propagate */
+} m2d_case;
+
+typedef struct m2d_report {
+    int it;
+    double dt, norm, normpl, rmass, fmi, fme, Fd;
+    int itp_used;
+} m2d_report;
+
+typedef struct m2d_ctx m2d_ctx;
+
+int m2d_create(const m2d_case *c, int device, m2d_ctx **out);
+int m2d_destroy(m2d_ctx *ctx);
+int m2d_dims(const m2d_ctx *ctx, int *nx, int *ny);
+/* one pass of the `it` loop body, src/mach2d_main.f90:94-445 */
+int m2d_iterate(m2d_ctx *ctx, m2d_report *rep);
+/* up to itmax iterations with the reference's stopping rule
+ * (normpl < tolt first at it, then stop at it_stop = 2 it; :441-443) */
+int m2d_run(m2d_ctx *ctx, int itmax, m2d_report *last);
+/* copy a named field (reference variable name: "u", "p", "au", "Tbn", ...) */
+int m2d_get_field(m2d_ctx *ctx, const char *name, double *host, long n);
+int m2d_set_field(m2d_ctx *ctx, const char *name, const double *host, long n);
+/* named scalars: dt, norm, normpl, rmass, p_avg, Href, Cpref, fm1D, Fd1D,
+ * Fpv1D, Sg, it, it_stop */
+int m2d_get_scalar(const m2d_ctx *ctx, const char *name, double *out);
+/* post-processing integrals (src/user/internal_flow/mod_intflow.f90:1591-1643,
+ * mod_intflow_postp.f90:1211 Cd = fme/fm1D, :430-445,1454-1465 wall pressure
+ * p(i,ny-1) for i = 1..nx into pwall, may be null) */
+int m2d_integrals(m2d_ctx *ctx, double *fmi, double *fme, double *Fd, double *Cd,
+                  double *pwall);
+/* the cudaStream_t the context launches on, and the device address of a
+ * named field (for callers that time or chain their own kernels) */
+int m2d_ctx_stream(const m2d_ctx *ctx, void **stream);
+int m2d_ctx_field_device(m2d_ctx *ctx, const char *name, double **dptr, long *n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

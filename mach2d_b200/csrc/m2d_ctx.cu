@@ -1,0 +1,478 @@
+// m2d_ctx.cu -- device-resident SIMPLEC context: one nozzle instance whose
+// every field lives in HBM for the whole run.  m2d_iterate is the `it` loop
+// body of src/mach2d_main.f90:94-445, launched on one stream; the only host
+// round trips are the ones where the reference takes a control decision
+// (the p' loop exit, :307-309) and one copy of the iteration's scalars at the
+// end (norms, mass residual, convergence coefficients for dt).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include "m2d_fields.cuh"
+#include "m2d_setup.h"
+#include "m2d_solvers.cuh"
+
+using namespace m2d;
+
+namespace {
+enum Slot {
+    S_PSUM = 0, S_MAXPL, S_NU_A, S_NU_B, S_NV_A, S_NV_B, S_NP, S_NT_A, S_NT_B, S_RMASS,
+    S_CC_U, S_CC_V, S_CC_T, S_CC_P, S_FMI, S_FME, S_FD, S_RR = 20, S_COUNT = 40
+};
+enum ISlot { I_NIT_U = 0, I_NIT_V, I_NIT_P, I_NIT_T, I_ERR, I_COUNT = 8 };
+}
+
+struct m2d_ctx {
+    m2d_case c;
+    int device = 0;
+    cudaStream_t st = nullptr;
+    int nx = 0, ny = 0;
+    size_t N = 0;
+    Fields f;
+    Params q;
+    double *arena = nullptr;
+    double *dl9[2], *du9[2], *wk9[2], *dl5, *du5, *wk5, *P, *Q, *part;
+    double *dsc = nullptr;
+    int *dint = nullptr;
+    double *hsc = nullptr;   // pinned mirror of dsc
+    int *hint = nullptr;     // pinned mirror of dint
+    double dt = 0, norm = 0, normpl = 0, rmass = 0, p_avg = 0;
+    double Href = 0, Cpref = 0, fm1D = 0, Fd1D = 0, Fpv1D = 0, Sg = 0;
+    int it = 0, it_stop = -1, itp_used = 0;
+    long long launches = 0;   // kernels launched by m2d_iterate so far
+};
+
+static int ctx_fail(int code, const char *msg)
+{
+    extern void m2d_set_last_error_msg(const char *);
+    m2d_set_last_error_msg(msg);
+    return code;
+}
+
+#define TRY(expr)                                                                 \
+    do {                                                                          \
+        cudaError_t _e = (expr);                                                  \
+        if (_e != cudaSuccess) { m2d_set_last_error(_e, #expr, __FILE__, __LINE__); return M2D_ERR_CUDA; } \
+    } while (0)
+
+// launch through the context `x`, counting the kernels it starts
+#define KL(expr, n)              \
+    do {                         \
+        TRY(expr);               \
+        x->launches += (n);      \
+    } while (0)
+
+static double *plane_ptr(m2d_ctx *x, const char *name, long *n)
+{
+    Fields &f = x->f;
+    const long N = (long)x->N;
+#define M2D_MATCH(nm) if (!strcmp(name, #nm)) { *n = N; return f.nm; }
+    M2D_PLANES(M2D_MATCH)
+#undef M2D_MATCH
+    if (!strcmp(name, "au")) { *n = 9 * N; return f.au; }
+    if (!strcmp(name, "av")) { *n = 9 * N; return f.av; }
+    if (!strcmp(name, "at")) { *n = 9 * N; return f.at; }
+    if (!strcmp(name, "ap")) { *n = 5 * N; return f.ap; }
+    const struct { const char *nm; double *p; long len; } strips[] = {
+        {"uin", f.uin, x->ny}, {"vin", f.vin, x->ny}, {"pin", f.pin, x->ny}, {"Tin", f.Tin, x->ny},
+        {"Mw", f.Mw, x->ny}, {"plin", f.plin, x->ny}, {"pina", f.pina, x->ny}, {"Tbe", f.Tbe, x->ny},
+        {"Tbw", f.Tbw, x->ny}, {"Tbn", f.Tbn, x->nx}, {"Tbs", f.Tbs, x->nx}};
+    for (auto &s : strips)
+        if (!strcmp(name, s.nm)) { *n = s.len; return s.p; }
+    return nullptr;
+}
+
+extern "C" int m2d_create(const m2d_case *c, int device, m2d_ctx **out)
+{
+    if (!c || !out) return ctx_fail(M2D_ERR_ARG, "m2d_create: null argument");
+    *out = nullptr;
+    if (c->nxr < 3 || c->nyr < 3) return ctx_fail(M2D_ERR_ARG, "m2d_create: need at least 3x3 real volumes");
+    if (c->solver == 0 && c->nyr + 2 > msi_max_ny()) return ctx_fail(M2D_ERR_TOO_LARGE, "m2d_create: ny exceeds m2d_msi_max_ny()");
+    HostInstance h;
+    int rc = build_instance(*c, h);
+    if (rc) return ctx_fail(rc, "m2d_create: grid set-up failed");
+    m2d_ctx *x = new m2d_ctx();
+    x->c = *c;
+    x->device = device;
+    x->nx = h.nx; x->ny = h.ny;
+    x->N = (size_t)h.nx * h.ny;
+    const size_t N = x->N;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) { delete x; m2d_set_last_error(e, "cudaSetDevice", __FILE__, __LINE__); return M2D_ERR_CUDA; }
+    e = cudaStreamCreateWithFlags(&x->st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { delete x; m2d_set_last_error(e, "cudaStreamCreate", __FILE__, __LINE__); return M2D_ERR_CUDA; }
+    // one arena: planes + 9N x 3 + 5N + strips + solver scratch + reductions
+    const size_t nplanes = h.planes().size();
+    const size_t strips = (size_t)9 * h.ny + 2 * (size_t)h.nx + 64;
+    const size_t solver = 2 * (5 + 4 + 1) * N + (4 + 3 + 1) * N + 2 * N;
+    const size_t total = nplanes * N + 32 * N + strips + solver + (size_t)red_parts() + 64 + S_COUNT;
+    e = cudaMalloc(&x->arena, total * sizeof(double));
+    if (e != cudaSuccess) { cudaStreamDestroy(x->st); delete x; m2d_set_last_error(e, "cudaMalloc", __FILE__, __LINE__); return M2D_ERR_NOMEM; }
+    cudaMemsetAsync(x->arena, 0, total * sizeof(double), x->st);
+    double *cur = x->arena;
+    auto take = [&](size_t n) { double *p = cur; cur += n; return p; };
+    Fields &f = x->f;
+    memset(&f, 0, sizeof f);
+    f.nx = h.nx; f.ny = h.ny;
+#define M2D_TAKE(nm) f.nm = take(N);
+    M2D_PLANES(M2D_TAKE)
+#undef M2D_TAKE
+    f.au = take(9 * N); f.av = take(9 * N); f.at = take(9 * N); f.ap = take(5 * N);
+    f.uin = take(h.ny); f.vin = take(h.ny); f.pin = take(h.ny); f.Tin = take(h.ny);
+    f.Mw = take(h.ny); f.plin = take(h.ny); f.pina = take(h.ny); f.Tbe = take(h.ny); f.Tbw = take(h.ny);
+    f.Tbn = take(h.nx); f.Tbs = take(h.nx);
+    for (int k = 0; k < 2; k++) { x->dl9[k] = take(5 * N); x->du9[k] = take(4 * N); x->wk9[k] = take(N); }
+    x->dl5 = take(4 * N); x->du5 = take(3 * N); x->wk5 = take(N);
+    x->P = take(N); x->Q = take(N);
+    x->part = take((size_t)red_parts() + 8);
+    x->dsc = take(S_COUNT);
+    x->dint = (int *)take(I_COUNT);
+    if ((size_t)(cur - x->arena) > total) { m2d_destroy(x); return ctx_fail(M2D_ERR_NOMEM, "m2d_create: arena overflow"); }
+    e = cudaMallocHost(&x->hsc, S_COUNT * sizeof(double));
+    if (e == cudaSuccess) e = cudaMallocHost(&x->hint, I_COUNT * sizeof(int));
+    if (e != cudaSuccess) { m2d_destroy(x); m2d_set_last_error(e, "cudaMallocHost", __FILE__, __LINE__); return M2D_ERR_NOMEM; }
+    // ap(:,3) = 1 (src/mod_mach2d_data.f90:403)
+    {
+        std::vector<double> ap(5 * N, 0.0);
+        std::fill(ap.begin() + 2 * N, ap.begin() + 3 * N, 1.0);
+        e = cudaMemcpyAsync(f.ap, ap.data(), 5 * N * sizeof(double), cudaMemcpyHostToDevice, x->st);
+        for (auto &kv : h.planes()) {
+            long n; double *d = plane_ptr(x, kv.first, &n);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(d, kv.second->data(), N * sizeof(double), cudaMemcpyHostToDevice, x->st);
+        }
+        const struct { double *d; std::vector<double> *v; } sv[] = {
+            {f.uin, &h.uin}, {f.vin, &h.vin}, {f.pin, &h.pin}, {f.Tin, &h.Tin}, {f.Mw, &h.Mw},
+            {f.plin, &h.plin}, {f.pina, &h.pina}, {f.Tbe, &h.Tbe}, {f.Tbw, &h.Tbw}, {f.Tbn, &h.Tbn},
+            {f.Tbs, &h.Tbs}};
+        for (auto &s : sv)
+            if (e == cudaSuccess) e = cudaMemcpyAsync(s.d, s.v->data(), s.v->size() * sizeof(double), cudaMemcpyHostToDevice, x->st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(x->st);
+        if (e != cudaSuccess) { m2d_destroy(x); m2d_set_last_error(e, "upload", __FILE__, __LINE__); return M2D_ERR_CUDA; }
+    }
+    Params &q = x->q;
+    memset(&q, 0, sizeof q);
+    q.modvis = c->modvis; q.coord = c->coord; q.beta = c->beta; q.Rg = c->Rg; q.gamma = c->gamma;
+    q.p0 = c->p0; q.T0 = c->T0; q.Cpref = h.Cpref; q.Href = h.Href; q.Twall = c->Twall;
+    x->Href = h.Href; x->Cpref = h.Cpref; x->fm1D = h.fm1D; x->Fd1D = h.Fd1D; x->Fpv1D = h.Fpv1D;
+    x->Sg = h.Sg; x->dt = h.dt0;
+    *out = x;
+    return M2D_OK;
+}
+
+extern "C" int m2d_destroy(m2d_ctx *x)
+{
+    if (!x) return M2D_OK;
+    if (x->st) cudaStreamSynchronize(x->st);
+    if (x->arena) cudaFree(x->arena);
+    if (x->hsc) cudaFreeHost(x->hsc);
+    if (x->hint) cudaFreeHost(x->hint);
+    if (x->st) cudaStreamDestroy(x->st);
+    delete x;
+    return M2D_OK;
+}
+
+extern "C" int m2d_dims(const m2d_ctx *x, int *nx, int *ny)
+{
+    if (!x) return ctx_fail(M2D_ERR_ARG, "m2d_dims: null context");
+    if (nx) *nx = x->nx;
+    if (ny) *ny = x->ny;
+    return M2D_OK;
+}
+
+static RedArgs red(const m2d_ctx *x, int kind)
+{
+    RedArgs r;
+    memset(&r, 0, sizeof r);
+    r.kind = kind; r.nx = x->nx; r.ny = x->ny;
+    return r;
+}
+
+// linear solves of the iteration: solver9d%solve / solver5d%solve
+static int solve9(m2d_ctx *x, int nsys, double *const *a, double *const *b, double *const *v,
+                  const int *islot, const int *rslot)
+{
+    const m2d_case &c = x->c;
+    if (c.solver == 0) {
+        MsiLaunch L;
+        memset(&L, 0, sizeof L);
+        L.nx = x->nx; L.ny = x->ny; L.nitm = c.nitm_u; L.tol = c.tol_u;
+        L.err = x->dint + I_ERR;
+        for (int k = 0; k < nsys; k++) {
+            L.s[k].a = a[k]; L.s[k].b = b[k]; L.s[k].x = v[k];
+            L.s[k].dl = x->dl9[k]; L.s[k].du = x->du9[k]; L.s[k].wk = x->wk9[k];
+            L.s[k].nit = x->dint + islot[k]; L.s[k].rr = x->dsc + rslot[k];
+        }
+        KL(launch_msi(9, L, nsys, x->st), 1);
+    } else {
+        for (int k = 0; k < nsys; k++)
+            KL(launch_tdma(9, x->nx, x->ny, c.nitm_u, a[k], b[k], v[k], x->P, x->Q, x->st), 4 * c.nitm_u);
+    }
+    return M2D_OK;
+}
+
+static int solve5(m2d_ctx *x)
+{
+    const m2d_case &c = x->c;
+    if (c.solver == 0) {
+        MsiLaunch L;
+        memset(&L, 0, sizeof L);
+        L.nx = x->nx; L.ny = x->ny; L.nitm = c.nitm_p; L.tol = c.tol_p;
+        L.err = x->dint + I_ERR;
+        L.s[0].a = x->f.ap; L.s[0].b = x->f.bp; L.s[0].x = x->f.pl;
+        L.s[0].dl = x->dl5; L.s[0].du = x->du5; L.s[0].wk = x->wk5;
+        L.s[0].nit = x->dint + I_NIT_P; L.s[0].rr = x->dsc + S_RR + 4;
+        KL(launch_msi(5, L, 1, x->st), 1);
+    } else {
+        KL(launch_tdma(5, x->nx, x->ny, c.nitm_p, x->f.ap, x->f.bp, x->f.pl, x->P, x->Q, x->st), 4 * c.nitm_p);
+    }
+    return M2D_OK;
+}
+
+static double max4(double a, double b, double c, double d, int nan_policy)
+{
+    double v[4] = {a, b, c, d};
+    if (nan_policy == 1) {
+        for (double t : v) if (std::isnan(t)) return NAN;
+        double m = a;
+        for (int k = 1; k < 4; k++) if (v[k] > m) m = v[k];
+        return m;
+    }
+    double m = NAN;
+    for (double t : v) {
+        if (std::isnan(t)) continue;
+        if (std::isnan(m) || t > m) m = t;
+    }
+    return m;
+}
+
+extern "C" int m2d_iterate(m2d_ctx *x, m2d_report *rep)
+{
+    if (!x) return ctx_fail(M2D_ERR_ARG, "m2d_iterate: null context");
+    TRY(cudaSetDevice(x->device));
+    const m2d_case &c = x->c;
+    Fields &f = x->f;
+    Params q = x->q;
+    cudaStream_t st = x->st;
+    const int it = ++x->it;
+    q.dt = x->dt;
+    TRY(cudaMemsetAsync(x->dint, 0, I_COUNT * sizeof(int), st));
+    KL(launch_backup(f, st), 1);
+    KL(launch_inlet_update(f, q, st), 1);
+    {
+        RedArgs r = red(x, RED_SUM_REAL); r.x = f.p;
+        KL(launch_reduce(r, x->part, x->dsc + S_PSUM, st), 2);
+    }
+    KL(launch_g(f, q.Rg, st), 1);
+    TRY(cudaMemcpyAsync(x->hsc, x->dsc, S_COUNT * sizeof(double), cudaMemcpyDeviceToHost, st));
+    bool have_pavg = false;
+    int itp_used = 0;
+    for (int itm = 1; itm <= c.itmmax; itm++) {
+        KL(launch_u_assembly(f, q, ASM_COEF | ASM_SRC, st), 1);
+        KL(launch_set_bcu(f, c.modvis, st), 1);
+        KL(launch_v_assembly(f, q, ASM_COEF | ASM_SRC, st), 1);
+        KL(launch_set_bcv(f, c.modvis, st), 1);
+        KL(launch_internal_simplec(f, st), 1);
+        KL(launch_boundary_simplec(f, st), 1);
+        {
+            double *a[2] = {f.au, f.av}, *b[2] = {f.bu, f.bv}, *v[2] = {f.u, f.v};
+            int is[2] = {I_NIT_U, I_NIT_V}, rs[2] = {S_RR, S_RR + 2};
+            int rc = solve9(x, 2, a, b, v, is, rs);
+            if (rc) return rc;
+        }
+        {
+            RedArgs r = red(x, RED_NORM_L1_9D); r.a = f.au; r.b = f.bu; r.x = f.u;
+            KL(launch_reduce(r, x->part, x->dsc + S_NU_A, st), 2);
+            r.kind = RED_SUM_ABS_B;
+            KL(launch_reduce(r, x->part, x->dsc + S_NU_B, st), 2);
+            r = red(x, RED_NORM_L1_9D); r.a = f.av; r.b = f.bv; r.x = f.v;
+            KL(launch_reduce(r, x->part, x->dsc + S_NV_A, st), 2);
+            r.kind = RED_SUM_ABS_B;
+            KL(launch_reduce(r, x->part, x->dsc + S_NV_B, st), 2);
+        }
+        KL(launch_velocities_at_internal_faces(f, q.dt, st), 1);
+        KL(launch_velocities_at_boundary_faces(f, c.modvis, st), 1);
+        TRY(cudaMemsetAsync(f.pl, 0, x->N * sizeof(double), st));
+        for (int itp = 1; itp <= c.itpmax; itp++) {
+            itp_used = itp;
+            KL(launch_p_assembly(f, q, ASM_COEF, st), 1);
+            KL(launch_set_bcpl(f, st), 1);
+            KL(launch_p_assembly(f, q, ASM_SRC, st), 1);
+            int rc = solve5(x);
+            if (rc) return rc;
+            KL(launch_velocity_correction_at_faces(f, st), 1);
+            KL(launch_velocities_at_boundary_faces(f, c.modvis, st), 1);
+            KL(launch_p_ro_correction(f, 1, 1, st), 1);
+            KL(launch_density_at_faces(f, c.beta, st), 1);
+            RedArgs r = red(x, RED_MAXABS_ALL); r.x = f.pl;
+            KL(launch_reduce(r, x->part, x->dsc + S_MAXPL, st), 2);
+            TRY(cudaMemcpyAsync(x->hsc + S_MAXPL, x->dsc + S_MAXPL, sizeof(double), cudaMemcpyDeviceToHost, st));
+            TRY(cudaStreamSynchronize(st));
+            if (!have_pavg) {
+                x->p_avg = x->hsc[S_PSUM] / ((double)(x->nx - 2) * (double)(x->ny - 2));
+                have_pavg = true;
+            }
+            x->normpl = x->hsc[S_MAXPL] / x->p_avg;
+            if (x->normpl < c.tolm) break;
+        }
+        {
+            RedArgs r = red(x, RED_NORM_L1_5D); r.a = f.ap; r.b = f.bp; r.x = f.pl;
+            KL(launch_reduce(r, x->part, x->dsc + S_NP, st), 2);
+        }
+        KL(launch_uv_nodes_correction(f, st), 1);
+        KL(launch_extrapolate_uv(f, c.modvis, st), 1);
+    }
+    {
+        RedArgs r = red(x, RED_MASS);
+        r.rp = f.rp; r.re = f.re; r.rn = f.rn; r.Jp = f.Jp; r.ro = f.ro; r.roa = f.roa;
+        r.ron = f.ron; r.roe = f.roe; r.Uce = f.Uce; r.Vcn = f.Vcn; r.dt = q.dt;
+        KL(launch_reduce(r, x->part, x->dsc + S_RMASS, st), 2);
+    }
+    const bool h_conservation = (c.modvis == 0);   // constant properties only in this build
+    if (h_conservation) {
+        KL(launch_T_from_H(f, x->Href, x->Cpref, st), 2);
+    } else {
+        KL(launch_T_assembly(f, q, st), 1);
+        KL(launch_set_bcT(f, c.Twall, st), 1);
+        double *a[1] = {f.at}, *b[1] = {f.bt}, *v[1] = {f.T};
+        int is[1] = {I_NIT_T}, rs[1] = {S_RR + 6};
+        int rc = solve9(x, 1, a, b, v, is, rs);
+        if (rc) return rc;
+        RedArgs r = red(x, RED_NORM_L1_9D); r.a = f.at; r.b = f.bt; r.x = f.T;
+        KL(launch_reduce(r, x->part, x->dsc + S_NT_A, st), 2);
+        r.kind = RED_SUM_ABS_B;
+        KL(launch_reduce(r, x->part, x->dsc + S_NT_B, st), 2);
+    }
+    KL(launch_density_at_nodes(f, q.Rg, st), 1);
+    KL(launch_density_at_faces(f, c.beta, st), 1);
+    if (c.dtmodel == 1) {
+        RedArgs r = red(x, RED_MEAN_CC_9D); r.a = f.au;
+        KL(launch_reduce(r, x->part, x->dsc + S_CC_U, st), 2);
+        r.a = f.av;
+        KL(launch_reduce(r, x->part, x->dsc + S_CC_V, st), 2);
+        r.a = f.at;
+        KL(launch_reduce(r, x->part, x->dsc + S_CC_T, st), 2);
+        r = red(x, RED_MEAN_CC_5D); r.a = f.ap;
+        KL(launch_reduce(r, x->part, x->dsc + S_CC_P, st), 2);
+    }
+    KL(launch_mass_flow_thrust(f, x->dsc + S_FMI, st), 1);
+    TRY(cudaMemcpyAsync(x->hsc, x->dsc, S_COUNT * sizeof(double), cudaMemcpyDeviceToHost, st));
+    TRY(cudaMemcpyAsync(x->hint, x->dint, I_COUNT * sizeof(int), cudaMemcpyDeviceToHost, st));
+    TRY(cudaStreamSynchronize(st));
+    const double *hs = x->hsc;
+    const double eps = 10.0 * 2.220446049250313e-16;
+    double norm = 0.0;
+    norm = norm + (hs[S_NU_B] > eps ? hs[S_NU_A] / hs[S_NU_B] : hs[S_NU_A]);
+    norm = norm + (hs[S_NV_B] > eps ? hs[S_NV_A] / hs[S_NV_B] : hs[S_NV_A]);
+    norm = norm + hs[S_NP];
+    if (!h_conservation) norm = norm + (hs[S_NT_B] > eps ? hs[S_NT_A] / hs[S_NT_B] : hs[S_NT_A]);
+    x->norm = norm;
+    x->rmass = hs[S_RMASS];
+    x->itp_used = itp_used;
+    if (c.dtmodel == 1) {
+        double cc = max4(hs[S_CC_U], hs[S_CC_V], hs[S_CC_T], hs[S_CC_P], c.nan_policy);
+        double hh;
+        if (cc < c.mincc) hh = c.h0 * std::sqrt(1.0 - cc / c.mincc);
+        else if (c.maxcc < cc) hh = -(c.h0 * std::sqrt(cc / c.maxcc - 1.0));
+        else hh = 0.0;
+        x->dt = x->dt * (1.0 + hh);
+    } else {
+        x->dt = ramp_dt(it, c);
+    }
+    if (rep) {
+        rep->it = it; rep->dt = x->dt; rep->norm = x->norm; rep->normpl = x->normpl;
+        rep->rmass = x->rmass; rep->fmi = hs[S_FMI]; rep->fme = hs[S_FME]; rep->Fd = hs[S_FD];
+        rep->itp_used = itp_used;
+    }
+    if (x->hint[I_ERR] & ERR_WAIT_TIMEOUT) return ctx_fail(M2D_ERR_TIMEOUT, "m2d_iterate: MSI iteration cap reached");
+    if (std::isnan(x->norm)) return ctx_fail(M2D_ERR_NAN, "m2d_iterate: NaN detected");
+    if (x->normpl < c.tolt && x->it_stop < 0) x->it_stop = it * 2;
+    return M2D_OK;
+}
+
+extern "C" int m2d_run(m2d_ctx *x, int itmax, m2d_report *last)
+{
+    if (!x) return ctx_fail(M2D_ERR_ARG, "m2d_run: null context");
+    for (int k = 0; k < itmax; k++) {
+        int rc = m2d_iterate(x, last);
+        if (rc) return rc;
+        if (x->it_stop == x->it) break;
+    }
+    return M2D_OK;
+}
+
+extern "C" int m2d_get_field(m2d_ctx *x, const char *name, double *host, long n)
+{
+    if (!x || !name || !host) return ctx_fail(M2D_ERR_ARG, "m2d_get_field: null argument");
+    long len = 0;
+    double *d = plane_ptr(x, name, &len);
+    if (!d) return ctx_fail(M2D_ERR_ARG, "m2d_get_field: unknown field");
+    if (n < len) return ctx_fail(M2D_ERR_ARG, "m2d_get_field: host buffer too small");
+    TRY(cudaSetDevice(x->device));
+    TRY(cudaMemcpyAsync(host, d, (size_t)len * sizeof(double), cudaMemcpyDeviceToHost, x->st));
+    TRY(cudaStreamSynchronize(x->st));
+    return M2D_OK;
+}
+
+extern "C" int m2d_set_field(m2d_ctx *x, const char *name, const double *host, long n)
+{
+    if (!x || !name || !host) return ctx_fail(M2D_ERR_ARG, "m2d_set_field: null argument");
+    long len = 0;
+    double *d = plane_ptr(x, name, &len);
+    if (!d) return ctx_fail(M2D_ERR_ARG, "m2d_set_field: unknown field");
+    if (n != len) return ctx_fail(M2D_ERR_ARG, "m2d_set_field: size mismatch");
+    TRY(cudaSetDevice(x->device));
+    TRY(cudaMemcpyAsync(d, host, (size_t)len * sizeof(double), cudaMemcpyHostToDevice, x->st));
+    TRY(cudaStreamSynchronize(x->st));
+    return M2D_OK;
+}
+
+extern "C" int m2d_get_scalar(const m2d_ctx *x, const char *name, double *out)
+{
+    if (!x || !name || !out) return ctx_fail(M2D_ERR_ARG, "m2d_get_scalar: null argument");
+    const struct { const char *nm; double v; } tab[] = {
+        {"dt", x->dt}, {"norm", x->norm}, {"normpl", x->normpl}, {"rmass", x->rmass},
+        {"p_avg", x->p_avg}, {"Href", x->Href}, {"Cpref", x->Cpref}, {"fm1D", x->fm1D},
+        {"Fd1D", x->Fd1D}, {"Fpv1D", x->Fpv1D}, {"Sg", x->Sg}, {"it", (double)x->it},
+        {"it_stop", (double)x->it_stop}, {"itp_used", (double)x->itp_used},
+        {"launches", (double)x->launches}, {"nit_u", (double)x->hint[I_NIT_U]}, {"nit_v", (double)x->hint[I_NIT_V]},
+        {"nit_p", (double)x->hint[I_NIT_P]}, {"nit_T", (double)x->hint[I_NIT_T]}};
+    for (auto &t : tab)
+        if (!strcmp(name, t.nm)) { *out = t.v; return M2D_OK; }
+    return ctx_fail(M2D_ERR_ARG, "m2d_get_scalar: unknown scalar");
+}
+
+extern "C" int m2d_ctx_stream(const m2d_ctx *x, void **stream)
+{
+    if (!x || !stream) return ctx_fail(M2D_ERR_ARG, "m2d_ctx_stream: null argument");
+    *stream = (void *)x->st;
+    return M2D_OK;
+}
+
+extern "C" int m2d_ctx_field_device(m2d_ctx *x, const char *name, double **dptr, long *n)
+{
+    if (!x || !name || !dptr) return ctx_fail(M2D_ERR_ARG, "m2d_ctx_field_device: null argument");
+    long len = 0;
+    double *d = plane_ptr(x, name, &len);
+    if (!d) return ctx_fail(M2D_ERR_ARG, "m2d_ctx_field_device: unknown field");
+    *dptr = d;
+    if (n) *n = len;
+    return M2D_OK;
+}
+
+extern "C" int m2d_integrals(m2d_ctx *x, double *fmi, double *fme, double *Fd, double *Cd,
+                             double *pwall)
+{
+    if (!x) return ctx_fail(M2D_ERR_ARG, "m2d_integrals: null context");
+    TRY(cudaSetDevice(x->device));
+    KL(launch_mass_flow_thrust(x->f, x->dsc + S_FMI, x->st), 1);
+    TRY(cudaMemcpyAsync(x->hsc + S_FMI, x->dsc + S_FMI, 3 * sizeof(double), cudaMemcpyDeviceToHost, x->st));
+    if (pwall)
+        TRY(cudaMemcpyAsync(pwall, x->f.p + (size_t)(x->ny - 2) * x->nx, (size_t)x->nx * sizeof(double),
+                            cudaMemcpyDeviceToHost, x->st));
+    TRY(cudaStreamSynchronize(x->st));
+    if (fmi) *fmi = x->hsc[S_FMI];
+    if (fme) *fme = x->hsc[S_FME];
+    if (Fd) *Fd = x->hsc[S_FD];
+    if (Cd) *Cd = x->hsc[S_FME] / x->fm1D;
+    return M2D_OK;
+}

@@ -1,0 +1,48 @@
+// m2d_solvers.cuh -- MSI (Schneider-Zedan strongly implicit) and line-TDMA
+// solvers for the 9- and 5-diagonal systems of MACH-2D.
+#pragma once
+#include "m2d_common.cuh"
+
+namespace m2d {
+
+// One linear system A x = b.  A is plane-major (ND planes of N doubles),
+// dl/du are the incomplete factors (5+4 planes for ND=9, 4+3 for ND=5), wk
+// is one plane of scratch (residual, then L^-1 r in place).
+struct MsiSys {
+    const double *a;
+    const double *b;
+    double *x;
+    double *dl, *du, *wk;
+    int *nit;          // iterations performed (device int)
+    double *rr;        // [0] = |r0|^2, [1] = |r_final|^2 (device doubles)
+};
+
+struct MsiLaunch {
+    int nx, ny, nitm;
+    double tol;
+    MsiSys s[2];               // up to two systems passed by value ...
+    const MsiSys *dev;         // ... or an array of gridDim.x systems in device memory
+    int *err;                  // device error word (ERR_* bits), may be null
+};
+
+// Largest ny the one-CTA wavefront kernel accepts (its shared-memory ring
+// holds 4 steps x 4 factor values per row).
+int msi_max_ny();
+int msi_block_threads(int ny);
+size_t msi_smem_bytes(int nd, int ny);
+
+// Solves gridDim.x = nsys systems, one CTA each: LU factorisation (lu2d9 /
+// lu2d5) followed by the fb2d9 / fb2d5 iteration, all inside one launch.
+cudaError_t launch_msi(int nd, const MsiLaunch &L, int nsys, cudaStream_t st);
+
+// tdma2d9 / tdma2d5: nitm x (x-line sweep, y-line sweep).  P, Q: N doubles each.
+cudaError_t launch_tdma(int nd, int nx, int ny, int nitm, const double *a, const double *b,
+                        double *x, double *P, double *Q, cudaStream_t st);
+
+// independent tridiagonal lines, line l element i at l*n + i (the x-line
+// layout of tdma2d9): aw, ap, ae, d -> x
+cudaError_t launch_tdma_lines(int n, int nlines, const double *aw, const double *ap,
+                              const double *ae, const double *d, double *x, double *P,
+                              double *Q, cudaStream_t st);
+
+}  // namespace m2d

@@ -1,0 +1,157 @@
+"""Device-resident SIMPLEC driver: the set-up and `it` loop of
+src/mach2d_main.f90:25-445 for internal flow, run through the C ABI context
+(m2d_create / m2d_iterate / m2d_run)."""
+import ctypes
+
+import numpy as np
+
+from ._lib import check, lib
+
+
+class Case(ctypes.Structure):
+    """m2d_case of include/mach2d_b200.h (one nozzle instance)."""
+
+    _fields_ = [
+        ("geom", ctypes.c_int), ("Lc", ctypes.c_double), ("Ld", ctypes.c_double),
+        ("Rin", ctypes.c_double), ("Rout", ctypes.c_double), ("Rth", ctypes.c_double),
+        ("Rc1", ctypes.c_double), ("Rc2", ctypes.c_double), ("Rc3", ctypes.c_double),
+        ("alf", ctypes.c_double), ("bet", ctypes.c_double), ("Lchamb", ctypes.c_double),
+        ("nxr", ctypes.c_int), ("nyr", ctypes.c_int), ("kg", ctypes.c_int), ("kcm", ctypes.c_int),
+        ("a1", ctypes.c_double), ("coord", ctypes.c_int), ("modvis", ctypes.c_int),
+        ("beta", ctypes.c_double), ("p0", ctypes.c_double), ("T0", ctypes.c_double),
+        ("Twall", ctypes.c_double), ("Rg", ctypes.c_double), ("gamma", ctypes.c_double),
+        ("mu", ctypes.c_double), ("kappa", ctypes.c_double), ("itmmax", ctypes.c_int),
+        ("itpmax", ctypes.c_int), ("tolm", ctypes.c_double), ("tolt", ctypes.c_double),
+        ("solver", ctypes.c_int), ("nitm_u", ctypes.c_int), ("nitm_p", ctypes.c_int),
+        ("tol_u", ctypes.c_double), ("tol_p", ctypes.c_double), ("dtmodel", ctypes.c_int),
+        ("dt1", ctypes.c_double), ("dt2", ctypes.c_double), ("it1", ctypes.c_int),
+        ("it2", ctypes.c_int), ("h0", ctypes.c_double), ("mincc", ctypes.c_double),
+        ("maxcc", ctypes.c_double), ("nan_policy", ctypes.c_int),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Report(ctypes.Structure):
+    """m2d_report: the columns of the residual file (src/mach2d_main.f90:495-516)."""
+
+    _fields_ = [("it", ctypes.c_int), ("dt", ctypes.c_double), ("norm", ctypes.c_double),
+                ("normpl", ctypes.c_double), ("rmass", ctypes.c_double), ("fmi", ctypes.c_double),
+                ("fme", ctypes.c_double), ("Fd", ctypes.c_double), ("itp_used", ctypes.c_int)]
+
+
+def euler_cosine_case(nxr=80, nyr=40, **over):
+    """Euler, constant properties, C01 cosine nozzle (Lc = 2, Ld = 4, throat
+    r = 1 m, inlet r = 2, exit r = 1.8), p0 = 1e6 Pa, T0 = 1000 K, with the
+    solver and time-stepper settings of the reference's
+    mach2d_input/parametersNozzleEulerPTC.txt deck."""
+    c = Case(geom=0, Lc=2.0, Ld=4.0, Rin=2.0, Rout=1.8, nxr=nxr, nyr=nyr, kg=1, kcm=1, a1=5e-6,
+             coord=1, modvis=0, beta=0.0, p0=1.0e6, T0=1000.0, Twall=-616.7, Rg=287.0, gamma=1.4,
+             mu=1.0e-5, kappa=1.0e-3, itmmax=1, itpmax=20, tolm=1.0e-2, tolt=1.0e-10, solver=0,
+             nitm_u=5, nitm_p=20, tol_u=1.0e-2, tol_p=1.0e-2, dtmodel=1, dt1=1e-8, dt2=2e-5,
+             it1=100, it2=600, h0=0.01, mincc=0.99, maxcc=0.9999, nan_policy=1)
+    for k, v in over.items():
+        setattr(c, k, v)
+    return c
+
+
+def n01_case(nxr=20, nyr=10, **over):
+    """The reference's own deck: mach2d_input/parametersNozzleEulerPTC.txt with
+    geometry_n01.txt (Euler, constant properties, N01 nozzle, 20x10)."""
+    c = Case(geom=1, Rth=2.29108e-2, Rin=6.4395244991040e-02, Rout=3.7366383992332e-02,
+             Rc1=3.6068e-2, Rc2=4.572e-2, Rc3=4.572e-2, alf=30.0, bet=15.0, Lchamb=2.29108e-2,
+             nxr=nxr, nyr=nyr, kg=1, kcm=1, a1=5e-6, coord=1, modvis=0, beta=0.0, p0=1038350.4,
+             T0=833.33333333, Twall=-616.7, Rg=287.0, gamma=1.4, mu=1.0e-5, kappa=1.0e-3,
+             itmmax=1, itpmax=20, tolm=1.0e-2, tolt=1.0e-10, solver=0, nitm_u=5, nitm_p=20,
+             tol_u=1.0e-2, tol_p=1.0e-2, dtmodel=1, dt1=1e-8, dt2=2e-5, it1=100, it2=600,
+             h0=0.01, mincc=0.99, maxcc=0.9999, nan_policy=0)
+    for k, v in over.items():
+        setattr(c, k, v)
+    return c
+
+
+class Simplec:
+    """One nozzle instance resident on a GPU."""
+
+    def __init__(self, case, device=0):
+        self.case = case
+        self._ctx = ctypes.c_void_p()
+        L = lib()
+        L.m2d_create.argtypes = [ctypes.POINTER(Case), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+        check(L.m2d_create(ctypes.byref(case), int(device), ctypes.byref(self._ctx)))
+        nx, ny = ctypes.c_int(), ctypes.c_int()
+        L.m2d_dims.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+        check(L.m2d_dims(self._ctx, ctypes.byref(nx), ctypes.byref(ny)))
+        self.nx, self.ny = nx.value, ny.value
+
+    def close(self):
+        if self._ctx:
+            lib().m2d_destroy(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def iterate(self):
+        rep = Report()
+        L = lib()
+        L.m2d_iterate.argtypes = [ctypes.c_void_p, ctypes.POINTER(Report)]
+        check(L.m2d_iterate(self._ctx, ctypes.byref(rep)))
+        return rep
+
+    def run(self, itmax):
+        rep = Report()
+        L = lib()
+        L.m2d_run.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(Report)]
+        check(L.m2d_run(self._ctx, int(itmax), ctypes.byref(rep)))
+        return rep
+
+    def field(self, name):
+        n = self._size(name)
+        out = np.empty(n, dtype=np.float64)
+        L = lib()
+        L.m2d_get_field.argtypes = [ctypes.c_void_p, ctypes.c_char_p,
+                                    ctypes.POINTER(ctypes.c_double), ctypes.c_long]
+        check(L.m2d_get_field(self._ctx, name.encode(), out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), n))
+        return out
+
+    def set_field(self, name, values):
+        values = np.ascontiguousarray(values, dtype=np.float64)
+        L = lib()
+        L.m2d_set_field.argtypes = [ctypes.c_void_p, ctypes.c_char_p,
+                                    ctypes.POINTER(ctypes.c_double), ctypes.c_long]
+        check(L.m2d_set_field(self._ctx, name.encode(),
+                              values.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), values.size))
+
+    def scalar(self, name):
+        v = ctypes.c_double()
+        L = lib()
+        L.m2d_get_scalar.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_double)]
+        check(L.m2d_get_scalar(self._ctx, name.encode(), ctypes.byref(v)))
+        return v.value
+
+    def integrals(self):
+        """(fmi, fme, Fd, Cd, p_wall[nx])"""
+        vals = [ctypes.c_double() for _ in range(4)]
+        pw = np.empty(self.nx, dtype=np.float64)
+        L = lib()
+        L.m2d_integrals.argtypes = [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_double)] * 5
+        check(L.m2d_integrals(self._ctx, *[ctypes.byref(v) for v in vals],
+                              pw.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return tuple(v.value for v in vals) + (pw,)
+
+    def _size(self, name):
+        N = self.nx * self.ny
+        if name in ("au", "av", "at"):
+            return 9 * N
+        if name == "ap":
+            return 5 * N
+        if name in ("uin", "vin", "pin", "Tin", "Mw", "plin", "pina", "Tbe", "Tbw"):
+            return self.ny
+        if name in ("Tbn", "Tbs"):
+            return self.nx
+        return N

@@ -1,0 +1,113 @@
+"""Linear-solver plug-ins with the interface of src/solvers/.
+
+`solvers_init` mirrors src/solvers/mod_solvers.f90:17-87 (selection by
+"MSI" / "TDMA", unknown option is an error); each class mirrors
+class_solver_*%init / %solve (src/solvers/mod_solver_msi.f90,
+mod_solver_tdma.f90).  `solve(a, b, sol)` updates `sol` in place like the
+Fortran `intent(inout)` argument.  a is a (k, nx*ny) float64 array whose row
+k-1 is diagonal k of the reference's a(nx*ny, k).
+"""
+import numpy as np
+
+from ._lib import call
+
+
+class ClassSolverMSI9d:
+    """class_solver_msi9d (src/solvers/mod_solver_msi.f90:96-133)."""
+
+    ndiag = 9
+
+    def init(self, nx, ny, nitm, tol):
+        self.nx, self.ny, self.nitm, self.tol = int(nx), int(ny), int(nitm), float(tol)
+        self.nit = 0
+        return self
+
+    def solve(self, a, b, sol):
+        import ctypes
+        nit = ctypes.c_int(0)
+        call("m2d_msi9_solve_it" if self.ndiag == 9 else "m2d_msi5_solve_it",
+             self.nx, self.ny, self.nitm, self.tol, _mat(a, self.ndiag, self.nx * self.ny),
+             _vec(b), _vec(sol), nit)
+        self.nit = nit.value
+
+
+class ClassSolverMSI5d(ClassSolverMSI9d):
+    """class_solver_msi5d (src/solvers/mod_solver_msi.f90:56-93)."""
+
+    ndiag = 5
+
+
+class ClassSolverTDMA9d:
+    """class_solver_tdma9d (src/solvers/mod_solver_tdma.f90:76-100)."""
+
+    ndiag = 9
+
+    def init(self, nx, ny, nitm):
+        self.nx, self.ny, self.nitm = int(nx), int(ny), int(nitm)
+        return self
+
+    def solve(self, a, b, sol):
+        call("m2d_tdma9_solve" if self.ndiag == 9 else "m2d_tdma5_solve",
+             self.nx, self.ny, self.nitm, _mat(a, self.ndiag, self.nx * self.ny), _vec(b), _vec(sol))
+
+
+class ClassSolverTDMA5d(ClassSolverTDMA9d):
+    """class_solver_tdma5d (src/solvers/mod_solver_tdma.f90:48-72)."""
+
+    ndiag = 5
+
+
+def solvers_init(nx, ny, ksolver, nitm_u, nitm_p, tol_u, tol_p):
+    """Returns (solver5d, solver9d) as src/solvers/mod_solvers.f90:17-87."""
+    k = ksolver.strip()
+    if k == "MSI":
+        return (ClassSolverMSI5d().init(nx, ny, nitm_p, tol_p),
+                ClassSolverMSI9d().init(nx, ny, nitm_u, tol_u))
+    if k == "TDMA":
+        return ClassSolverTDMA5d().init(nx, ny, nitm_p), ClassSolverTDMA9d().init(nx, ny, nitm_u)
+    raise ValueError(f"solvers_init: Unkown option: {k}")
+
+
+def norm_l1_5d(nx, ny, var, b, a, norm):
+    """src/solvers/mod_solvers.f90:91-125; returns the updated norm."""
+    import ctypes
+    n = ctypes.c_double(norm)
+    call("m2d_norm_l1_5d", nx, ny, _vec(var), _vec(b), _mat(a, 5, nx * ny), n)
+    return n.value
+
+
+def norm_l1_9d(nx, ny, var, b, a, norm):
+    """src/solvers/mod_solvers.f90:128-170."""
+    import ctypes
+    n = ctypes.c_double(norm)
+    call("m2d_norm_l1_9d", nx, ny, _vec(var), _vec(b), _mat(a, 9, nx * ny), n)
+    return n.value
+
+
+def norm_l1_9d_relative(nx, ny, var, b, a, norm):
+    """src/solvers/mod_solvers.f90:176-245."""
+    import ctypes
+    n = ctypes.c_double(norm)
+    call("m2d_norm_l1_9d_relative", nx, ny, _vec(var), _vec(b), _mat(a, 9, nx * ny), n)
+    return n.value
+
+
+def tdma_lines(aw, ap, ae, d):
+    """Independent tridiagonal lines, arrays of shape (nlines, n)."""
+    nlines, n = ap.shape
+    x = np.zeros_like(ap)
+    call("m2d_tdma_lines", n, nlines, _vec(aw), _vec(ap), _vec(ae), _vec(d), x)
+    return x
+
+
+def _vec(v):
+    if not (isinstance(v, np.ndarray) and v.dtype == np.float64 and v.flags.c_contiguous):
+        raise TypeError("arrays must be C-contiguous float64")
+    return v
+
+
+def _mat(a, k, n):
+    a = _vec(a)
+    if a.size != k * n:
+        raise ValueError(f"coefficient array must hold {k} planes of {n}")
+    return a

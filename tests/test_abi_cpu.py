@@ -1,0 +1,79 @@
+"""CPU-side checks of the C ABI: the library loads without a GPU, exports
+every entry point include/mach2d_b200.h declares, rejects bad arguments
+without touching the device, and the host-side mirrors behave like the
+reference's (solver factory, deck reader)."""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import mach2d_b200
+from mach2d_b200 import _lib
+from mach2d_b200.solvers import solvers_init
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = _lib.lib()
+    names = _lib.exported_symbols()
+    assert len(names) >= 40
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+    nm = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True, text=True).stdout
+    for n in names:
+        assert f" T {n}\n" in nm + "\n", n
+
+
+def test_bad_arguments_are_rejected_before_any_device_work():
+    nx = ctypes.c_int(2)
+    ny = ctypes.c_int(5)
+    nitm = ctypes.c_int(5)
+    tol = ctypes.c_double(1e-2)
+    L = _lib.lib()
+    buf = (ctypes.c_double * 90)()
+    rc = L.m2d_msi9_solve(ctypes.byref(nx), ctypes.byref(ny), ctypes.byref(nitm), ctypes.byref(tol),
+                          buf, buf, buf)
+    assert rc == 2
+    assert b"bad arguments" in L.m2d_last_error()
+    big = ctypes.c_int(100000)
+    ok = ctypes.c_int(10)
+    rc = L.m2d_msi5_solve(ctypes.byref(ok), ctypes.byref(big), ctypes.byref(nitm), ctypes.byref(tol),
+                          buf, buf, buf)
+    assert rc in (2, 6)
+
+
+def test_msi_max_ny_fits_shared_memory():
+    assert _lib.lib().m2d_msi_max_ny() >= 1026
+
+
+def test_solvers_init_mirrors_reference_factory():
+    s5, s9 = solvers_init(10, 8, "MSI", 5, 20, 1e-2, 1e-2)
+    assert (s5.nitm, s9.nitm, s5.ndiag, s9.ndiag) == (20, 5, 5, 9)
+    s5, s9 = solvers_init(10, 8, "TDMA ", 3, 4, 0, 0)
+    assert type(s9).__name__ == "ClassSolverTDMA9d"
+    with pytest.raises(ValueError):
+        solvers_init(10, 8, "CG", 1, 1, 0, 0)
+
+
+def test_array_arguments_are_type_checked():
+    with pytest.raises(TypeError):
+        _lib.dptr(np.zeros(4, dtype=np.float32))
+    with pytest.raises(TypeError):
+        _lib.dptr(np.zeros((4, 4))[:, 1])
+
+
+def test_deck_reader_maps_a_reference_style_deck(tmp_path):
+    from mach2d_b200.ifile import case_from_decks, parse
+    deck = os.path.join(ROOT, "tests", "golden", "deck_euler_n01.txt")
+    geom = os.path.join(ROOT, "tests", "golden", "geometry_n01.txt")
+    c = case_from_decks(deck, geom)
+    assert (c.geom, c.nxr, c.nyr, c.modvis, c.solver, c.dtmodel) == (1, 20, 10, 0, 0, 1)
+    assert c.Rth == pytest.approx(2.29108e-2)
+    assert parse(deck)["sim_id"] == "n01"
+
+
+def test_package_points_at_in_tree_library():
+    assert os.path.dirname(mach2d_b200.LIB_PATH) == os.path.join(ROOT, "mach2d_b200")

@@ -1,0 +1,110 @@
+"""Known-answer tests of the CPU oracle (the checker of the GPU tests).
+
+The reference ships no tests or golden vectors and cannot be compiled here,
+so the oracle is pinned by analytic results (dense solves, isentropic
+relations, exact enthalpy conservation) and by its own committed fixtures.
+"""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+from _oracle import OracleCase, call
+from _systems import dirichlet_system, dense_from_planes, tdma_lines_system
+from mach2d_b200.simplec import euler_cosine_case, n01_case
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden", "oracle_golden.json")
+
+
+@pytest.mark.parametrize("nd", [9, 5])
+def test_msi_converges_to_dense_solution(nd):
+    nx, ny = 12, 9
+    a, b = dirichlet_system(nd, nx, ny, seed=3)
+    x = np.zeros(nx * ny)
+    nit = call(f"msi{nd}_solve", nx, ny, 400, 1e-13, a, b, x)
+    ref = np.linalg.solve(dense_from_planes(a, nd, nx, ny), b)
+    assert nit < 400
+    assert np.max(np.abs(x - ref)) <= 1e-10 * np.max(np.abs(ref))
+
+
+@pytest.mark.parametrize("nd", [9, 5])
+def test_tdma_converges_to_dense_solution(nd):
+    nx, ny = 10, 7
+    a, b = dirichlet_system(nd, nx, ny, seed=5)
+    x = np.zeros(nx * ny)
+    call(f"tdma2d{nd}", nx, ny, 200, a, b, x)
+    ref = np.linalg.solve(dense_from_planes(a, nd, nx, ny), b)
+    assert np.max(np.abs(x - ref)) <= 1e-10 * np.max(np.abs(ref))
+
+
+def test_tdma_line_matches_dense():
+    aw, ap, ae, d = tdma_lines_system(n=50, nlines=1, seed=7)
+    x = np.zeros(50)
+    call("tdma_line", 50, aw[0].copy(), ap[0].copy(), ae[0].copy(), d[0].copy(), x)
+    A = np.diag(ap[0]) + np.diag(aw[0, 1:], -1) + np.diag(ae[0, :-1], 1)
+    assert np.allclose(x, np.linalg.solve(A, d[0]), rtol=1e-12, atol=1e-12)
+
+
+def test_msi_single_iteration_reduces_residual():
+    nx, ny = 16, 11
+    a, b = dirichlet_system(9, nx, ny, seed=11)
+    x = np.zeros(nx * ny)
+    nit = call("msi9_solve", nx, ny, 1, 1e-30, a, b, x)
+    assert nit == 1
+    A = dense_from_planes(a, 9, nx, ny)
+    assert np.linalg.norm(A @ x - b) < 0.2 * np.linalg.norm(b)
+
+
+def test_isentropic_relations():
+    g, R, p0, T0 = 1.4, 287.0, 1.0e6, 1000.0
+    fm = call("get_isentropic_mass_flow", p0, T0, g, R, math.pi)
+    # choked mass flow rho* a* A*
+    Ts = T0 * 2 / (g + 1)
+    ps = p0 * (2 / (g + 1)) ** (g / (g - 1))
+    assert fm == pytest.approx(ps / (R * Ts) * math.sqrt(g * R * Ts) * math.pi, rel=1e-13)
+    for kf, ar in ((0, 2.5), (1, 2.5), (0, 1.2), (1, 3.9)):
+        M = call("get_mach_area", kf, ar, g)
+        area = (1 / M) * ((2 / (g + 1)) * (1 + (g - 1) / 2 * M * M)) ** ((g + 1) / (2 * (g - 1)))
+        assert area == pytest.approx(ar, rel=1e-10)
+        assert (M < 1) == (kf == 0)
+
+
+def test_gp_ratio_root():
+    n, r = 256, 2.1e6
+    q = call("get_gp_ratio", n, r)
+    assert abs(q ** n + r * (1 - q) - 1) < 1e-6 * r
+
+
+def test_reference_deck_converges_and_matches_fixture():
+    gold = json.load(open(GOLD))["n01_euler_20x10"]
+    o = OracleCase(n01_case())
+    hist = []
+    for _ in range(3000):
+        rc, rep = o.iterate()
+        assert rc == 0
+        if len(hist) < len(gold["history"]):
+            hist.append([rep.it, rep.dt, rep.norm, rep.normpl, rep.rmass, rep.fmi, rep.fme, rep.Fd,
+                         rep.itp_used])
+        if o.scalar("it_stop") == rep.it:
+            break
+    assert hist == gold["history"]          # the oracle is deterministic
+    fin = gold["final"]
+    assert rep.it == fin["it"] and rep.normpl < 1e-10
+    assert rep.fme / o.scalar("fm1D") == fin["Cd"]
+    assert abs(rep.fme / rep.fmi - 1.0) < 1e-10     # mass conserved at convergence
+
+
+def test_total_enthalpy_is_conserved_for_euler():
+    o = OracleCase(euler_cosine_case(20, 10))
+    for _ in range(5):
+        rc, _ = o.iterate()
+        assert rc == 0
+    u, v, T = o.field("u"), o.field("v"), o.field("T")
+    cp, H = o.scalar("Cpref"), o.scalar("Href")
+    nx, ny = o.nx, o.ny
+    interior = np.zeros((ny, nx), bool)
+    interior[1:-1, 1:-1] = True
+    h = cp * T + (u * u + v * v) / 2
+    assert np.max(np.abs(h.reshape(ny, nx)[interior] / H - 1)) < 1e-13
