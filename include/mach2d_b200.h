@@ -79,6 +79,23 @@ int m2d_msi_solve_device(int nd, int nx, int ny, int nitm, double tol, const dou
                          const double *d_b, double *d_x, double *d_work, void *stream,
                          int *d_nit);
 
+/* No counterpart in the reference.  The same device-resident solve for
+ * callers that cannot allocate device memory when they solve: a host program
+ * whose device memory is all owned by its own pool (an OpenACC or CUDA
+ * Fortran runtime, a framework's caching allocator), or a time-critical loop
+ * that must not call cudaMalloc/cudaFree because they synchronise the device.
+ * Allocates nothing: the workspace is a 12 MiB array in the library's own
+ * device memory, held on every GPU that loads the library until exit.  Limit:
+ * nx*ny <= m2d_msi_noalloc_max_cells(nd) (157286 cells for nd = 9, 196607 for
+ * nd = 5); larger grids return M2D_ERR_TOO_LARGE.  The first call on a device
+ * looks up the array's device address (cudaGetSymbolAddress), so make it
+ * before any stream capture.  All calls share the array: calls that overlap
+ * on the GPU race and must be serialised by the caller. */
+long m2d_msi_noalloc_max_cells(int nd);
+int m2d_msi_solve_device_noalloc(int nd, int nx, int ny, int nitm, double tol,
+                                 const double *d_a, const double *d_b, double *d_x,
+                                 void *stream, int *d_nit);
+
 /* class_solver_tdma9d%solve / class_solver_tdma5d%solve
  * (src/solvers/mod_solver_tdma.f90:63-100): tdma2d9 src/solvers/tdma2d9.f90:38-322,
  * tdma2d5 src/solvers/tdma2d5.f90:38-241 */
