@@ -78,6 +78,15 @@ long m2d_msi_workspace_doubles(int nd, int nx, int ny);
 int m2d_msi_solve_device(int nd, int nx, int ny, int nitm, double tol, const double *d_a,
                          const double *d_b, double *d_x, double *d_work, void *stream,
                          int *d_nit);
+/* Diagnostics: the same solve, also writing seven %globaltimer stamps (ns)
+ * to the device array d_times[7]: start, after the factorisation, after the
+ * initial residual, after the first forward sweep, the first backward sweep
+ * and the first residual, and at the end (ny <= 1024 only; otherwise the
+ * stamps are left untouched). */
+int m2d_msi_solve_device_timed(int nd, int nx, int ny, int nitm, double tol,
+                               const double *d_a, const double *d_b, double *d_x,
+                               double *d_work, void *stream, int *d_nit,
+                               unsigned long long *d_times);
 
 /* No counterpart in the reference.  The same device-resident solve for
  * callers that cannot allocate device memory when they solve: a host program

@@ -201,6 +201,30 @@ int m2d_msi_solve_device(int nd, int nx, int ny, int nitm, double tol, const dou
     return ST_OK;
 }
 
+int m2d_msi_solve_device_timed(int nd, int nx, int ny, int nitm, double tol, const double *d_a,
+                               const double *d_b, double *d_x, double *d_work, void *stream,
+                               int *d_nit, unsigned long long *d_times)
+{
+    if ((nd != 9 && nd != 5) || nx < 4 || ny < 4 || !d_a || !d_b || !d_x || !d_work || !d_times)
+        return fail(ST_ARG, "msi_solve_device_timed: bad arguments");
+    if (ny > msi_max_ny()) return fail(ST_TOO_LARGE, "msi_solve_device_timed: ny exceeds m2d_msi_max_ny()");
+    const long N = (long)nx * ny;
+    MsiLaunch L;
+    memset(&L, 0, sizeof L);
+    L.nx = nx; L.ny = ny; L.nitm = nitm; L.tol = tol;
+    MsiSys &S = L.s[0];
+    S.a = d_a; S.b = d_b; S.x = d_x;
+    S.dl = d_work;
+    S.du = d_work + (nd == 9 ? 5 : 4) * N;
+    S.wk = S.du + (nd == 9 ? 4 : 3) * N;
+    S.rr = S.wk + N;
+    S.nit = d_nit;
+    L.prof = d_times;
+    cudaError_t e = launch_msi(nd, L, 1, (cudaStream_t)stream);
+    if (e != cudaSuccess) { m2d_set_last_error(e, "msi_solve_device_timed launch", __FILE__, __LINE__); return ST_CUDA; }
+    return ST_OK;
+}
+
 static int tdma_host(int nd, const int *nx, const int *ny, const int *nitm, const double *a,
                      const double *b, double *x)
 {

@@ -263,6 +263,13 @@ __global__ void __launch_bounds__(kMaxThreads) k_msi(MsiLaunch L)
 cudaError_t launch_msi(int nd, const MsiLaunch &L, int nsys, cudaStream_t st)
 {
     if (L.ny > msi_max_ny() || L.nx < 3 || L.ny < 3) return cudaErrorInvalidValue;
+    if (msi_warp_supported(L.ny)) return launch_msi_warp(nd, L, nsys, st);
+    return launch_msi_generic(nd, L, nsys, st);
+}
+
+cudaError_t launch_msi_generic(int nd, const MsiLaunch &L, int nsys, cudaStream_t st)
+{
+    if (L.ny > msi_max_ny() || L.nx < 3 || L.ny < 3) return cudaErrorInvalidValue;
     const int T = msi_block_threads(L.ny);
     const size_t sm = msi_smem_bytes(nd, L.ny);
     if (nd == 9) {

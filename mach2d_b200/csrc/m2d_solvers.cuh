@@ -23,6 +23,9 @@ struct MsiLaunch {
     MsiSys s[2];               // up to two systems passed by value ...
     const MsiSys *dev;         // ... or an array of gridDim.x systems in device memory
     int *err;                  // device error word (ERR_* bits), may be null
+    unsigned long long *prof;  // optional phase timestamps (ns, %globaltimer), may be null:
+                               // start, after LU, after r0, first forward, first backward,
+                               // first residual, end
 };
 
 // Largest ny the one-CTA wavefront kernel accepts (its shared-memory ring
@@ -34,6 +37,11 @@ size_t msi_smem_bytes(int nd, int ny);
 // Solves gridDim.x = nsys systems, one CTA each: LU factorisation (lu2d9 /
 // lu2d5) followed by the fb2d9 / fb2d5 iteration, all inside one launch.
 cudaError_t launch_msi(int nd, const MsiLaunch &L, int nsys, cudaStream_t st);
+// the warp-synchronous kernel used by launch_msi for ny <= 1024 (m2d_msi_warp.cu)
+bool msi_warp_supported(int ny);
+cudaError_t launch_msi_warp(int nd, const MsiLaunch &L, int nsys, cudaStream_t st);
+// the one-step-per-barrier kernel, any ny <= msi_max_ny() (m2d_msi.cu)
+cudaError_t launch_msi_generic(int nd, const MsiLaunch &L, int nsys, cudaStream_t st);
 
 // tdma2d9 / tdma2d5: nitm x (x-line sweep, y-line sweep).  P, Q: N doubles each.
 cudaError_t launch_tdma(int nd, int nx, int ny, int nitm, const double *a, const double *b,
