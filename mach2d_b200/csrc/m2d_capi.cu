@@ -120,9 +120,7 @@ int msi_solve_host(int nd, const int *nx, const int *ny, const int *nitm, const 
     S.a = s.in(a, (size_t)nd * N);
     S.b = s.in(b, N);
     S.x = s.inout(x, N);
-    S.dl = s.scratch((size_t)(nd == 9 ? 5 : 4) * N);
-    S.du = s.scratch((size_t)(nd == 9 ? 4 : 3) * N);
-    S.wk = s.scratch(N);
+    S.ws = s.scratch(msi_work_doubles(nd, *nx, *ny));
     double *misc = s.scratch(4);
     if (s.status) return s.status;
     S.nit = (int *)misc;
@@ -173,9 +171,8 @@ int m2d_msi5_solve_it(const int *nx, const int *ny, const int *nitm, const doubl
 long m2d_msi_workspace_doubles(int nd, int nx, int ny)
 {
     if ((nd != 9 && nd != 5) || nx < 4 || ny < 4) return -1;
-    const long N = (long)nx * ny;
-    // dl + du + wk planes, then 4 doubles for rr and the error word
-    return (nd == 9 ? 10 : 8) * N + 4;
+    // factor and residual planes, then 4 doubles for rr and the error word
+    return (long)msi_work_doubles(nd, nx, ny) + 4;
 }
 
 int m2d_msi_solve_device(int nd, int nx, int ny, int nitm, double tol, const double *d_a,
@@ -184,16 +181,13 @@ int m2d_msi_solve_device(int nd, int nx, int ny, int nitm, double tol, const dou
     if ((nd != 9 && nd != 5) || nx < 4 || ny < 4 || !d_a || !d_b || !d_x || !d_work)
         return fail(ST_ARG, "msi_solve_device: bad arguments");
     if (ny > msi_max_ny()) return fail(ST_TOO_LARGE, "msi_solve_device: ny exceeds m2d_msi_max_ny()");
-    const long N = (long)nx * ny;
     MsiLaunch L;
     memset(&L, 0, sizeof L);
     L.nx = nx; L.ny = ny; L.nitm = nitm; L.tol = tol;
     MsiSys &S = L.s[0];
     S.a = d_a; S.b = d_b; S.x = d_x;
-    S.dl = d_work;
-    S.du = d_work + (nd == 9 ? 5 : 4) * N;
-    S.wk = S.du + (nd == 9 ? 4 : 3) * N;
-    S.rr = S.wk + N;
+    S.ws = d_work;
+    S.rr = d_work + msi_work_doubles(nd, nx, ny);
     S.nit = d_nit;
     L.err = nullptr;
     cudaError_t e = launch_msi(nd, L, 1, (cudaStream_t)stream);
@@ -208,16 +202,13 @@ int m2d_msi_solve_device_timed(int nd, int nx, int ny, int nitm, double tol, con
     if ((nd != 9 && nd != 5) || nx < 4 || ny < 4 || !d_a || !d_b || !d_x || !d_work || !d_times)
         return fail(ST_ARG, "msi_solve_device_timed: bad arguments");
     if (ny > msi_max_ny()) return fail(ST_TOO_LARGE, "msi_solve_device_timed: ny exceeds m2d_msi_max_ny()");
-    const long N = (long)nx * ny;
     MsiLaunch L;
     memset(&L, 0, sizeof L);
     L.nx = nx; L.ny = ny; L.nitm = nitm; L.tol = tol;
     MsiSys &S = L.s[0];
     S.a = d_a; S.b = d_b; S.x = d_x;
-    S.dl = d_work;
-    S.du = d_work + (nd == 9 ? 5 : 4) * N;
-    S.wk = S.du + (nd == 9 ? 4 : 3) * N;
-    S.rr = S.wk + N;
+    S.ws = d_work;
+    S.rr = d_work + msi_work_doubles(nd, nx, ny);
     S.nit = d_nit;
     L.prof = d_times;
     cudaError_t e = launch_msi(nd, L, 1, (cudaStream_t)stream);

@@ -31,7 +31,7 @@ struct m2d_ctx {
     Fields f;
     Params q;
     double *arena = nullptr;
-    double *dl9[2], *du9[2], *wk9[2], *dl5, *du5, *wk5, *P, *Q, *part;
+    double *ws9[2], *ws5, *P, *Q, *part;
     double *dsc = nullptr;
     int *dint = nullptr;
     double *hsc = nullptr;   // pinned mirror of dsc
@@ -104,7 +104,7 @@ extern "C" int m2d_create(const m2d_case *c, int device, m2d_ctx **out)
     // one arena: planes + 9N x 3 + 5N + strips + solver scratch + reductions
     const size_t nplanes = h.planes().size();
     const size_t strips = (size_t)9 * h.ny + 2 * (size_t)h.nx + 64;
-    const size_t solver = 2 * (5 + 4 + 1) * N + (4 + 3 + 1) * N + 2 * N;
+    const size_t solver = 2 * msi_work_doubles(9, h.nx, h.ny) + msi_work_doubles(5, h.nx, h.ny) + 2 * N + 3 * 32;
     const size_t total = nplanes * N + 32 * N + strips + solver + (size_t)red_parts() + 64 + S_COUNT;
     e = cudaMalloc(&x->arena, total * sizeof(double));
     if (e != cudaSuccess) { cudaStreamDestroy(x->st); delete x; m2d_set_last_error(e, "cudaMalloc", __FILE__, __LINE__); return M2D_ERR_NOMEM; }
@@ -121,8 +121,10 @@ extern "C" int m2d_create(const m2d_case *c, int device, m2d_ctx **out)
     f.uin = take(h.ny); f.vin = take(h.ny); f.pin = take(h.ny); f.Tin = take(h.ny);
     f.Mw = take(h.ny); f.plin = take(h.ny); f.pina = take(h.ny); f.Tbe = take(h.ny); f.Tbw = take(h.ny);
     f.Tbn = take(h.nx); f.Tbs = take(h.nx);
-    for (int k = 0; k < 2; k++) { x->dl9[k] = take(5 * N); x->du9[k] = take(4 * N); x->wk9[k] = take(N); }
-    x->dl5 = take(4 * N); x->du5 = take(3 * N); x->wk5 = take(N);
+    // MSI scratch starts on 256-byte boundaries (one line per warp step)
+    auto take_aligned = [&](size_t n) { cur = x->arena + (((size_t)(cur - x->arena) + 31) / 32) * 32; return take(n); };
+    for (int k = 0; k < 2; k++) x->ws9[k] = take_aligned(msi_work_doubles(9, h.nx, h.ny));
+    x->ws5 = take_aligned(msi_work_doubles(5, h.nx, h.ny));
     x->P = take(N); x->Q = take(N);
     x->part = take((size_t)red_parts() + 8);
     x->dsc = take(S_COUNT);
@@ -199,7 +201,7 @@ static int solve9(m2d_ctx *x, int nsys, double *const *a, double *const *b, doub
         L.err = x->dint + I_ERR;
         for (int k = 0; k < nsys; k++) {
             L.s[k].a = a[k]; L.s[k].b = b[k]; L.s[k].x = v[k];
-            L.s[k].dl = x->dl9[k]; L.s[k].du = x->du9[k]; L.s[k].wk = x->wk9[k];
+            L.s[k].ws = x->ws9[k];
             L.s[k].nit = x->dint + islot[k]; L.s[k].rr = x->dsc + rslot[k];
         }
         KL(launch_msi(9, L, nsys, x->st), 1);
@@ -219,7 +221,7 @@ static int solve5(m2d_ctx *x)
         L.nx = x->nx; L.ny = x->ny; L.nitm = c.nitm_p; L.tol = c.tol_p;
         L.err = x->dint + I_ERR;
         L.s[0].a = x->f.ap; L.s[0].b = x->f.bp; L.s[0].x = x->f.pl;
-        L.s[0].dl = x->dl5; L.s[0].du = x->du5; L.s[0].wk = x->wk5;
+        L.s[0].ws = x->ws5;
         L.s[0].nit = x->dint + I_NIT_P; L.s[0].rr = x->dsc + S_RR + 4;
         KL(launch_msi(5, L, 1, x->st), 1);
     } else {

@@ -39,6 +39,17 @@ size_t msi_smem_bytes(int nd, int ny)
     int nu = (nd == 9) ? 4 : 3;
     return (size_t)kRingSlots * nu * ny * sizeof(double) + (size_t)msi_block_threads(ny) * sizeof(double);
 }
+size_t msi_skew_plane(int nx, int ny)
+{
+    return (size_t)((ny + 31) / 32) * (size_t)(nx + 62) * 32;
+}
+size_t msi_work_doubles(int nd, int nx, int ny)
+{
+    const size_t N = (size_t)nx * ny;
+    const size_t generic = (size_t)(nd == 9 ? 10 : 8) * N;            // dl, du, residual
+    const size_t skew = (size_t)(nd == 9 ? 12 : 10) * msi_skew_plane(nx, ny);   // + 1/dl1, correction
+    return generic > skew ? generic : skew;
+}
 int msi_max_ny()
 {
     // 227 KB of opt-in shared memory per CTA on sm_100
@@ -120,9 +131,10 @@ __global__ void __launch_bounds__(kMaxThreads) k_msi(MsiLaunch L)
     double *ring = smem;
     double *red = smem + (size_t)kRingSlots * NU * ny;
     const double *__restrict__ a = S.a;
-    double *__restrict__ dl = S.dl;
-    double *__restrict__ du = S.du;
-    double *wk = S.wk;
+    // plain plane-major scratch: dl planes, du planes, one residual plane
+    double *__restrict__ dl = S.ws;
+    double *__restrict__ du = S.ws + (ND == 9 ? 5 : 4) * N;
+    double *wk = du + NU * N;
     double *x = S.x;
     bool bad_pivot = false;
 

@@ -13,20 +13,27 @@
 //     the producer sits in another CTA).  Hand-offs are point to point: after
 //     each batch the producer publishes a release counter, the consumer waits
 //     for it with an acquire load, and the consumer's own counter tells the
-//     producer which ring slots are free again.  No warp waits for anything
-//     but its two neighbours, and every wait is bounded (on timeout the
-//     kernel records ERR_WAIT_TIMEOUT and runs to its end);
-//   * coefficients are prefetched D steps ahead into a rotating register
-//     buffer, so the loads never sit on the recurrence;
-//   * divisions use the divisor's correctly rounded reciprocal and two FMA
-//     correction steps (Markstein's method): the correctly rounded quotient,
-//     i.e. exactly the result of IEEE division;
-//   * the residual passes and the L2 norm of the stopping test use all
-//     threads of all CTAs of the cluster; partial sums are combined in a fixed
-//     order in CTA 0 and broadcast, so the stopping decision is deterministic.
+//     producer which ring slots are free again.  Every wait is bounded (on
+//     timeout the kernel records ERR_WAIT_TIMEOUT and runs to its end);
+//   * the factors, the residual and the sweep results live in
+//     "wavefront-major" planes: the 32 cells a warp touches in one step are
+//     one contiguous 256-byte line, so one batch of one plane is a single
+//     4 KB block.  The sweeps stage those blocks into shared memory with bulk
+//     asynchronous copies (TMA, completion on an mbarrier) several batches
+//     ahead, so no global-memory latency sits on the recurrence;
+//   * divisions on the recurrence use the divisor's correctly rounded
+//     reciprocal and two FMA corrections (Markstein's method), which yields
+//     the IEEE quotient whenever both operands lie in [2^-500, 2^500] (or the
+//     dividend is zero).  A batch in which any cell falls outside that range
+//     is recomputed with IEEE division before it is published;
+//   * the backward sweep writes the correction z; x += z and the residual
+//     r = A x - b run as cluster-wide passes over all threads, as does the
+//     L2 norm of the stopping test (partial sums combined in a fixed order in
+//     CTA 0 and broadcast, so the stopping decision is deterministic).
 // A cell outside the grid (before its row starts, after it ends, rows >= ny)
 // produces zeros, which is exactly the zero-neighbour rule of the general
 // formula, so results stay bitwise equal to the lexicographic reference loop.
+#include <cstdint>
 #include <cooperative_groups.h>
 #include "m2d_solvers.cuh"
 
@@ -40,36 +47,40 @@ constexpr int kRing = 128;        // ring slots; a producer may lead its consume
 constexpr int kLead = (kRing - 2 * kLag) / kLag - 1;
 constexpr int kThreads = 256;     // threads per CTA (wavefront warps + helpers)
 constexpr int kMaxCluster = 16;
+constexpr int kSkewPad = 62;      // slots per warp = nx + 62 (slot s = i + 2 lane)
+constexpr int kLine = 32;         // doubles per slot line, one per lane
+constexpr int kBlock = kLag * kLine;   // doubles of one plane for one batch (4 KB)
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kMaxIterUnbounded = 10000;
 constexpr long long kSpinLimit = 1LL << 24;
+constexpr long long kBarSpinLimit = 1LL << 22;
 }
 
 #define PL(p, k, np) (p)[(long long)((k) - 1) * N + (np)]
 
 // a / b from y = RN(1/b): q0 = a y, then two corrections q += (a - q b) y
-// with exact FMA remainders.  For |b| in [2^-900, 2^900] and |a| < 2^900,
-// a = 0 or |a| > 2^-900, the result is the correctly rounded quotient
-// (Markstein, IBM J. Res. Dev. 34, 1990), i.e. the IEEE quotient; for a = 0
-// the first product a y already is that quotient.  recip_ok tells when it applies,
-// and callers fall back to div_ieee outside that range.
+// with exact FMA remainders (Markstein, IBM J. Res. Dev. 34, 1990).  With
+// |a|, |b| in [2^-500, 2^500] no intermediate leaves the normal range and the
+// result is the correctly rounded quotient; for a = 0 the first product a y
+// already is the IEEE quotient.  range_ok tells when these conditions hold.
 __device__ __forceinline__ double div_recip(double a, double b, double y)
 {
     const double q0 = a * y;
     const double r0 = fma(-q0, b, a);
     const double q1 = fma(r0, y, q0);
     const double r1 = fma(-q1, b, a);
-    return (a == 0.0) ? q0 : fma(r1, y, q1);   // a zero quotient keeps the IEEE sign
+    return (a == 0.0) ? q0 : fma(r1, y, q1);
 }
-__device__ __forceinline__ bool recip_ok(double a, double b)
+__device__ __forceinline__ bool range_ok(double a, double b)
 {
     const double fa = fabs(a), fb = fabs(b);
-    return fb > 0x1p-900 && fb < 0x1p+900 && fa < 0x1p+900 && (fa > 0x1p-900 || fa == 0.0);
+    return fb >= 0x1p-500 && fb <= 0x1p+500 && (fa == 0.0 || (fa >= 0x1p-500 && fa <= 0x1p+500));
 }
-__device__ __noinline__ double div_ieee(double a, double b) { return a / b; }
-__device__ __forceinline__ double qdiv(double a, double b)
+// n / d on the fast path: the IEEE quotient unless bad is raised
+__device__ __forceinline__ double div_fast(double n, double d, bool &bad)
 {
-    return recip_ok(a, b) ? div_recip(a, b, __drcp_rn(b)) : div_ieee(a, b);
+    bad = bad || !range_ok(n, d);
+    return div_recip(n, d, __drcp_rn(d));
 }
 
 __device__ __forceinline__ void stamp(const MsiLaunch &L, int rank, int k)
@@ -92,7 +103,8 @@ __device__ __forceinline__ int ld_acquire(const int *p)
     asm volatile("ld.acquire.cluster.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
-// one lane waits until *p >= target (bounded); the warp then proceeds together
+// one lane waits until *p >= target (bounded; after a timeout it no longer
+// waits at all); the warp then proceeds together
 __device__ __forceinline__ void warp_wait(const int *p, int target, int lane_waiting, bool &timed_out)
 {
     if ((threadIdx.x & 31) == lane_waiting && !timed_out) {
@@ -104,12 +116,113 @@ __device__ __forceinline__ void warp_wait(const int *p, int target, int lane_wai
     __syncwarp();
 }
 
+// ---- bulk asynchronous copies into shared memory, completion on an mbarrier
+__device__ __forceinline__ unsigned smem_u32(const void *p)
+{
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_tx(unsigned long long *bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, unsigned long long *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+// 32-bit shared::cluster address of the same variable in CTA `rank`
+__device__ __forceinline__ unsigned cluster_addr(const void *p, int rank)
+{
+    unsigned r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_u32(p)), "r"(rank));
+    return r;
+}
+__device__ __forceinline__ void st_cluster(unsigned addr, double v)
+{
+    asm volatile("st.shared::cluster.f64 [%0], %1;" ::"r"(addr), "d"(v));
+}
+// generic-proxy global writes become visible to later bulk copies
+__device__ __forceinline__ void fence_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_shared() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// Per wavefront warp: NSTAGE staging blocks of NP planes x kLag lines, one
+// mbarrier each.  issued/consumed count staged batches over all phases, so
+// block = count % NSTAGE and the mbarrier parity = (count / NSTAGE) & 1.
+template <int NSTAGE, int PMAX>
+struct Stager {
+    double *mem;                 // the CTA's staging memory
+    int base;                    // this warp's area in it (doubles)
+    unsigned long long *bar;
+    int issued, consumed;
+    __device__ int block(int q) const { return base + q * PMAX * kBlock; }
+};
+
+// stage slot lines [s_lo, s_lo + kLag) of NP wavefront-major planes (lines
+// outside [0, sw) are not copied: every cell on them is invalid)
+template <int NP, int NSTAGE, int PMAX>
+__device__ __forceinline__ void stage_issue(Stager<NSTAGE, PMAX> &st, double *const *planes,
+                                            long long line0, int s_lo, int sw)
+{
+    const int q = st.issued % NSTAGE;
+    if ((threadIdx.x & 31) == 0) {
+        fence_async_shared();   // earlier reads of this block precede the copies into it
+        const int lo = max(s_lo, 0), hi = min(s_lo + kLag, sw);
+        const unsigned bytes = hi > lo ? (unsigned)(hi - lo) * kLine * 8u : 0u;
+        mbar_arrive_tx(&st.bar[q], bytes * NP);
+        if (bytes) {
+            double *dst = st.mem + st.block(q) + (lo - s_lo) * kLine;
+#pragma unroll
+            for (int p = 0; p < NP; p++)
+                bulk_g2s(dst + p * kBlock, planes[p] + (line0 + lo) * kLine, bytes, &st.bar[q]);
+        }
+    }
+    st.issued++;
+}
+// waits for the next staged batch; returns its block's offset in st.mem
+template <int NSTAGE, int PMAX>
+__device__ __forceinline__ int stage_wait(Stager<NSTAGE, PMAX> &st, bool &timed_out)
+{
+    const int q = st.consumed % NSTAGE;
+    const unsigned parity = (unsigned)(st.consumed / NSTAGE) & 1u;
+    long long k = 0;
+    while (!mbar_try_wait(&st.bar[q], parity)) {
+        if (++k > kBarSpinLimit) { timed_out = true; break; }
+    }
+    __syncwarp();
+    st.consumed++;
+    return st.block(q);
+}
+
+// wavefront-major slot of cell (i, j): warp j/32, step offset i + 2 (j%32), lane j%32
+__device__ __forceinline__ long long skew_slot(int i, int j, int sw)
+{
+    return ((long long)(j >> 5) * sw + i + 2 * (j & 31)) * kLine + (j & 31);
+}
+
 // r = A x - b for one cell, in-range neighbours in ascending diagonal order
 template <int ND>
 __device__ __forceinline__ double residual_cell(const double *__restrict__ a, const double *__restrict__ b,
-                                                const double *x, long long np, int nx, int ny, long long N)
+                                                const double *x, long long np, int i, int j, int nx, int ny,
+                                                long long N)
 {
-    const int i = (int)(np % nx), j = (int)(np / nx);
     const bool w = i > 0, e = i < nx - 1, s = j > 0, n = j < ny - 1;
     double v = -b[np];
     if (ND == 9) {
@@ -132,25 +245,37 @@ __device__ __forceinline__ double residual_cell(const double *__restrict__ a, co
     return v;
 }
 
-// r = A x - b over the cluster (this CTA takes a contiguous slice of cells),
-// returns the cluster-wide sum of r^2, identical in every thread.  Starts with
-// a cluster barrier: x of every row must be final.
+// Cluster-wide pass (this CTA takes a contiguous slice of cells): first
+// x += z when z (wavefront-major) is given, then r = A x - b stored
+// wavefront-major.  Returns the cluster-wide sum of r^2, identical in every
+// thread.  Starts with a cluster barrier: every row's sweep must be final.
 template <int ND>
 __device__ double cluster_residual(cg::cluster_group &cl, const double *__restrict__ a,
-                                   const double *__restrict__ b, const double *x, double *r,
-                                   int nx, int ny, double *red, double *part)
+                                   const double *__restrict__ b, double *x, const double *z, double *r,
+                                   int nx, int ny, int sw, double *red, double *part)
 {
     cl.sync();
     const long long N = (long long)nx * ny;
     const int C = (int)cl.num_blocks(), rank = (int)cl.block_rank();
     const long long per = (N + C - 1) / C;
     const long long lo = per * rank, hi = (lo + per < N) ? lo + per : N;
+    if (z) {
+#pragma unroll 4
+        for (long long np = lo + threadIdx.x; np < hi; np += kThreads) {
+            const int j = (int)(np / nx), i = (int)(np - (long long)j * nx);
+            x[np] = z[skew_slot(i, j, sw)] + x[np];
+        }
+        cl.sync();
+    }
     double acc = 0.0;
+#pragma unroll 2
     for (long long np = lo + threadIdx.x; np < hi; np += kThreads) {
-        const double v = residual_cell<ND>(a, b, x, np, nx, ny, N);
-        r[np] = v;
+        const int j = (int)(np / nx), i = (int)(np - (long long)j * nx);
+        const double v = residual_cell<ND>(a, b, x, np, i, j, nx, ny, N);
+        r[skew_slot(i, j, sw)] = v;
         acc = acc + v * v;
     }
+    fence_async_global();   // the forward sweep reads r with bulk copies
     red[threadIdx.x] = acc;
     __syncthreads();
     for (int s = kThreads / 2; s > 0; s >>= 1) {
@@ -171,19 +296,77 @@ __device__ double cluster_residual(cg::cluster_group &cl, const double *__restri
     return part[kMaxCluster];
 }
 
-template <int ND, int WPC, int DLU, int DSW>
+// One factorisation step of one cell (lu2d9 / lu2d5).  cb is the row of A
+// (a unit row for an invalid cell), mw the own row's previous u, a1/a2/a3
+// the row below's u at SE/S/SW.  FAST divides with div_fast and raises bad
+// when that may differ from IEEE division; otherwise it divides with '/'.
+template <int ND, bool FAST>
+__device__ __forceinline__ void lu_cell(const double (&cb)[ND], double alpha, const double *mw,
+                                        const double *a1, const double *a2, const double *a3, double *l,
+                                        double *u, bool &bad)
+{
+    auto dv = [&](double n, double d) -> double { return FAST ? div_fast(n, d, bad) : n / d; };
+    if (ND == 9) {
+        const double b1 = cb[0], b2 = cb[1], b3 = cb[2], b4 = cb[3], b5 = cb[4];
+        const double b6 = cb[5], b7 = cb[6], b8 = cb[7], b9 = cb[8];
+        double l5 = b1;
+        double l4 = dv(b2 - l5 * a3[0] - alpha * b3 * a1[0], 1.0 - alpha * a2[0] * a1[0]);
+        double l3 = b3 - l4 * a2[0];
+        double l2 = dv(b4 - l4 * a2[1] - l5 * a3[2] - 2.0 * alpha * l5 * a3[1], 1 + 2.0 * alpha * mw[1]);
+        double phi1 = l3 * a1[0], phi2 = l5 * a3[1], phi3 = l3 * a1[3], phi4 = l2 * mw[1];
+        double l1 = b5 - l2 * mw[0] - l3 * a1[1] - l4 * a2[2] - l5 * a3[3]
+                  + alpha * (2.0 * phi1 + phi2 + phi3 + 2.0 * phi4);
+        const double n0 = b6 - l3 * a1[2] - l4 * a2[3] - 2.0 * alpha * (phi1 + phi3);
+        const double n1 = b7 - l2 * mw[2];
+        const double n2 = b8 - l2 * mw[3] - alpha * phi4;
+        if (FAST) {
+            const double y = __drcp_rn(l1);
+            bad = bad || !range_ok(n0, l1) || !range_ok(n1, l1) || !range_ok(n2, l1) || !range_ok(b9, l1);
+            u[0] = div_recip(n0, l1, y); u[1] = div_recip(n1, l1, y);
+            u[2] = div_recip(n2, l1, y); u[3] = div_recip(b9, l1, y);
+        } else {
+            u[0] = n0 / l1; u[1] = n1 / l1; u[2] = n2 / l1; u[3] = b9 / l1;
+        }
+        l[0] = l1; l[1] = l2; l[2] = l3; l[3] = l4; l[4] = l5;
+    } else {
+        const double b1 = cb[0], b2 = cb[1], b3 = cb[2], b4 = cb[3], b5 = cb[4];
+        double l4 = dv(b1, 1.0 - alpha * a2[0] * a1[0]);
+        double l3 = -l4 * a2[0];
+        double l2 = dv(b2 - l4 * a2[1], 1.0 + 2.0 * alpha * mw[1]);
+        double phi1 = l3 * a1[0], phi4 = l2 * mw[1];
+        double l1 = b3 - l2 * mw[0] - l3 * a1[1] - l4 * a2[2] + 2.0 * alpha * (phi1 + phi4);
+        const double n0 = b4 - l3 * a1[2] - 2.0 * alpha * phi1;
+        const double n1 = -l2 * mw[2];
+        const double n2 = b5 - alpha * phi4;
+        if (FAST) {
+            const double y = __drcp_rn(l1);
+            bad = bad || !range_ok(n0, l1) || !range_ok(n1, l1) || !range_ok(n2, l1);
+            u[0] = div_recip(n0, l1, y); u[1] = div_recip(n1, l1, y); u[2] = div_recip(n2, l1, y);
+        } else {
+            u[0] = n0 / l1; u[1] = n1 / l1; u[2] = n2 / l1;
+        }
+        l[0] = l1; l[1] = l2; l[2] = l3; l[3] = l4;
+    }
+}
+
+template <int ND, int WPC, int NSTAGE, int DLU>
 __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
 {
     constexpr int NU = (ND == 9) ? 4 : 3;
     constexpr int NL = (ND == 9) ? 5 : 4;
-    static_assert(kLag % DLU == 0 && kLag % DSW == 0, "prefetch distance must divide kLag");
+    constexpr int PMAX = NL + 2;                  // planes staged per batch (forward sweep)
+    constexpr int DIAG = (ND == 9) ? 4 : 2;      // index of the main diagonal in a row of A
+    static_assert(kLag % DLU == 0, "prefetch distance must divide kLag");
     // per wavefront warp of this CTA: incoming rings and counters
     __shared__ double ring_up[WPC][kRing][NU];   // from the warp below (LU, forward)
     __shared__ double ring_dn[WPC][kRing];       // from the warp above (backward)
     __shared__ int up_ready[WPC], dn_ready[WPC]; // batches delivered to this warp
     __shared__ int up_done[WPC], dn_done[WPC];   // batches of this warp's output consumed
+    __shared__ double lu_save[WPC][4 * NU][32];  // factorisation state at batch start
+    __shared__ unsigned long long stage_bar[WPC][NSTAGE];
     __shared__ double red[kThreads];
     __shared__ double part[kMaxCluster + 1];
+    extern __shared__ __align__(128) double stage_mem[];   // WPC x NSTAGE x PMAX x kBlock
     cg::cluster_group cl = cg::this_cluster();
     const int C = (int)cl.num_blocks(), rank = (int)cl.block_rank();
     const int sys = blockIdx.x / C;
@@ -198,37 +381,58 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
     const bool row_ok = front && j < ny;
     const int nsteps = ((nx + 2 * (ny - 1) + kLag * (NWG - 1) + kLag - 1) / kLag) * kLag;
     const int nbatch = nsteps / kLag;
+    const int SW = nx + kSkewPad;                 // slots per warp
+    const long long PS = (long long)((ny + 31) / 32) * SW * kLine;   // one wavefront-major plane
+    const int soff = (64 + kLag) * wg;            // step at which this warp's slot 0 comes up
     const double *__restrict__ a = S.a;
-    double *__restrict__ dl = S.dl;
-    double *__restrict__ du = S.du;
-    double *wk = S.wk;
     double *x = S.x;
     const long long rowbase = (long long)j * nx;
+    // wavefront-major planes: dl1..dlNL, du1..duNU, 1/dl1, residual, sweep result
+    double *dlp = S.ws;
+    double *dup = dlp + NL * PS;
+    double *rl1 = dup + NU * PS;
+    double *rp = rl1 + PS;
+    double *wp = rp + PS;
+    // a wavefront warp past the last row group (possible when WPC > 1) owns no
+    // slots: it reads group 0 (values unused, all its cells are invalid) and
+    // stores nothing
+    const bool has_rows = front && wg * 32 < ny;
+    const long long line0 = (long long)(has_rows ? wg : 0) * SW;
+    const long long wbase = line0 * kLine + lane;
+#define SK(p, s) (p)[wbase + (long long)(s) * kLine]
 
     if (threadIdx.x < WPC) {
         up_ready[threadIdx.x] = 0; dn_ready[threadIdx.x] = 0;
         up_done[threadIdx.x] = 0; dn_done[threadIdx.x] = 0;
+        for (int q = 0; q < NSTAGE; q++) mbar_init(&stage_bar[threadIdx.x][q], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    Stager<NSTAGE, PMAX> st;
+    st.mem = stage_mem;
+    st.base = (front ? wl : 0) * NSTAGE * PMAX * kBlock;
+    st.bar = &stage_bar[front ? wl : 0][0];
+    st.issued = 0;
+    st.consumed = 0;
     // links of this warp: up channel (LU, forward) feeds warp g+1, down channel
     // (backward) feeds warp g-1; the partner may sit in a neighbouring CTA
     const bool has_below = front && wg > 0, has_above = front && wg < NWG - 1;
-    double *up_ring_dst = nullptr, *dn_ring_dst = nullptr;
+    unsigned up_ring_dst = 0, dn_ring_dst = 0;   // shared::cluster addresses
     int *up_ready_dst = nullptr, *dn_ready_dst = nullptr, *up_done_dst = nullptr, *dn_done_dst = nullptr;
     if (front) {
         if (has_above) {
             const int cw = (wl + 1 < WPC) ? wl + 1 : 0, cr = (wl + 1 < WPC) ? rank : rank + 1;
-            up_ring_dst = cl.map_shared_rank(&ring_up[cw][0][0], cr);
+            up_ring_dst = cluster_addr(&ring_up[cw][0][0], cr);
             up_ready_dst = cl.map_shared_rank(&up_ready[cw], cr);
             dn_done_dst = cl.map_shared_rank(&dn_done[cw], cr);
         }
         if (has_below) {
             const int pw = (wl > 0) ? wl - 1 : WPC - 1, pr = (wl > 0) ? rank : rank - 1;
-            dn_ring_dst = cl.map_shared_rank(&ring_dn[pw][0], pr);
+            dn_ring_dst = cluster_addr(&ring_dn[pw][0], pr);
             dn_ready_dst = cl.map_shared_rank(&dn_ready[pw], pr);
             up_done_dst = cl.map_shared_rank(&up_done[pw], pr);
         }
     }
-    cl.sync();   // counters initialised before any remote access
+    cl.sync();   // counters and mbarriers initialised before any use
     bool bad_pivot = false, timed_out = false;
     int up_base = 0, dn_base = 0;       // batches already run on each channel
     stamp(L, rank, 0);
@@ -240,7 +444,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
         for (int q = 0; q < NU; q++) { mw[q] = 0.0; a1[q] = 0.0; a2[q] = 0.0; a3[q] = 0.0; }
 #pragma unroll
         for (int d = 0; d < DLU; d++) {
-            const int ic = d - 2 * j - kLag * wg;           // cell of step d
+            const int ic = d - soff - 2 * lane;             // cell of step d
 #pragma unroll
             for (int k = 0; k < ND; k++)
                 buf[d][k] = (row_ok && ic >= 0 && ic < nx) ? PL(a, k + 1, rowbase + ic) : 0.0;
@@ -250,13 +454,20 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
             if (has_below) warp_wait(&up_ready[wl], up_base + b, 0, timed_out);
             if (has_above && b > kLead) warp_wait(&up_done[wl], up_base + b - kLead, 31, timed_out);
 #pragma unroll
+            for (int q = 0; q < NU; q++) {
+                lu_save[wl][q][lane] = mw[q]; lu_save[wl][NU + q][lane] = a1[q];
+                lu_save[wl][2 * NU + q][lane] = a2[q]; lu_save[wl][3 * NU + q][lane] = a3[q];
+            }
+            bool bad = false;
+#pragma unroll
             for (int kk = 0; kk < kLag; kk++) {
                 const int tau = tb + kk;
-                const int i = tau - 2 * j - kLag * wg;
+                const int s = tau - soff;
+                const int i = s - 2 * lane;
                 const bool valid = row_ok && i >= 0 && i < nx;
                 double cb[ND];
 #pragma unroll
-                for (int k = 0; k < ND; k++) cb[k] = buf[kk % DLU][k];
+                for (int k = 0; k < ND; k++) cb[k] = valid ? buf[kk % DLU][k] : (k == DIAG ? 1.0 : 0.0);
                 if (row_ok && i + DLU >= 0 && i + DLU < nx) {
 #pragma unroll
                     for (int k = 0; k < ND; k++) buf[kk % DLU][k] = PL(a, k + 1, rowbase + i + DLU);
@@ -269,77 +480,91 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                     if (lane == 0) v = (has_below && src >= 0) ? ring_up[wl][rs][q] : 0.0;
                     a3[q] = a2[q]; a2[q] = a1[q]; a1[q] = v;
                 }
-                double u[NU];
+                // an invalid cell sees a unit row: all its divisions are by 1 and
+                // its outputs are replaced by zeros below
+                const double alpha = (valid && i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2) ? 0.5 : 0.0;
+                double l[NL], u[NU];
+                bool bc = false;
+                lu_cell<ND, true>(cb, alpha, mw, a1, a2, a3, l, u, bc);
+                bad = bad || (valid && bc);
+                if (valid && (!(fabs(l[0]) > 0.0) || !isfinite(l[0]))) bad_pivot = true;
 #pragma unroll
-                for (int q = 0; q < NU; q++) u[q] = 0.0;
-                if (valid) {
-                    const long long np = rowbase + i;
-                    const double alpha = (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2) ? 0.5 : 0.0;
-                    // neighbours: W = own previous cell, SE = a1, S = a2, SW = a3
-                    if (ND == 9) {
-                        const double b1 = cb[0], b2 = cb[1], b3 = cb[2], b4 = cb[3], b5 = cb[4];
-                        const double b6 = cb[5], b7 = cb[6], b8 = cb[7], b9 = cb[8];
-                        double l5 = b1;
-                        double l4 = qdiv(b2 - l5 * a3[0] - alpha * b3 * a1[0], 1.0 - alpha * a2[0] * a1[0]);
-                        double l3 = b3 - l4 * a2[0];
-                        double l2 = qdiv(b4 - l4 * a2[1] - l5 * a3[2] - 2.0 * alpha * l5 * a3[1], 1 + 2.0 * alpha * mw[1]);
-                        double phi1 = l3 * a1[0], phi2 = l5 * a3[1], phi3 = l3 * a1[3], phi4 = l2 * mw[1];
-                        double l1 = b5 - l2 * mw[0] - l3 * a1[1] - l4 * a2[2] - l5 * a3[3]
-                                  + alpha * (2.0 * phi1 + phi2 + phi3 + 2.0 * phi4);
-                        const double n0 = b6 - l3 * a1[2] - l4 * a2[3] - 2.0 * alpha * (phi1 + phi3);
-                        const double n1 = b7 - l2 * mw[2];
-                        const double n2 = b8 - l2 * mw[3] - alpha * phi4;
-                        const double n3 = b9;
-                        if (recip_ok(n0, l1) && recip_ok(n1, l1) && recip_ok(n2, l1) && recip_ok(n3, l1)) {
-                            const double y = __drcp_rn(l1);
-                            u[0] = div_recip(n0, l1, y); u[1] = div_recip(n1, l1, y);
-                            u[2] = div_recip(n2, l1, y); u[3] = div_recip(n3, l1, y);
-                        } else {
-                            u[0] = div_ieee(n0, l1); u[1] = div_ieee(n1, l1);
-                            u[2] = div_ieee(n2, l1); u[3] = div_ieee(n3, l1);
-                        }
-                        if (!(fabs(l1) > 0.0) || !isfinite(l1)) bad_pivot = true;
-                        PL(dl, 1, np) = l1; PL(dl, 2, np) = l2; PL(dl, 3, np) = l3; PL(dl, 4, np) = l4; PL(dl, 5, np) = l5;
-                    } else {
-                        const double b1 = cb[0], b2 = cb[1], b3 = cb[2], b4 = cb[3], b5 = cb[4];
-                        double l4 = qdiv(b1, 1.0 - alpha * a2[0] * a1[0]);
-                        double l3 = -l4 * a2[0];
-                        double l2 = qdiv(b2 - l4 * a2[1], 1.0 + 2.0 * alpha * mw[1]);
-                        double phi1 = l3 * a1[0], phi4 = l2 * mw[1];
-                        double l1 = b3 - l2 * mw[0] - l3 * a1[1] - l4 * a2[2] + 2.0 * alpha * (phi1 + phi4);
-                        const double n0 = b4 - l3 * a1[2] - 2.0 * alpha * phi1;
-                        const double n1 = -l2 * mw[2];
-                        const double n2 = b5 - alpha * phi4;
-                        if (recip_ok(n0, l1) && recip_ok(n1, l1) && recip_ok(n2, l1)) {
-                            const double y = __drcp_rn(l1);
-                            u[0] = div_recip(n0, l1, y); u[1] = div_recip(n1, l1, y); u[2] = div_recip(n2, l1, y);
-                        } else {
-                            u[0] = div_ieee(n0, l1); u[1] = div_ieee(n1, l1); u[2] = div_ieee(n2, l1);
-                        }
-                        if (!(fabs(l1) > 0.0) || !isfinite(l1)) bad_pivot = true;
-                        PL(dl, 1, np) = l1; PL(dl, 2, np) = l2; PL(dl, 3, np) = l3; PL(dl, 4, np) = l4;
-                    }
+                for (int q = 0; q < NU; q++) u[q] = valid ? u[q] : 0.0;
+                if (has_rows && s >= 0 && s < SW) {
+                    const double y = __drcp_rn(l[0]);   // forward sweep's reciprocal pivot
 #pragma unroll
-                    for (int q = 0; q < NU; q++) PL(du, q + 1, np) = u[q];
+                    for (int k = 0; k < NL; k++) SK(dlp + k * PS, s) = valid ? l[k] : 0.0;
+#pragma unroll
+                    for (int q = 0; q < NU; q++) SK(dup + q * PS, s) = u[q];
+                    SK(rl1, s) = valid ? y : 0.0;
                 }
 #pragma unroll
                 for (int q = 0; q < NU; q++) mw[q] = u[q];
                 if (lane == 31 && has_above) {
                     const int ws = (int)(((unsigned)up_base * kLag + (unsigned)tau) & (kRing - 1));
 #pragma unroll
-                    for (int q = 0; q < NU; q++) up_ring_dst[ws * NU + q] = u[q];
+                    for (int q = 0; q < NU; q++) st_cluster(up_ring_dst + (unsigned)(ws * NU + q) * 8u, u[q]);
+                }
+            }
+            if (__any_sync(kFull, bad)) {
+                // some quotient of this batch may differ from IEEE division:
+                // recompute the batch from its start state with IEEE division
+#pragma unroll
+                for (int q = 0; q < NU; q++) {
+                    mw[q] = lu_save[wl][q][lane]; a1[q] = lu_save[wl][NU + q][lane];
+                    a2[q] = lu_save[wl][2 * NU + q][lane]; a3[q] = lu_save[wl][3 * NU + q][lane];
+                }
+                for (int kk = 0; kk < kLag; kk++) {
+                    const int tau = tb + kk;
+                    const int s = tau - soff;
+                    const int i = s - 2 * lane;
+                    const bool valid = row_ok && i >= 0 && i < nx;
+                    double cb[ND];
+#pragma unroll
+                    for (int k = 0; k < ND; k++) cb[k] = valid ? PL(a, k + 1, rowbase + i) : (k == DIAG ? 1.0 : 0.0);
+                    const int src = tau - 1 - kLag;
+                    const int rs = (int)(((unsigned)up_base * kLag + (unsigned)src) & (kRing - 1));
+#pragma unroll
+                    for (int q = 0; q < NU; q++) {
+                        double v = __shfl_up_sync(kFull, mw[q], 1);
+                        if (lane == 0) v = (has_below && src >= 0) ? ring_up[wl][rs][q] : 0.0;
+                        a3[q] = a2[q]; a2[q] = a1[q]; a1[q] = v;
+                    }
+                    const double alpha = (valid && i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2) ? 0.5 : 0.0;
+                    double l[NL], u[NU];
+                    bool unused = false;
+                    lu_cell<ND, false>(cb, alpha, mw, a1, a2, a3, l, u, unused);
+                    if (valid && (!(fabs(l[0]) > 0.0) || !isfinite(l[0]))) bad_pivot = true;
+#pragma unroll
+                    for (int q = 0; q < NU; q++) u[q] = valid ? u[q] : 0.0;
+                    if (has_rows && s >= 0 && s < SW) {
+                        const double y = __drcp_rn(l[0]);
+#pragma unroll
+                        for (int k = 0; k < NL; k++) SK(dlp + k * PS, s) = valid ? l[k] : 0.0;
+#pragma unroll
+                        for (int q = 0; q < NU; q++) SK(dup + q * PS, s) = u[q];
+                        SK(rl1, s) = valid ? y : 0.0;
+                    }
+#pragma unroll
+                    for (int q = 0; q < NU; q++) mw[q] = u[q];
+                    if (lane == 31 && has_above) {
+                        const int ws = (int)(((unsigned)up_base * kLag + (unsigned)tau) & (kRing - 1));
+#pragma unroll
+                        for (int q = 0; q < NU; q++) st_cluster(up_ring_dst + (unsigned)(ws * NU + q) * 8u, u[q]);
+                    }
                 }
             }
             if (lane == 31 && has_above) st_release(up_ready_dst, up_base + b + 1);
             if (lane == 0 && has_below) st_release(up_done_dst, up_base + b + 1);
         }
+        fence_async_global();   // the sweeps read the factors with bulk copies
     }
     up_base += nbatch;
     if (bad_pivot && L.err) atomicOr(L.err, ERR_NONFINITE_PIVOT);
     stamp(L, rank, 1);
 
     // ---- fb2d9 / fb2d5 (msi2d9-v03.f90:42-262, msi2d5-v03.f90:42-233)
-    const double rr0 = cluster_residual<ND>(cl, a, S.b, x, wk, nx, ny, red, part);
+    const double rr0 = cluster_residual<ND>(cl, a, S.b, x, nullptr, rp, nx, ny, SW, red, part);
     stamp(L, rank, 2);
     const double gammarp = L.tol * sqrt(rr0);
     const int cap = (L.nitm > 0) ? L.nitm : kMaxIterUnbounded;
@@ -347,108 +572,154 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
     double rr = rr0;
     for (;;) {
         nit = nit + 1;
-        // forward: L w = -r, w overwrites r in wk.  buf[d] = {r, dl1..dlNL}
+        // forward: L w = -r.  Staged planes {r, dl1..dlNL, 1/dl1}; step kk of
+        // a batch is line kk of its block
         if (front) {
-            double mine = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0, buf[DSW][NL + 1];
+            double *fp[NL + 2];
+            fp[0] = rp;
 #pragma unroll
-            for (int d = 0; d < DSW; d++) {
-                const int ic = d - 2 * j - kLag * wg;
-                const bool ok = row_ok && ic >= 0 && ic < nx;
-                buf[d][0] = ok ? wk[rowbase + ic] : 0.0;
-#pragma unroll
-                for (int k = 0; k < NL; k++) buf[d][k + 1] = ok ? PL(dl, k + 1, rowbase + ic) : 1.0;
-            }
-            double ycur = __drcp_rn(buf[0][1]);
+            for (int k = 0; k < NL; k++) fp[k + 1] = dlp + k * PS;
+            fp[NL + 1] = rl1;
+            for (int t = 0; t < NSTAGE - 1 && t < nbatch; t++) stage_issue<NL + 2>(st, fp, line0, t * kLag - soff, SW);
+            double mine = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
             for (int b = 0; b < nbatch; b++) {
                 const int tb = b * kLag;
                 if (has_below) warp_wait(&up_ready[wl], up_base + b, 0, timed_out);
                 if (has_above && b > kLead) warp_wait(&up_done[wl], up_base + b - kLead, 31, timed_out);
+                const int bo = stage_wait(st, timed_out) + lane;
+                if (b + NSTAGE - 1 < nbatch) stage_issue<NL + 2>(st, fp, line0, (b + NSTAGE - 1) * kLag - soff, SW);
+                const double m0 = mine, b1 = a1, b2 = a2, b3 = a3;   // state at batch start
+                const unsigned rbase = (unsigned)up_base * kLag;       // ring position of step 0
+                const unsigned wbase_ring = up_ring_dst + ((rbase + (unsigned)tb) & (kRing - 1)) * (NU * 8u);
+                bool bad = false;
+                // c: staged coefficients of the current step, rv: ring value
+                // (lane 0's south-east neighbour); both loaded one step ahead
+                double c[NL + 2], rv;
+#pragma unroll
+                for (int k = 0; k < NL + 2; k++) c[k] = stage_mem[bo + k * kBlock];
+                rv = ring_up[wl][(rbase + (unsigned)(tb - 1 - kLag)) & (kRing - 1)][0];
 #pragma unroll
                 for (int kk = 0; kk < kLag; kk++) {
                     const int tau = tb + kk;
-                    const int i = tau - 2 * j - kLag * wg;
+                    const int s = tau - soff;
+                    const int i = s - 2 * lane;
                     const bool valid = row_ok && i >= 0 && i < nx;
-                    double c[NL + 1];
+                    double cn[NL + 2], rvn = 0.0;
+                    if (kk + 1 < kLag) {
 #pragma unroll
-                    for (int k = 0; k <= NL; k++) c[k] = buf[kk % DSW][k];
-                    const double y = ycur;
-                    ycur = __drcp_rn(buf[(kk + 1) % DSW][1]);   // next cell's pivot, off the recurrence
-                    if (row_ok && i + DSW >= 0 && i + DSW < nx) {
-                        buf[kk % DSW][0] = wk[rowbase + i + DSW];
-#pragma unroll
-                        for (int k = 0; k < NL; k++) buf[kk % DSW][k + 1] = PL(dl, k + 1, rowbase + i + DSW);
+                        for (int k = 0; k < NL + 2; k++) cn[k] = stage_mem[bo + k * kBlock + (kk + 1) * kLine];
+                        rvn = ring_up[wl][(rbase + (unsigned)(tau - kLag)) & (kRing - 1)][0];
                     }
                     const int src = tau - 1 - kLag;
                     double v = __shfl_up_sync(kFull, mine, 1);
-                    if (lane == 0)
-                        v = (has_below && src >= 0) ? ring_up[wl][((unsigned)up_base * kLag + (unsigned)src) & (kRing - 1)][0] : 0.0;
+                    if (lane == 0) v = (has_below && src >= 0) ? rv : 0.0;
                     a3 = a2; a2 = a1; a1 = v;
-                    double wv = 0.0;
-                    if (valid) {
-                        // w = -(r + dl2 w_W + dl3 w_SE + dl4 w_S [+ dl5 w_SW]) / dl1
-                        double num;
-                        if (ND == 9) num = c[0] + c[2] * mine + c[3] * a1 + c[4] * a2 + c[5] * a3;
-                        else num = c[0] + c[2] * mine + c[3] * a1 + c[4] * a2;
-                        wv = recip_ok(num, c[1]) ? -div_recip(num, c[1], y) : -div_ieee(num, c[1]);
-                        wk[rowbase + i] = wv;
-                    }
+                    // w = -(r + dl2 w_W + dl3 w_SE + dl4 w_S [+ dl5 w_SW]) / dl1
+                    double num;
+                    if (ND == 9) num = c[0] + c[2] * mine + c[3] * a1 + c[4] * a2 + c[5] * a3;
+                    else num = c[0] + c[2] * mine + c[3] * a1 + c[4] * a2;
+                    const double q = div_recip(num, c[1], c[NL + 1]);
+                    bad = bad || (valid && !range_ok(num, c[1]));
+                    const double wv = valid ? -q : 0.0;
+                    if (has_rows && s >= 0 && s < SW) SK(wp, s) = wv;
                     mine = wv;
-                    if (lane == 31 && has_above)
-                        up_ring_dst[(((unsigned)up_base * kLag + (unsigned)tau) & (kRing - 1)) * NU] = wv;
+                    if (lane == 31 && has_above) st_cluster(wbase_ring + (unsigned)kk * (NU * 8u), wv);
+                    if (kk + 1 < kLag) {
+#pragma unroll
+                        for (int k = 0; k < NL + 2; k++) c[k] = cn[k];
+                        rv = rvn;
+                    }
+                }
+                if (__any_sync(kFull, bad)) {
+                    // some quotient of this batch may differ from IEEE division:
+                    // recompute the batch from its start state with IEEE division
+                    mine = m0; a1 = b1; a2 = b2; a3 = b3;
+                    for (int kk = 0; kk < kLag; kk++) {
+                        const int tau = tb + kk;
+                        const int s = tau - soff;
+                        const int i = s - 2 * lane;
+                        const bool valid = row_ok && i >= 0 && i < nx;
+                        double cs[NL + 1];
+#pragma unroll
+                        for (int k = 0; k < NL + 1; k++) cs[k] = stage_mem[bo + k * kBlock + kk * kLine];
+                        const int src = tau - 1 - kLag;
+                        double v = __shfl_up_sync(kFull, mine, 1);
+                        if (lane == 0)
+                            v = (has_below && src >= 0) ? ring_up[wl][(rbase + (unsigned)src) & (kRing - 1)][0] : 0.0;
+                        a3 = a2; a2 = a1; a1 = v;
+                        double num;
+                        if (ND == 9) num = cs[0] + cs[2] * mine + cs[3] * a1 + cs[4] * a2 + cs[5] * a3;
+                        else num = cs[0] + cs[2] * mine + cs[3] * a1 + cs[4] * a2;
+                        const double wv = valid ? -(num / cs[1]) : 0.0;
+                        if (has_rows && s >= 0 && s < SW) SK(wp, s) = wv;
+                        mine = wv;
+                        if (lane == 31 && has_above)
+                            st_cluster(up_ring_dst + ((rbase + (unsigned)tau) & (kRing - 1)) * (NU * 8u), wv);
+                    }
                 }
                 if (lane == 31 && has_above) st_release(up_ready_dst, up_base + b + 1);
                 if (lane == 0 && has_below) st_release(up_done_dst, up_base + b + 1);
             }
+            fence_async_global();   // the backward sweep reads w with bulk copies
+            __syncwarp();
         }
         up_base += nbatch;
         if (nit == 1) stamp(L, rank, 3);
-        // backward: U z = w, var = z + var; time runs from the top-right
-        // corner.  buf[d] = {w, x, du1..duNU}
+        // backward: U z = w; time runs from the top-right corner, so step tau
+        // is slot Tmax - tau - soff and step kk of a batch is line kLag-1-kk of
+        // its block.  Staged planes {w, du1..duNU}
         if (front) {
-            double mine = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0, buf[DSW][NU + 2];
-            const int wrev = NWG - 1 - wg;
+            const int Tmax = (nx - 1) + 2 * (ny - 1) + kLag * (NWG - 1);
+            double *bp[NU + 1];
+            bp[0] = wp;
 #pragma unroll
-            for (int d = 0; d < DSW; d++) {
-                const int ic = nx - 1 - (d - 2 * (ny - 1 - j) - kLag * wrev);
-                const bool ok = row_ok && ic >= 0 && ic < nx;
-                buf[d][0] = ok ? wk[rowbase + ic] : 0.0;
-                buf[d][1] = ok ? x[rowbase + ic] : 0.0;
-#pragma unroll
-                for (int k = 0; k < NU; k++) buf[d][k + 2] = ok ? PL(du, k + 1, rowbase + ic) : 0.0;
-            }
+            for (int k = 0; k < NU; k++) bp[k + 1] = dup + k * PS;
+            for (int t = 0; t < NSTAGE - 1 && t < nbatch; t++)
+                stage_issue<NU + 1>(st, bp, line0, Tmax - (t * kLag + kLag - 1) - soff, SW);
+            double mine = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
             for (int b = 0; b < nbatch; b++) {
                 const int tb = b * kLag;
                 if (has_above) warp_wait(&dn_ready[wl], dn_base + b, 31, timed_out);
                 if (has_below && b > kLead) warp_wait(&dn_done[wl], dn_base + b - kLead, 0, timed_out);
+                const int bo = stage_wait(st, timed_out) + lane;
+                if (b + NSTAGE - 1 < nbatch)
+                    stage_issue<NU + 1>(st, bp, line0, Tmax - ((b + NSTAGE - 1) * kLag + kLag - 1) - soff, SW);
+                const unsigned rbase = (unsigned)dn_base * kLag;
+                // c: staged {w, du} of the current step, rv: ring value (lane
+                // 31's north-west neighbour); both loaded one step ahead
+                double c[NU + 1], rv;
+#pragma unroll
+                for (int k = 0; k < NU + 1; k++) c[k] = stage_mem[bo + k * kBlock + (kLag - 1) * kLine];
+                rv = ring_dn[wl][(rbase + (unsigned)(tb - 1 - kLag)) & (kRing - 1)];
 #pragma unroll
                 for (int kk = 0; kk < kLag; kk++) {
                     const int tau = tb + kk;
-                    const int i = nx - 1 - (tau - 2 * (ny - 1 - j) - kLag * wrev);
+                    const int s = Tmax - tau - soff;
+                    const int i = s - 2 * lane;
                     const bool valid = row_ok && i >= 0 && i < nx;
-                    double c[NU + 2];
+                    double cn[NU + 1], rvn = 0.0;
+                    if (kk + 1 < kLag) {
 #pragma unroll
-                    for (int k = 0; k < NU + 2; k++) c[k] = buf[kk % DSW][k];
-                    if (row_ok && i - DSW >= 0 && i - DSW < nx) {
-                        buf[kk % DSW][0] = wk[rowbase + i - DSW];
-                        buf[kk % DSW][1] = x[rowbase + i - DSW];
-#pragma unroll
-                        for (int k = 0; k < NU; k++) buf[kk % DSW][k + 2] = PL(du, k + 1, rowbase + i - DSW);
+                        for (int k = 0; k < NU + 1; k++) cn[k] = stage_mem[bo + k * kBlock + (kLag - 2 - kk) * kLine];
+                        rvn = ring_dn[wl][(rbase + (unsigned)(tau - kLag)) & (kRing - 1)];
                     }
                     const int src = tau - 1 - kLag;
                     double v = __shfl_down_sync(kFull, mine, 1);
-                    if (lane == 31)
-                        v = (has_above && src >= 0) ? ring_dn[wl][((unsigned)dn_base * kLag + (unsigned)src) & (kRing - 1)] : 0.0;
+                    if (lane == 31) v = (has_above && src >= 0) ? rv : 0.0;
                     a3 = a2; a2 = a1; a1 = v;
-                    double z = 0.0;
-                    if (valid) {
-                        // z = w - du1 z_E - du2 z_NW - du3 z_N [- du4 z_NE]; E = own previous
-                        if (ND == 9) z = c[0] - c[2] * mine - c[3] * a1 - c[4] * a2 - c[5] * a3;
-                        else z = c[0] - c[2] * mine - c[3] * a1 - c[4] * a2;
-                        x[rowbase + i] = z + c[1];
-                    }
+                    // z = w - du1 z_E - du2 z_NW - du3 z_N [- du4 z_NE]; E = own previous
+                    double z;
+                    if (ND == 9) z = c[0] - c[1] * mine - c[2] * a1 - c[3] * a2 - c[4] * a3;
+                    else z = c[0] - c[1] * mine - c[2] * a1 - c[3] * a2;
+                    z = valid ? z : 0.0;
+                    if (has_rows && s >= 0 && s < SW) SK(wp, s) = z;
                     mine = z;
-                    if (lane == 0 && has_below)
-                        dn_ring_dst[((unsigned)dn_base * kLag + (unsigned)tau) & (kRing - 1)] = z;
+                    if (lane == 0 && has_below) st_cluster(dn_ring_dst + ((rbase + (unsigned)tau) & (kRing - 1)) * 8u, z);
+                    if (kk + 1 < kLag) {
+#pragma unroll
+                        for (int k = 0; k < NU + 1; k++) c[k] = cn[k];
+                        rv = rvn;
+                    }
                 }
                 if (lane == 0 && has_below) st_release(dn_ready_dst, dn_base + b + 1);
                 if (lane == 31 && has_above) st_release(dn_done_dst, dn_base + b + 1);
@@ -456,13 +727,20 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
         }
         dn_base += nbatch;
         if (nit == 1) stamp(L, rank, 4);
-        rr = cluster_residual<ND>(cl, a, S.b, x, wk, nx, ny, red, part);
+        // var = z + var, then the new residual
+        rr = cluster_residual<ND>(cl, a, S.b, x, wp, rp, nx, ny, SW, red, part);
         if (nit == 1) stamp(L, rank, 5);
         if (sqrt(rr) < gammarp) break;
         if (nit == cap) {
             if (L.nitm <= 0 && L.err && rank == 0 && threadIdx.x == 0) atomicOr(L.err, ERR_WAIT_TIMEOUT);
             break;
         }
+    }
+#undef SK
+    if (front && st.consumed < st.issued) {
+        // only after a timed-out wait: let the copies still in flight land
+        // before this CTA's shared memory goes away (bounded)
+        while (st.consumed < st.issued) (void)stage_wait(st, timed_out);
     }
     if (timed_out && L.err) atomicOr(L.err, ERR_WAIT_TIMEOUT);
     if (rank == 0 && threadIdx.x == 0) {
@@ -475,22 +753,30 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
 
 bool msi_warp_supported(int ny) { return ny <= 1024; }
 
+template <int ND, int WPC, int NSTAGE>
+static size_t stage_bytes()
+{
+    return (size_t)WPC * NSTAGE * ((ND == 9 ? 5 : 4) + 2) * kBlock * sizeof(double);
+}
+
 // launches one cluster per system if the cluster shape can be scheduled;
 // *fits = false (and nothing launched) otherwise
-template <int ND, int WPC, int DLU, int DSW>
+template <int ND, int WPC, int NSTAGE>
 static cudaError_t launch_cluster(const MsiLaunch &L, int nsys, cudaStream_t st, bool *fits)
 {
     *fits = false;
     const int nwarps = (L.ny + 31) / 32;
     const int C = (nwarps + WPC - 1) / WPC;
     if (C > kMaxCluster) return cudaSuccess;
-    auto kern = k_msi_c<ND, WPC, DLU, DSW>;
+    auto kern = k_msi_c<ND, WPC, NSTAGE, (ND == 9 ? 2 : 4)>;
+    const size_t smem = stage_bytes<ND, WPC, NSTAGE>();
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(C * nsys));
     cfg.blockDim = dim3(kThreads);
-    cfg.dynamicSmemBytes = 0;
+    cfg.dynamicSmemBytes = smem;
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -512,14 +798,18 @@ static cudaError_t launch_cluster(const MsiLaunch &L, int nsys, cudaStream_t st,
 template <int ND>
 static cudaError_t launch_nd(const MsiLaunch &L, int nsys, cudaStream_t st)
 {
-    // fewest wavefront warps per CTA (one SM per warp) whose cluster fits
-    bool fits = false;
-    cudaError_t e = launch_cluster<ND, 1, (ND == 9 ? 2 : 4), 4>(L, nsys, st, &fits);
-    if (e != cudaSuccess || fits) return e;
-    e = launch_cluster<ND, 2, (ND == 9 ? 2 : 4), 4>(L, nsys, st, &fits);
-    if (e != cudaSuccess || fits) return e;
-    e = launch_cluster<ND, 4, (ND == 9 ? 2 : 4), 4>(L, nsys, st, &fits);
-    if (e != cudaSuccess || fits) return e;
+    // the bulk copies need 16-byte aligned scratch; systems given through a
+    // device array cannot be checked here
+    bool aligned = L.dev == nullptr;
+    for (int k = 0; k < nsys && aligned; k++) aligned = ((uintptr_t)L.s[k].ws % 16) == 0;
+    if (aligned) {
+        // fewest wavefront warps per CTA (one SM per warp) whose cluster fits
+        bool fits = false;
+        cudaError_t e = launch_cluster<ND, 1, 4>(L, nsys, st, &fits);
+        if (e != cudaSuccess || fits) return e;
+        e = launch_cluster<ND, 2, 3>(L, nsys, st, &fits);
+        if (e != cudaSuccess || fits) return e;
+    }
     return launch_msi_generic(ND, L, nsys, st);
 }
 

@@ -5,17 +5,25 @@
 
 namespace m2d {
 
-// One linear system A x = b.  A is plane-major (ND planes of N doubles),
-// dl/du are the incomplete factors (5+4 planes for ND=9, 4+3 for ND=5), wk
-// is one plane of scratch (residual, then L^-1 r in place).
+// One linear system A x = b.  A is plane-major (ND planes of N doubles).
+// ws is msi_work_doubles(ND, nx, ny) doubles of scratch holding the
+// incomplete factors (5+4 planes for ND=9, 4+3 for ND=5) and the residual;
+// its layout belongs to the kernel that runs.
 struct MsiSys {
     const double *a;
     const double *b;
     double *x;
-    double *dl, *du, *wk;
+    double *ws;
     int *nit;          // iterations performed (device int)
     double *rr;        // [0] = |r0|^2, [1] = |r_final|^2 (device doubles)
 };
+
+// scratch doubles one system needs (the larger of the two kernels' layouts)
+size_t msi_work_doubles(int nd, int nx, int ny);
+// the cluster kernel's factor planes are "wavefront-major": slot
+// ((j/32) * (nx + 62) + i + 2 (j%32)) * 32 + j%32 holds cell (i, j), so the
+// 32 rows a warp sweeps read and write one contiguous 256-byte line per step
+size_t msi_skew_plane(int nx, int ny);
 
 struct MsiLaunch {
     int nx, ny, nitm;
