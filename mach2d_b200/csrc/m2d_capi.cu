@@ -175,24 +175,36 @@ long m2d_msi_workspace_doubles(int nd, int nx, int ny)
     return (long)msi_work_doubles(nd, nx, ny) + 4;
 }
 
-int m2d_msi_solve_device(int nd, int nx, int ny, int nitm, double tol, const double *d_a,
-                         const double *d_b, double *d_x, double *d_work, void *stream, int *d_nit)
+// one device-resident solve on caller scratch of work_doubles doubles (the
+// factor planes, then rr in the last 4 doubles); the caller has checked that
+// work_doubles covers at least the plain-layout kernel
+int m2d_msi_solve_device_ws(int nd, int nx, int ny, int nitm, double tol, const double *d_a,
+                            const double *d_b, double *d_x, double *d_work, long work_doubles,
+                            void *stream, int *d_nit, unsigned long long *d_times)
 {
-    if ((nd != 9 && nd != 5) || nx < 4 || ny < 4 || !d_a || !d_b || !d_x || !d_work)
-        return fail(ST_ARG, "msi_solve_device: bad arguments");
-    if (ny > msi_max_ny()) return fail(ST_TOO_LARGE, "msi_solve_device: ny exceeds m2d_msi_max_ny()");
     MsiLaunch L;
     memset(&L, 0, sizeof L);
     L.nx = nx; L.ny = ny; L.nitm = nitm; L.tol = tol;
     MsiSys &S = L.s[0];
     S.a = d_a; S.b = d_b; S.x = d_x;
     S.ws = d_work;
-    S.rr = d_work + msi_work_doubles(nd, nx, ny);
+    S.rr = d_work + (work_doubles - 4);
     S.nit = d_nit;
-    L.err = nullptr;
+    L.ws_cap = (size_t)(work_doubles - 4);
+    L.prof = d_times;
     cudaError_t e = launch_msi(nd, L, 1, (cudaStream_t)stream);
     if (e != cudaSuccess) { m2d_set_last_error(e, "msi_solve_device launch", __FILE__, __LINE__); return ST_CUDA; }
     return ST_OK;
+}
+
+int m2d_msi_solve_device(int nd, int nx, int ny, int nitm, double tol, const double *d_a,
+                         const double *d_b, double *d_x, double *d_work, void *stream, int *d_nit)
+{
+    if ((nd != 9 && nd != 5) || nx < 4 || ny < 4 || !d_a || !d_b || !d_x || !d_work)
+        return fail(ST_ARG, "msi_solve_device: bad arguments");
+    if (ny > msi_max_ny()) return fail(ST_TOO_LARGE, "msi_solve_device: ny exceeds m2d_msi_max_ny()");
+    return m2d_msi_solve_device_ws(nd, nx, ny, nitm, tol, d_a, d_b, d_x, d_work,
+                                   m2d_msi_workspace_doubles(nd, nx, ny), stream, d_nit, nullptr);
 }
 
 int m2d_msi_solve_device_timed(int nd, int nx, int ny, int nitm, double tol, const double *d_a,
@@ -202,18 +214,8 @@ int m2d_msi_solve_device_timed(int nd, int nx, int ny, int nitm, double tol, con
     if ((nd != 9 && nd != 5) || nx < 4 || ny < 4 || !d_a || !d_b || !d_x || !d_work || !d_times)
         return fail(ST_ARG, "msi_solve_device_timed: bad arguments");
     if (ny > msi_max_ny()) return fail(ST_TOO_LARGE, "msi_solve_device_timed: ny exceeds m2d_msi_max_ny()");
-    MsiLaunch L;
-    memset(&L, 0, sizeof L);
-    L.nx = nx; L.ny = ny; L.nitm = nitm; L.tol = tol;
-    MsiSys &S = L.s[0];
-    S.a = d_a; S.b = d_b; S.x = d_x;
-    S.ws = d_work;
-    S.rr = d_work + msi_work_doubles(nd, nx, ny);
-    S.nit = d_nit;
-    L.prof = d_times;
-    cudaError_t e = launch_msi(nd, L, 1, (cudaStream_t)stream);
-    if (e != cudaSuccess) { m2d_set_last_error(e, "msi_solve_device_timed launch", __FILE__, __LINE__); return ST_CUDA; }
-    return ST_OK;
+    return m2d_msi_solve_device_ws(nd, nx, ny, nitm, tol, d_a, d_b, d_x, d_work,
+                                   m2d_msi_workspace_doubles(nd, nx, ny), stream, d_nit, d_times);
 }
 
 static int tdma_host(int nd, const int *nx, const int *ny, const int *nitm, const double *a,

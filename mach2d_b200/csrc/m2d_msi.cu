@@ -43,12 +43,19 @@ size_t msi_skew_plane(int nx, int ny)
 {
     return (size_t)((ny + 31) / 32) * (size_t)(nx + 62) * 32;
 }
+size_t msi_generic_work_doubles(int nd, int nx, int ny)
+{
+    return (size_t)(nd == 9 ? 10 : 8) * (size_t)nx * ny;                 // dl, du, residual
+}
+size_t msi_cluster_work_doubles(int nd, int nx, int ny)
+{
+    // dl, du, 1/dl1, residual, correction and A, wavefront-major
+    return (size_t)(nd == 9 ? 21 : 15) * msi_skew_plane(nx, ny);
+}
 size_t msi_work_doubles(int nd, int nx, int ny)
 {
-    const size_t N = (size_t)nx * ny;
-    const size_t generic = (size_t)(nd == 9 ? 10 : 8) * N;            // dl, du, residual
-    const size_t skew = (size_t)(nd == 9 ? 12 : 10) * msi_skew_plane(nx, ny);   // + 1/dl1, correction
-    return generic > skew ? generic : skew;
+    const size_t g = msi_generic_work_doubles(nd, nx, ny), c = msi_cluster_work_doubles(nd, nx, ny);
+    return g > c ? g : c;
 }
 int msi_max_ny()
 {

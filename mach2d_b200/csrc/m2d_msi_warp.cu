@@ -8,19 +8,21 @@
 //     the backward sweep); the own-row neighbour stays in registers;
 //   * global warp g runs kLag steps behind the plain t = i + 2j schedule of
 //     warp g-1, so the value its lane 0 needs from lane 31 of warp g-1 was
-//     produced in an earlier batch of kLag steps.  It travels through a ring
-//     in the consumer's shared memory (a distributed-shared-memory store when
-//     the producer sits in another CTA).  Hand-offs are point to point: after
-//     each batch the producer publishes a release counter, the consumer waits
-//     for it with an acquire load, and the consumer's own counter tells the
-//     producer which ring slots are free again.  Every wait is bounded (on
-//     timeout the kernel records ERR_WAIT_TIMEOUT and runs to its end);
-//   * the factors, the residual and the sweep results live in
-//     "wavefront-major" planes: the 32 cells a warp touches in one step are
-//     one contiguous 256-byte line, so one batch of one plane is a single
-//     4 KB block.  The sweeps stage those blocks into shared memory with bulk
-//     asynchronous copies (TMA, completion on an mbarrier) several batches
-//     ahead, so no global-memory latency sits on the recurrence;
+//     produced in an earlier batch of kLag steps.  Each batch of such values
+//     travels as one bulk shared-to-shared copy into a ring in the consumer's
+//     shared memory (distributed shared memory when the producer sits in
+//     another CTA), completing on an mbarrier the consumer waits on; the
+//     consumer frees ring slots by arriving on the producer's mbarriers.  No
+//     warp waits for anything but its two neighbours, and every wait is
+//     bounded (on timeout the kernel records ERR_WAIT_TIMEOUT and runs to its
+//     end);
+//   * A (after a transposing pre-pass, k_skew_a), the factors, the residual
+//     and the sweep results live in "wavefront-major" planes: the 32 cells a
+//     warp touches in one step are one contiguous 256-byte line, so one batch
+//     of one plane is a single 4 KB block.  The factorisation and the sweeps
+//     stage those blocks into shared memory with bulk asynchronous copies
+//     (TMA, completion on an mbarrier) several batches ahead, so no
+//     global-memory latency sits on the recurrence;
 //   * divisions on the recurrence use the divisor's correctly rounded
 //     reciprocal and two FMA corrections (Markstein's method), which yields
 //     the IEEE quotient whenever both operands lie in [2^-500, 2^500] (or the
@@ -44,15 +46,14 @@ namespace m2d {
 namespace {
 constexpr int kLag = 16;          // steps per batch = per-warp time lag
 constexpr int kRing = 128;        // ring slots; a producer may lead its consumer by 5 batches
-constexpr int kLead = (kRing - 2 * kLag) / kLag - 1;
 constexpr int kThreads = 256;     // threads per CTA (wavefront warps + helpers)
 constexpr int kMaxCluster = 16;
 constexpr int kSkewPad = 62;      // slots per warp = nx + 62 (slot s = i + 2 lane)
 constexpr int kLine = 32;         // doubles per slot line, one per lane
 constexpr int kBlock = kLag * kLine;   // doubles of one plane for one batch (4 KB)
+constexpr int kSlots = kRing / kLag;    // ring slots, one batch each
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kMaxIterUnbounded = 10000;
-constexpr long long kSpinLimit = 1LL << 24;
 constexpr long long kBarSpinLimit = 1LL << 22;
 }
 
@@ -90,30 +91,6 @@ __device__ __forceinline__ void stamp(const MsiLaunch &L, int rank, int k)
         asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
         L.prof[k] = t;
     }
-}
-
-// cluster-scope release store / acquire load on a (possibly remote) counter
-__device__ __forceinline__ void st_release(int *p, int v)
-{
-    asm volatile("st.release.cluster.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-__device__ __forceinline__ int ld_acquire(const int *p)
-{
-    int v;
-    asm volatile("ld.acquire.cluster.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-// one lane waits until *p >= target (bounded; after a timeout it no longer
-// waits at all); the warp then proceeds together
-__device__ __forceinline__ void warp_wait(const int *p, int target, int lane_waiting, bool &timed_out)
-{
-    if ((threadIdx.x & 31) == lane_waiting && !timed_out) {
-        long long k = 0;
-        while (ld_acquire(p) < target) {
-            if (++k > kSpinLimit) { timed_out = true; break; }
-        }
-    }
-    __syncwarp();
 }
 
 // ---- bulk asynchronous copies into shared memory, completion on an mbarrier
@@ -158,6 +135,28 @@ __device__ __forceinline__ unsigned cluster_addr(const void *p, int rank)
 __device__ __forceinline__ void st_cluster(unsigned addr, double v)
 {
     asm volatile("st.shared::cluster.f64 [%0], %1;" ::"r"(addr), "d"(v));
+}
+// all lanes: bounded wait for the completion of phase `parity` (after an
+// earlier timeout the warp no longer waits at all)
+__device__ __forceinline__ void mbar_wait(unsigned long long *bar, unsigned parity, bool &timed_out)
+{
+    if (!timed_out) {
+        long long k = 0;
+        while (!mbar_try_wait(bar, parity)) {
+            if (++k > kBarSpinLimit) { timed_out = true; break; }
+        }
+    }
+    __syncwarp();
+}
+__device__ __forceinline__ void bulk_s2s(unsigned dst, const void *src, unsigned bytes, unsigned bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.shared::cta.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(dst), "r"(smem_u32(src)), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_remote_arrive(unsigned bar)
+{
+    asm volatile("mbarrier.arrive.shared::cluster.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 // generic-proxy global writes become visible to later bulk copies
 __device__ __forceinline__ void fence_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
@@ -209,6 +208,39 @@ __device__ __forceinline__ int stage_wait(Stager<NSTAGE, PMAX> &st, bool &timed_
     __syncwarp();
     st.consumed++;
     return st.block(q);
+}
+
+// ---- warp-to-warp hand-off (one channel = one direction between two warps)
+// The producer stages the values of its batch n (its lane 31 for the warp
+// above, lane 0 for the warp below) in slot n % kSlots of a local buffer and
+// ships the slot with one bulk shared-to-shared copy into the same slot of the
+// consumer's ring; the copy completes on the consumer's "full" barrier of that
+// slot.  The consumer frees the slot by arriving on the producer's "empty"
+// barrier.  Batch numbers n count over all phases of a channel, so the k-th
+// use of a slot is phase k of its barriers.
+__device__ __forceinline__ void chan_recv(unsigned long long *full, int n, unsigned bytes, bool &timed_out)
+{
+    unsigned long long *bar = &full[n & (kSlots - 1)];
+    if ((threadIdx.x & 31) == 0) mbar_arrive_tx(bar, bytes);
+    __syncwarp();
+    mbar_wait(bar, (unsigned)(n / kSlots) & 1u, timed_out);
+}
+// producer, before staging batch n: the consumer has released batch n - kSlots
+__device__ __forceinline__ void chan_slot_free(unsigned long long *empty, int n, bool &timed_out)
+{
+    if (n >= kSlots) mbar_wait(&empty[n & (kSlots - 1)], (unsigned)(n / kSlots - 1) & 1u, timed_out);
+}
+// producer lane that staged the values: ship batch n (vals doubles)
+__device__ __forceinline__ void chan_send(unsigned ring_dst, unsigned full_dst, const double *out, int n, int vals)
+{
+    const int slot = n & (kSlots - 1);
+    fence_async_shared();   // the staged values become visible to the bulk copy
+    bulk_s2s(ring_dst + (unsigned)(slot * vals) * 8u, out + slot * vals, (unsigned)vals * 8u,
+             full_dst + (unsigned)slot * 8u);
+}
+__device__ __forceinline__ void chan_release(unsigned empty_dst, int n)
+{
+    mbar_remote_arrive(empty_dst + (unsigned)(n & (kSlots - 1)) * 8u);
 }
 
 // wavefront-major slot of cell (i, j): warp j/32, step offset i + 2 (j%32), lane j%32
@@ -349,21 +381,57 @@ __device__ __forceinline__ void lu_cell(const double (&cb)[ND], double alpha, co
     }
 }
 
-template <int ND, int WPC, int NSTAGE, int DLU>
+// A (plane-major, cell order) -> wavefront-major planes for the factorisation's
+// bulk copies: line (w, s) lane l holds cell (s - 2 l, 32 w + l).  A CTA
+// transposes a tile of 32 rows x (kSkewTile + 62) cells through shared memory
+// into kSkewTile lines; cells outside the grid become zeros.
+constexpr int kSkewTile = 64;
+template <int ND>
+__global__ void __launch_bounds__(256) k_skew_a(MsiLaunch L)
+{
+    __shared__ double tile[32][kSkewTile + kSkewPad + 1];
+    const MsiSys S = L.s[blockIdx.z];
+    const int nx = L.nx, ny = L.ny;
+    const long long N = (long long)nx * ny;
+    const int NL = (ND == 9) ? 5 : 4, NU = (ND == 9) ? 4 : 3;
+    const int SW = nx + kSkewPad;
+    const long long PS = (long long)((ny + 31) / 32) * SW * kLine;
+    double *as = S.ws + (long long)(NL + NU + 3) * PS;
+    const int w = blockIdx.y, c0 = blockIdx.x * kSkewTile;
+    constexpr int TW = kSkewTile + kSkewPad;
+    for (int k = 0; k < ND; k++) {
+        for (int idx = threadIdx.x; idx < 32 * TW; idx += blockDim.x) {
+            const int r = idx / TW, c = idx - r * TW;
+            const int i = c0 - kSkewPad + c, j = 32 * w + r;
+            tile[r][c] = (j < ny && i >= 0 && i < nx) ? PL(S.a, k + 1, (long long)j * nx + i) : 0.0;
+        }
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < kSkewTile * 32; idx += blockDim.x) {
+            const int t = idx >> 5, l = idx & 31, s = c0 + t;
+            if (s < SW) as[(long long)k * PS + ((long long)w * SW + s) * kLine + l] = tile[l][t + kSkewPad - 2 * l];
+        }
+        __syncthreads();
+    }
+}
+
+template <int ND, int WPC, int NSTAGE>
 __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
 {
     constexpr int NU = (ND == 9) ? 4 : 3;
     constexpr int NL = (ND == 9) ? 5 : 4;
-    constexpr int PMAX = NL + 2;                  // planes staged per batch (forward sweep)
+    constexpr int PMAX = (ND > NL + 2) ? ND : NL + 2;   // planes staged per batch
     constexpr int DIAG = (ND == 9) ? 4 : 2;      // index of the main diagonal in a row of A
-    static_assert(kLag % DLU == 0, "prefetch distance must divide kLag");
-    // per wavefront warp of this CTA: incoming rings and counters
-    __shared__ double ring_up[WPC][kRing][NU];   // from the warp below (LU, forward)
-    __shared__ double ring_dn[WPC][kRing];       // from the warp above (backward)
-    __shared__ int up_ready[WPC], dn_ready[WPC]; // batches delivered to this warp
-    __shared__ int up_done[WPC], dn_done[WPC];   // batches of this warp's output consumed
-    __shared__ double lu_save[WPC][4 * NU][32];  // factorisation state at batch start
+    // per wavefront warp of this CTA.  Consumer side: rings of values from the
+    // neighbour warps and their "full" barriers; producer side: staging of the
+    // values for the neighbours and the "empty" barriers the neighbours release.
+    __shared__ __align__(16) double ring_up[WPC][kRing * NU];   // from the warp below (LU, forward)
+    __shared__ __align__(16) double out_up[WPC][kRing * NU];    // for the warp above
+    __shared__ __align__(16) double ring_dn[WPC][kRing];        // from the warp above (backward)
+    __shared__ __align__(16) double out_dn[WPC][kRing];         // for the warp below
+    __shared__ unsigned long long full_up[WPC][kSlots], empty_up[WPC][kSlots];
+    __shared__ unsigned long long full_dn[WPC][kSlots], empty_dn[WPC][kSlots];
     __shared__ unsigned long long stage_bar[WPC][NSTAGE];
+    __shared__ double lu_save[WPC][4 * NU][32];  // factorisation state at batch start
     __shared__ double red[kThreads];
     __shared__ double part[kMaxCluster + 1];
     extern __shared__ __align__(128) double stage_mem[];   // WPC x NSTAGE x PMAX x kBlock
@@ -372,9 +440,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
     const int sys = blockIdx.x / C;
     const MsiSys S = L.dev ? L.dev[sys] : L.s[sys];
     const int nx = L.nx, ny = L.ny;
-    const long long N = (long long)nx * ny;
     const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
     const bool front = wl < WPC;                  // wavefront warp?
+    const int fw = front ? wl : 0;               // this warp's per-warp arrays (helpers: unused)
     const int NWG = C * WPC;                      // wavefront warps in the cluster
     const int wg = rank * WPC + wl;               // global wavefront warp index
     const int j = wg * 32 + lane;
@@ -386,13 +454,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
     const int soff = (64 + kLag) * wg;            // step at which this warp's slot 0 comes up
     const double *__restrict__ a = S.a;
     double *x = S.x;
-    const long long rowbase = (long long)j * nx;
-    // wavefront-major planes: dl1..dlNL, du1..duNU, 1/dl1, residual, sweep result
+    // wavefront-major planes: dl1..dlNL, du1..duNU, 1/dl1, residual, sweep
+    // result, then A (written by k_skew_a)
     double *dlp = S.ws;
     double *dup = dlp + NL * PS;
     double *rl1 = dup + NU * PS;
     double *rp = rl1 + PS;
     double *wp = rp + PS;
+    double *asp = wp + PS;
     // a wavefront warp past the last row group (possible when WPC > 1) owns no
     // slots: it reads group 0 (values unused, all its cells are invalid) and
     // stores nothing
@@ -402,118 +471,79 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
 #define SK(p, s) (p)[wbase + (long long)(s) * kLine]
 
     if (threadIdx.x < WPC) {
-        up_ready[threadIdx.x] = 0; dn_ready[threadIdx.x] = 0;
-        up_done[threadIdx.x] = 0; dn_done[threadIdx.x] = 0;
+        for (int q = 0; q < kSlots; q++) {
+            mbar_init(&full_up[threadIdx.x][q], 1); mbar_init(&empty_up[threadIdx.x][q], 1);
+            mbar_init(&full_dn[threadIdx.x][q], 1); mbar_init(&empty_dn[threadIdx.x][q], 1);
+        }
         for (int q = 0; q < NSTAGE; q++) mbar_init(&stage_bar[threadIdx.x][q], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     Stager<NSTAGE, PMAX> st;
     st.mem = stage_mem;
-    st.base = (front ? wl : 0) * NSTAGE * PMAX * kBlock;
-    st.bar = &stage_bar[front ? wl : 0][0];
+    st.base = fw * NSTAGE * PMAX * kBlock;
+    st.bar = &stage_bar[fw][0];
     st.issued = 0;
     st.consumed = 0;
-    // links of this warp: up channel (LU, forward) feeds warp g+1, down channel
+    // links: the up channel (LU, forward) feeds warp g+1, the down channel
     // (backward) feeds warp g-1; the partner may sit in a neighbouring CTA
     const bool has_below = front && wg > 0, has_above = front && wg < NWG - 1;
-    unsigned up_ring_dst = 0, dn_ring_dst = 0;   // shared::cluster addresses
-    int *up_ready_dst = nullptr, *dn_ready_dst = nullptr, *up_done_dst = nullptr, *dn_done_dst = nullptr;
-    if (front) {
-        if (has_above) {
-            const int cw = (wl + 1 < WPC) ? wl + 1 : 0, cr = (wl + 1 < WPC) ? rank : rank + 1;
-            up_ring_dst = cluster_addr(&ring_up[cw][0][0], cr);
-            up_ready_dst = cl.map_shared_rank(&up_ready[cw], cr);
-            dn_done_dst = cl.map_shared_rank(&dn_done[cw], cr);
-        }
-        if (has_below) {
-            const int pw = (wl > 0) ? wl - 1 : WPC - 1, pr = (wl > 0) ? rank : rank - 1;
-            dn_ring_dst = cluster_addr(&ring_dn[pw][0], pr);
-            dn_ready_dst = cl.map_shared_rank(&dn_ready[pw], pr);
-            up_done_dst = cl.map_shared_rank(&up_done[pw], pr);
-        }
+    unsigned up_ring_dst = 0, up_full_dst = 0, dn_empty_dst = 0;   // partner above
+    unsigned dn_ring_dst = 0, dn_full_dst = 0, up_empty_dst = 0;   // partner below
+    if (has_above) {
+        const int cw = (wl + 1 < WPC) ? wl + 1 : 0, cr = (wl + 1 < WPC) ? rank : rank + 1;
+        up_ring_dst = cluster_addr(&ring_up[cw][0], cr);
+        up_full_dst = cluster_addr(&full_up[cw][0], cr);
+        dn_empty_dst = cluster_addr(&empty_dn[cw][0], cr);
     }
-    cl.sync();   // counters and mbarriers initialised before any use
+    if (has_below) {
+        const int pw = (wl > 0) ? wl - 1 : WPC - 1, pr = (wl > 0) ? rank : rank - 1;
+        dn_ring_dst = cluster_addr(&ring_dn[pw][0], pr);
+        dn_full_dst = cluster_addr(&full_dn[pw][0], pr);
+        up_empty_dst = cluster_addr(&empty_up[pw][0], pr);
+    }
+    cl.sync();   // mbarriers initialised before any use; A staged by k_skew_a
     bool bad_pivot = false, timed_out = false;
-    int up_base = 0, dn_base = 0;       // batches already run on each channel
+    int up_base = 0, dn_base = 0;       // batches sent so far on each channel
     stamp(L, rank, 0);
 
     // ---- incomplete LU (lu2d9 msi2d9-v03.f90:277-432, lu2d5 msi2d5-v03.f90:247-330)
     if (front) {
-        double mw[NU], a1[NU], a2[NU], a3[NU], buf[DLU][ND];
+        double *ap[ND];
+#pragma unroll
+        for (int k = 0; k < ND; k++) ap[k] = asp + k * PS;
+        for (int t = 0; t < NSTAGE - 1 && t < nbatch; t++) stage_issue<ND>(st, ap, line0, t * kLag - soff, SW);
+        double mw[NU], a1[NU], a2[NU], a3[NU];
 #pragma unroll
         for (int q = 0; q < NU; q++) { mw[q] = 0.0; a1[q] = 0.0; a2[q] = 0.0; a3[q] = 0.0; }
-#pragma unroll
-        for (int d = 0; d < DLU; d++) {
-            const int ic = d - soff - 2 * lane;             // cell of step d
-#pragma unroll
-            for (int k = 0; k < ND; k++)
-                buf[d][k] = (row_ok && ic >= 0 && ic < nx) ? PL(a, k + 1, rowbase + ic) : 0.0;
-        }
         for (int b = 0; b < nbatch; b++) {
             const int tb = b * kLag;
-            if (has_below) warp_wait(&up_ready[wl], up_base + b, 0, timed_out);
-            if (has_above && b > kLead) warp_wait(&up_done[wl], up_base + b - kLead, 31, timed_out);
+            const int n = up_base + b;                          // global batch number on the channel
+            const bool send = has_above && b <= nbatch - 2;   // the last batch is never read
+            if (has_below && b >= 1) chan_recv(&full_up[fw][0], n - 1, kLag * NU * 8, timed_out);
+            if (send) chan_slot_free(&empty_up[fw][0], n, timed_out);
+            const int bo = stage_wait(st, timed_out) + lane;
+            if (b + NSTAGE - 1 < nbatch) stage_issue<ND>(st, ap, line0, (b + NSTAGE - 1) * kLag - soff, SW);
 #pragma unroll
             for (int q = 0; q < NU; q++) {
-                lu_save[wl][q][lane] = mw[q]; lu_save[wl][NU + q][lane] = a1[q];
-                lu_save[wl][2 * NU + q][lane] = a2[q]; lu_save[wl][3 * NU + q][lane] = a3[q];
+                lu_save[fw][q][lane] = mw[q]; lu_save[fw][NU + q][lane] = a1[q];
+                lu_save[fw][2 * NU + q][lane] = a2[q]; lu_save[fw][3 * NU + q][lane] = a3[q];
             }
+            const unsigned rbase = (unsigned)up_base * kLag;
             bool bad = false;
 #pragma unroll
-            for (int kk = 0; kk < kLag; kk++) {
-                const int tau = tb + kk;
-                const int s = tau - soff;
-                const int i = s - 2 * lane;
-                const bool valid = row_ok && i >= 0 && i < nx;
-                double cb[ND];
+            for (int pass = 0; pass < 2; pass++) {
+                // pass 0: fast divisions; pass 1 (only if some cell of pass 0
+                // may differ from IEEE division): the batch again from its
+                // start state with IEEE division
+                if (pass == 1) {
+                    if (!__any_sync(kFull, bad)) break;
 #pragma unroll
-                for (int k = 0; k < ND; k++) cb[k] = valid ? buf[kk % DLU][k] : (k == DIAG ? 1.0 : 0.0);
-                if (row_ok && i + DLU >= 0 && i + DLU < nx) {
-#pragma unroll
-                    for (int k = 0; k < ND; k++) buf[kk % DLU][k] = PL(a, k + 1, rowbase + i + DLU);
-                }
-                const int src = tau - 1 - kLag;
-                const int rs = (int)(((unsigned)up_base * kLag + (unsigned)src) & (kRing - 1));
-#pragma unroll
-                for (int q = 0; q < NU; q++) {
-                    double v = __shfl_up_sync(kFull, mw[q], 1);
-                    if (lane == 0) v = (has_below && src >= 0) ? ring_up[wl][rs][q] : 0.0;
-                    a3[q] = a2[q]; a2[q] = a1[q]; a1[q] = v;
-                }
-                // an invalid cell sees a unit row: all its divisions are by 1 and
-                // its outputs are replaced by zeros below
-                const double alpha = (valid && i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2) ? 0.5 : 0.0;
-                double l[NL], u[NU];
-                bool bc = false;
-                lu_cell<ND, true>(cb, alpha, mw, a1, a2, a3, l, u, bc);
-                bad = bad || (valid && bc);
-                if (valid && (!(fabs(l[0]) > 0.0) || !isfinite(l[0]))) bad_pivot = true;
-#pragma unroll
-                for (int q = 0; q < NU; q++) u[q] = valid ? u[q] : 0.0;
-                if (has_rows && s >= 0 && s < SW) {
-                    const double y = __drcp_rn(l[0]);   // forward sweep's reciprocal pivot
-#pragma unroll
-                    for (int k = 0; k < NL; k++) SK(dlp + k * PS, s) = valid ? l[k] : 0.0;
-#pragma unroll
-                    for (int q = 0; q < NU; q++) SK(dup + q * PS, s) = u[q];
-                    SK(rl1, s) = valid ? y : 0.0;
+                    for (int q = 0; q < NU; q++) {
+                        mw[q] = lu_save[fw][q][lane]; a1[q] = lu_save[fw][NU + q][lane];
+                        a2[q] = lu_save[fw][2 * NU + q][lane]; a3[q] = lu_save[fw][3 * NU + q][lane];
+                    }
                 }
 #pragma unroll
-                for (int q = 0; q < NU; q++) mw[q] = u[q];
-                if (lane == 31 && has_above) {
-                    const int ws = (int)(((unsigned)up_base * kLag + (unsigned)tau) & (kRing - 1));
-#pragma unroll
-                    for (int q = 0; q < NU; q++) st_cluster(up_ring_dst + (unsigned)(ws * NU + q) * 8u, u[q]);
-                }
-            }
-            if (__any_sync(kFull, bad)) {
-                // some quotient of this batch may differ from IEEE division:
-                // recompute the batch from its start state with IEEE division
-#pragma unroll
-                for (int q = 0; q < NU; q++) {
-                    mw[q] = lu_save[wl][q][lane]; a1[q] = lu_save[wl][NU + q][lane];
-                    a2[q] = lu_save[wl][2 * NU + q][lane]; a3[q] = lu_save[wl][3 * NU + q][lane];
-                }
                 for (int kk = 0; kk < kLag; kk++) {
                     const int tau = tb + kk;
                     const int s = tau - soff;
@@ -521,24 +551,34 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                     const bool valid = row_ok && i >= 0 && i < nx;
                     double cb[ND];
 #pragma unroll
-                    for (int k = 0; k < ND; k++) cb[k] = valid ? PL(a, k + 1, rowbase + i) : (k == DIAG ? 1.0 : 0.0);
+                    for (int k = 0; k < ND; k++)
+                        cb[k] = valid ? stage_mem[bo + k * kBlock + kk * kLine] : (k == DIAG ? 1.0 : 0.0);
                     const int src = tau - 1 - kLag;
-                    const int rs = (int)(((unsigned)up_base * kLag + (unsigned)src) & (kRing - 1));
+                    const unsigned rs = (rbase + (unsigned)src) & (kRing - 1);
 #pragma unroll
                     for (int q = 0; q < NU; q++) {
                         double v = __shfl_up_sync(kFull, mw[q], 1);
-                        if (lane == 0) v = (has_below && src >= 0) ? ring_up[wl][rs][q] : 0.0;
+                        const double r = ring_up[fw][rs * NU + q];
+                        if (lane == 0) v = (has_below && src >= 0) ? r : 0.0;
                         a3[q] = a2[q]; a2[q] = a1[q]; a1[q] = v;
                     }
+                    // an invalid cell sees a unit row: all its divisions are by 1
+                    // and its outputs are replaced by zeros below
                     const double alpha = (valid && i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2) ? 0.5 : 0.0;
                     double l[NL], u[NU];
-                    bool unused = false;
-                    lu_cell<ND, false>(cb, alpha, mw, a1, a2, a3, l, u, unused);
+                    if (pass == 0) {
+                        bool bc = false;
+                        lu_cell<ND, true>(cb, alpha, mw, a1, a2, a3, l, u, bc);
+                        bad = bad || (valid && bc);
+                    } else {
+                        bool unused = false;
+                        lu_cell<ND, false>(cb, alpha, mw, a1, a2, a3, l, u, unused);
+                    }
                     if (valid && (!(fabs(l[0]) > 0.0) || !isfinite(l[0]))) bad_pivot = true;
 #pragma unroll
                     for (int q = 0; q < NU; q++) u[q] = valid ? u[q] : 0.0;
                     if (has_rows && s >= 0 && s < SW) {
-                        const double y = __drcp_rn(l[0]);
+                        const double y = __drcp_rn(l[0]);   // forward sweep's reciprocal pivot
 #pragma unroll
                         for (int k = 0; k < NL; k++) SK(dlp + k * PS, s) = valid ? l[k] : 0.0;
 #pragma unroll
@@ -547,19 +587,20 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                     }
 #pragma unroll
                     for (int q = 0; q < NU; q++) mw[q] = u[q];
-                    if (lane == 31 && has_above) {
-                        const int ws = (int)(((unsigned)up_base * kLag + (unsigned)tau) & (kRing - 1));
+                    if (lane == 31 && send) {
+                        const unsigned ws = (rbase + (unsigned)tau) & (kRing - 1);
 #pragma unroll
-                        for (int q = 0; q < NU; q++) st_cluster(up_ring_dst + (unsigned)(ws * NU + q) * 8u, u[q]);
+                        for (int q = 0; q < NU; q++) out_up[fw][ws * NU + q] = u[q];
                     }
                 }
             }
-            if (lane == 31 && has_above) st_release(up_ready_dst, up_base + b + 1);
-            if (lane == 0 && has_below) st_release(up_done_dst, up_base + b + 1);
+            if (lane == 31 && send) chan_send(up_ring_dst, up_full_dst, &out_up[fw][0], n, kLag * NU);
+            if (lane == 0 && has_below && b >= 2) chan_release(up_empty_dst, n - 2);
         }
+        if (lane == 0 && has_below && nbatch >= 2) chan_release(up_empty_dst, up_base + nbatch - 2);
         fence_async_global();   // the sweeps read the factors with bulk copies
     }
-    up_base += nbatch;
+    up_base += nbatch - 1;
     if (bad_pivot && L.err) atomicOr(L.err, ERR_NONFINITE_PIVOT);
     stamp(L, rank, 1);
 
@@ -584,86 +625,83 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
             double mine = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
             for (int b = 0; b < nbatch; b++) {
                 const int tb = b * kLag;
-                if (has_below) warp_wait(&up_ready[wl], up_base + b, 0, timed_out);
-                if (has_above && b > kLead) warp_wait(&up_done[wl], up_base + b - kLead, 31, timed_out);
+                const int n = up_base + b;
+                const bool send = has_above && b <= nbatch - 2;
+                if (has_below && b >= 1) chan_recv(&full_up[fw][0], n - 1, kLag * 8, timed_out);
+                if (send) chan_slot_free(&empty_up[fw][0], n, timed_out);
                 const int bo = stage_wait(st, timed_out) + lane;
                 if (b + NSTAGE - 1 < nbatch) stage_issue<NL + 2>(st, fp, line0, (b + NSTAGE - 1) * kLag - soff, SW);
                 const double m0 = mine, b1 = a1, b2 = a2, b3 = a3;   // state at batch start
                 const unsigned rbase = (unsigned)up_base * kLag;       // ring position of step 0
-                const unsigned wbase_ring = up_ring_dst + ((rbase + (unsigned)tb) & (kRing - 1)) * (NU * 8u);
                 bool bad = false;
-                // c: staged coefficients of the current step, rv: ring value
-                // (lane 0's south-east neighbour); both loaded one step ahead
-                double c[NL + 2], rv;
-#pragma unroll
-                for (int k = 0; k < NL + 2; k++) c[k] = stage_mem[bo + k * kBlock];
-                rv = ring_up[wl][(rbase + (unsigned)(tb - 1 - kLag)) & (kRing - 1)][0];
-#pragma unroll
-                for (int kk = 0; kk < kLag; kk++) {
-                    const int tau = tb + kk;
-                    const int s = tau - soff;
-                    const int i = s - 2 * lane;
-                    const bool valid = row_ok && i >= 0 && i < nx;
-                    double cn[NL + 2], rvn = 0.0;
-                    if (kk + 1 < kLag) {
-#pragma unroll
-                        for (int k = 0; k < NL + 2; k++) cn[k] = stage_mem[bo + k * kBlock + (kk + 1) * kLine];
-                        rvn = ring_up[wl][(rbase + (unsigned)(tau - kLag)) & (kRing - 1)][0];
+                double ob[kLag];   // results of the batch, stored after its last step
+    #pragma unroll
+            for (int pass = 0; pass < 2; pass++) {
+                    if (pass == 1) {
+                        // some quotient of pass 0 may differ from IEEE division:
+                        // the batch again from its start state with IEEE division
+                        if (!__any_sync(kFull, bad)) break;
+                        mine = m0; a1 = b1; a2 = b2; a3 = b3;
                     }
-                    const int src = tau - 1 - kLag;
-                    double v = __shfl_up_sync(kFull, mine, 1);
-                    if (lane == 0) v = (has_below && src >= 0) ? rv : 0.0;
-                    a3 = a2; a2 = a1; a1 = v;
-                    // w = -(r + dl2 w_W + dl3 w_SE + dl4 w_S [+ dl5 w_SW]) / dl1
-                    double num;
-                    if (ND == 9) num = c[0] + c[2] * mine + c[3] * a1 + c[4] * a2 + c[5] * a3;
-                    else num = c[0] + c[2] * mine + c[3] * a1 + c[4] * a2;
-                    const double q = div_recip(num, c[1], c[NL + 1]);
-                    bad = bad || (valid && !range_ok(num, c[1]));
-                    const double wv = valid ? -q : 0.0;
-                    if (has_rows && s >= 0 && s < SW) SK(wp, s) = wv;
-                    mine = wv;
-                    if (lane == 31 && has_above) st_cluster(wbase_ring + (unsigned)kk * (NU * 8u), wv);
-                    if (kk + 1 < kLag) {
+                    // c: staged coefficients of the current step, rv: ring value
+                    // (lane 0's south-east neighbour); both loaded one step ahead
+                    double c[NL + 2], rv;
 #pragma unroll
-                        for (int k = 0; k < NL + 2; k++) c[k] = cn[k];
-                        rv = rvn;
-                    }
-                }
-                if (__any_sync(kFull, bad)) {
-                    // some quotient of this batch may differ from IEEE division:
-                    // recompute the batch from its start state with IEEE division
-                    mine = m0; a1 = b1; a2 = b2; a3 = b3;
+                    for (int k = 0; k < NL + 2; k++) c[k] = stage_mem[bo + k * kBlock];
+                    rv = ring_up[fw][(rbase + (unsigned)(tb - 1 - kLag)) & (kRing - 1)];
+#pragma unroll
                     for (int kk = 0; kk < kLag; kk++) {
                         const int tau = tb + kk;
                         const int s = tau - soff;
                         const int i = s - 2 * lane;
                         const bool valid = row_ok && i >= 0 && i < nx;
-                        double cs[NL + 1];
+                        double cn[NL + 2], rvn = 0.0;
+                        if (kk + 1 < kLag) {
 #pragma unroll
-                        for (int k = 0; k < NL + 1; k++) cs[k] = stage_mem[bo + k * kBlock + kk * kLine];
+                            for (int k = 0; k < NL + 2; k++) cn[k] = stage_mem[bo + k * kBlock + (kk + 1) * kLine];
+                            rvn = ring_up[fw][(rbase + (unsigned)(tau - kLag)) & (kRing - 1)];
+                        }
                         const int src = tau - 1 - kLag;
                         double v = __shfl_up_sync(kFull, mine, 1);
-                        if (lane == 0)
-                            v = (has_below && src >= 0) ? ring_up[wl][(rbase + (unsigned)src) & (kRing - 1)][0] : 0.0;
+                        if (lane == 0) v = (has_below && src >= 0) ? rv : 0.0;
                         a3 = a2; a2 = a1; a1 = v;
+                        // w = -(r + dl2 w_W + dl3 w_SE + dl4 w_S [+ dl5 w_SW]) / dl1
                         double num;
-                        if (ND == 9) num = cs[0] + cs[2] * mine + cs[3] * a1 + cs[4] * a2 + cs[5] * a3;
-                        else num = cs[0] + cs[2] * mine + cs[3] * a1 + cs[4] * a2;
-                        const double wv = valid ? -(num / cs[1]) : 0.0;
-                        if (has_rows && s >= 0 && s < SW) SK(wp, s) = wv;
+                        if (ND == 9) num = c[0] + c[2] * mine + c[3] * a1 + c[4] * a2 + c[5] * a3;
+                        else num = c[0] + c[2] * mine + c[3] * a1 + c[4] * a2;
+                        double wv;
+                        if (pass == 0) {
+                            wv = -div_recip(num, c[1], c[NL + 1]);
+                            bad = bad || (valid && !range_ok(num, c[1]));
+                        } else {
+                            wv = -(num / c[1]);
+                        }
+                        wv = valid ? wv : 0.0;
+                        ob[kk] = wv;
                         mine = wv;
-                        if (lane == 31 && has_above)
-                            st_cluster(up_ring_dst + ((rbase + (unsigned)tau) & (kRing - 1)) * (NU * 8u), wv);
+                        if (lane == 31 && send) out_up[fw][(rbase + (unsigned)tau) & (kRing - 1)] = wv;
+                        if (kk + 1 < kLag) {
+#pragma unroll
+                            for (int k = 0; k < NL + 2; k++) c[k] = cn[k];
+                            rv = rvn;
+                        }
                     }
                 }
-                if (lane == 31 && has_above) st_release(up_ready_dst, up_base + b + 1);
-                if (lane == 0 && has_below) st_release(up_done_dst, up_base + b + 1);
+                if (lane == 31 && send) chan_send(up_ring_dst, up_full_dst, &out_up[fw][0], n, kLag);
+                if (lane == 0 && has_below && b >= 2) chan_release(up_empty_dst, n - 2);
+                // the batch's lines of w
+                if (has_rows) {
+                    const int s0 = tb - soff;
+#pragma unroll
+                    for (int kk = 0; kk < kLag; kk++)
+                        if (s0 + kk >= 0 && s0 + kk < SW) SK(wp, s0 + kk) = ob[kk];
+                }
             }
+            if (lane == 0 && has_below && nbatch >= 2) chan_release(up_empty_dst, up_base + nbatch - 2);
             fence_async_global();   // the backward sweep reads w with bulk copies
             __syncwarp();
         }
-        up_base += nbatch;
+        up_base += nbatch - 1;
         if (nit == 1) stamp(L, rank, 3);
         // backward: U z = w; time runs from the top-right corner, so step tau
         // is slot Tmax - tau - soff and step kk of a batch is line kLag-1-kk of
@@ -679,18 +717,20 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
             double mine = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
             for (int b = 0; b < nbatch; b++) {
                 const int tb = b * kLag;
-                if (has_above) warp_wait(&dn_ready[wl], dn_base + b, 31, timed_out);
-                if (has_below && b > kLead) warp_wait(&dn_done[wl], dn_base + b - kLead, 0, timed_out);
+                const int n = dn_base + b;
+                const bool send = has_below && b <= nbatch - 2;
+                if (has_above && b >= 1) chan_recv(&full_dn[fw][0], n - 1, kLag * 8, timed_out);
+                if (send) chan_slot_free(&empty_dn[fw][0], n, timed_out);
                 const int bo = stage_wait(st, timed_out) + lane;
                 if (b + NSTAGE - 1 < nbatch)
                     stage_issue<NU + 1>(st, bp, line0, Tmax - ((b + NSTAGE - 1) * kLag + kLag - 1) - soff, SW);
                 const unsigned rbase = (unsigned)dn_base * kLag;
                 // c: staged {w, du} of the current step, rv: ring value (lane
                 // 31's north-west neighbour); both loaded one step ahead
-                double c[NU + 1], rv;
+                double c[NU + 1], rv, ob[kLag];
 #pragma unroll
                 for (int k = 0; k < NU + 1; k++) c[k] = stage_mem[bo + k * kBlock + (kLag - 1) * kLine];
-                rv = ring_dn[wl][(rbase + (unsigned)(tb - 1 - kLag)) & (kRing - 1)];
+                rv = ring_dn[fw][(rbase + (unsigned)(tb - 1 - kLag)) & (kRing - 1)];
 #pragma unroll
                 for (int kk = 0; kk < kLag; kk++) {
                     const int tau = tb + kk;
@@ -701,7 +741,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                     if (kk + 1 < kLag) {
 #pragma unroll
                         for (int k = 0; k < NU + 1; k++) cn[k] = stage_mem[bo + k * kBlock + (kLag - 2 - kk) * kLine];
-                        rvn = ring_dn[wl][(rbase + (unsigned)(tau - kLag)) & (kRing - 1)];
+                        rvn = ring_dn[fw][(rbase + (unsigned)(tau - kLag)) & (kRing - 1)];
                     }
                     const int src = tau - 1 - kLag;
                     double v = __shfl_down_sync(kFull, mine, 1);
@@ -712,20 +752,28 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                     if (ND == 9) z = c[0] - c[1] * mine - c[2] * a1 - c[3] * a2 - c[4] * a3;
                     else z = c[0] - c[1] * mine - c[2] * a1 - c[3] * a2;
                     z = valid ? z : 0.0;
-                    if (has_rows && s >= 0 && s < SW) SK(wp, s) = z;
+                    ob[kk] = z;
                     mine = z;
-                    if (lane == 0 && has_below) st_cluster(dn_ring_dst + ((rbase + (unsigned)tau) & (kRing - 1)) * 8u, z);
+                    if (lane == 0 && send) out_dn[fw][(rbase + (unsigned)tau) & (kRing - 1)] = z;
                     if (kk + 1 < kLag) {
 #pragma unroll
                         for (int k = 0; k < NU + 1; k++) c[k] = cn[k];
                         rv = rvn;
                     }
                 }
-                if (lane == 0 && has_below) st_release(dn_ready_dst, dn_base + b + 1);
-                if (lane == 31 && has_above) st_release(dn_done_dst, dn_base + b + 1);
+                if (lane == 0 && send) chan_send(dn_ring_dst, dn_full_dst, &out_dn[fw][0], n, kLag);
+                if (lane == 31 && has_above && b >= 2) chan_release(dn_empty_dst, n - 2);
+                // the batch's lines of z
+                if (has_rows) {
+                    const int s0 = Tmax - tb - soff;
+#pragma unroll
+                    for (int kk = 0; kk < kLag; kk++)
+                        if (s0 - kk >= 0 && s0 - kk < SW) SK(wp, s0 - kk) = ob[kk];
+                }
             }
+            if (lane == 31 && has_above && nbatch >= 2) chan_release(dn_empty_dst, dn_base + nbatch - 2);
         }
-        dn_base += nbatch;
+        dn_base += nbatch - 1;
         if (nit == 1) stamp(L, rank, 4);
         // var = z + var, then the new residual
         rr = cluster_residual<ND>(cl, a, S.b, x, wp, rp, nx, ny, SW, red, part);
@@ -740,7 +788,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
     if (front && st.consumed < st.issued) {
         // only after a timed-out wait: let the copies still in flight land
         // before this CTA's shared memory goes away (bounded)
-        while (st.consumed < st.issued) (void)stage_wait(st, timed_out);
+        bool again = false;
+        while (st.consumed < st.issued) (void)stage_wait(st, again);
     }
     if (timed_out && L.err) atomicOr(L.err, ERR_WAIT_TIMEOUT);
     if (rank == 0 && threadIdx.x == 0) {
@@ -756,7 +805,9 @@ bool msi_warp_supported(int ny) { return ny <= 1024; }
 template <int ND, int WPC, int NSTAGE>
 static size_t stage_bytes()
 {
-    return (size_t)WPC * NSTAGE * ((ND == 9 ? 5 : 4) + 2) * kBlock * sizeof(double);
+    constexpr int NL = (ND == 9) ? 5 : 4;
+    constexpr int PMAX = (ND > NL + 2) ? ND : NL + 2;
+    return (size_t)WPC * NSTAGE * PMAX * kBlock * sizeof(double);
 }
 
 // launches one cluster per system if the cluster shape can be scheduled;
@@ -768,7 +819,7 @@ static cudaError_t launch_cluster(const MsiLaunch &L, int nsys, cudaStream_t st,
     const int nwarps = (L.ny + 31) / 32;
     const int C = (nwarps + WPC - 1) / WPC;
     if (C > kMaxCluster) return cudaSuccess;
-    auto kern = k_msi_c<ND, WPC, NSTAGE, (ND == 9 ? 2 : 4)>;
+    auto kern = k_msi_c<ND, WPC, NSTAGE>;
     const size_t smem = stage_bytes<ND, WPC, NSTAGE>();
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -792,22 +843,29 @@ static cudaError_t launch_cluster(const MsiLaunch &L, int nsys, cudaStream_t st,
         return cudaSuccess;
     }
     *fits = true;
+    // A into wavefront-major order first (all systems, whole GPU)
+    const dim3 sg((unsigned)((L.nx + kSkewPad + kSkewTile - 1) / kSkewTile), (unsigned)nwarps, (unsigned)nsys);
+    k_skew_a<ND><<<sg, 256, 0, st>>>(L);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
     return cudaLaunchKernelEx(&cfg, kern, L);
 }
 
 template <int ND>
 static cudaError_t launch_nd(const MsiLaunch &L, int nsys, cudaStream_t st)
 {
-    // the bulk copies need 16-byte aligned scratch; systems given through a
-    // device array cannot be checked here
+    // the bulk copies need 16-byte aligned scratch (systems given through a
+    // device array cannot be checked here) and the wavefront-major layout
+    // must fit in the scratch
     bool aligned = L.dev == nullptr;
     for (int k = 0; k < nsys && aligned; k++) aligned = ((uintptr_t)L.s[k].ws % 16) == 0;
-    if (aligned) {
+    const bool room = L.ws_cap == 0 || L.ws_cap >= msi_cluster_work_doubles(ND, L.nx, L.ny);
+    if (aligned && room) {
         // fewest wavefront warps per CTA (one SM per warp) whose cluster fits
         bool fits = false;
         cudaError_t e = launch_cluster<ND, 1, 4>(L, nsys, st, &fits);
         if (e != cudaSuccess || fits) return e;
-        e = launch_cluster<ND, 2, 3>(L, nsys, st, &fits);
+        e = launch_cluster<ND, 2, 2>(L, nsys, st, &fits);
         if (e != cudaSuccess || fits) return e;
     }
     return launch_msi_generic(ND, L, nsys, st);

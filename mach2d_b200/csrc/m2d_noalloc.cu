@@ -36,6 +36,9 @@ double *g_scratch_addr[kMaxDevices] = {nullptr};
 }  // namespace
 
 extern void m2d_set_last_error_msg(const char *);
+extern "C" int m2d_msi_solve_device_ws(int nd, int nx, int ny, int nitm, double tol, const double *d_a,
+                                   const double *d_b, double *d_x, double *d_work, long work_doubles,
+                                   void *stream, int *d_nit, unsigned long long *d_times);
 
 extern "C" long m2d_msi_noalloc_max_cells(int nd)
 {
@@ -51,8 +54,14 @@ extern "C" int m2d_msi_solve_device_noalloc(int nd, int nx, int ny, int nitm, do
         m2d_set_last_error_msg("msi_solve_device_noalloc: bad arguments");
         return M2D_ERR_ARG;
     }
-    const long need = m2d_msi_workspace_doubles(nd, nx, ny);
-    if (need < 0 || need > kNoallocScratchDoubles) {
+    // the plain-layout kernel must fit; the wavefront-major one is used when
+    // it fits as well
+    const long need = (long)m2d::msi_generic_work_doubles(nd, nx, ny) + 4;
+    if (ny > m2d::msi_max_ny()) {
+        m2d_set_last_error_msg("msi_solve_device_noalloc: ny exceeds m2d_msi_max_ny()");
+        return M2D_ERR_TOO_LARGE;
+    }
+    if (need > kNoallocScratchDoubles) {
         m2d_set_last_error_msg(nd == 9
             ? "msi_solve_device_noalloc: nx*ny exceeds the maximum of 157286 cells for the 9-diagonal solve"
             : "msi_solve_device_noalloc: nx*ny exceeds the maximum of 196607 cells for the 5-diagonal solve");
@@ -82,5 +91,6 @@ extern "C" int m2d_msi_solve_device_noalloc(int nd, int nx, int ny, int nitm, do
         }
         work = g_scratch_addr[dev];
     }
-    return m2d_msi_solve_device(nd, nx, ny, nitm, tol, d_a, d_b, d_x, work, stream, d_nit);
+    return m2d_msi_solve_device_ws(nd, nx, ny, nitm, tol, d_a, d_b, d_x, work, kNoallocScratchDoubles, stream,
+                                   d_nit, nullptr);
 }

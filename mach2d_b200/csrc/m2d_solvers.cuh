@@ -18,8 +18,12 @@ struct MsiSys {
     double *rr;        // [0] = |r0|^2, [1] = |r_final|^2 (device doubles)
 };
 
-// scratch doubles one system needs (the larger of the two kernels' layouts)
+// scratch doubles one system needs (the larger of the two kernels' layouts),
+// and what each layout needs on its own: launch_msi uses the cluster kernel
+// only when ws_cap leaves room for its layout
 size_t msi_work_doubles(int nd, int nx, int ny);
+size_t msi_generic_work_doubles(int nd, int nx, int ny);
+size_t msi_cluster_work_doubles(int nd, int nx, int ny);
 // the cluster kernel's factor planes are "wavefront-major": slot
 // ((j/32) * (nx + 62) + i + 2 (j%32)) * 32 + j%32 holds cell (i, j), so the
 // 32 rows a warp sweeps read and write one contiguous 256-byte line per step
@@ -34,6 +38,7 @@ struct MsiLaunch {
     unsigned long long *prof;  // optional phase timestamps (ns, %globaltimer), may be null:
                                // start, after LU, after r0, first forward, first backward,
                                // first residual, end
+    size_t ws_cap;             // doubles each ws holds; 0 = at least msi_work_doubles()
 };
 
 // Largest ny the one-CTA wavefront kernel accepts (its shared-memory ring
