@@ -125,6 +125,32 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned by
                  ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
                  : "memory");
 }
+// Ordered shared-memory loads and shuffles.  A sweep step's shuffle of the
+// previous step's result is its critical input; issued before the next
+// step's shared-memory loads, it does not queue behind them.
+__device__ __forceinline__ double lds_v(unsigned addr)
+{
+    double v;
+    asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(addr));
+    return v;
+}
+__device__ __forceinline__ double shfl_up_v(double x)
+{
+    double v;
+    asm volatile("{\n\t.reg .b32 lo, hi;\n\tmov.b64 {lo, hi}, %1;\n\t"
+                 "shfl.sync.up.b32 lo, lo, 1, 0, -1;\n\tshfl.sync.up.b32 hi, hi, 1, 0, -1;\n\t"
+                 "mov.b64 %0, {lo, hi};\n\t}" : "=d"(v) : "d"(x));
+    return v;
+}
+__device__ __forceinline__ double shfl_down_v(double x)
+{
+    double v;
+    asm volatile("{\n\t.reg .b32 lo, hi;\n\tmov.b64 {lo, hi}, %1;\n\t"
+                 "shfl.sync.down.b32 lo, lo, 1, 31, -1;\n\tshfl.sync.down.b32 hi, hi, 1, 31, -1;\n\t"
+                 "mov.b64 %0, {lo, hi};\n\t}" : "=d"(v) : "d"(x));
+    return v;
+}
+
 // 32-bit shared::cluster address of the same variable in CTA `rank`
 __device__ __forceinline__ unsigned cluster_addr(const void *p, int rank)
 {
@@ -292,17 +318,17 @@ __device__ double cluster_residual(cg::cluster_group &cl, const double *__restri
     const long long per = (N + C - 1) / C;
     const long long lo = per * rank, hi = (lo + per < N) ? lo + per : N;
     if (z) {
-#pragma unroll 4
+#pragma unroll 8
         for (long long np = lo + threadIdx.x; np < hi; np += kThreads) {
-            const int j = (int)(np / nx), i = (int)(np - (long long)j * nx);
+            const int j = (int)((unsigned)np / (unsigned)nx), i = (int)np - j * nx;   // N < 2^31
             x[np] = z[skew_slot(i, j, sw)] + x[np];
         }
         cl.sync();
     }
     double acc = 0.0;
-#pragma unroll 2
+#pragma unroll 8
     for (long long np = lo + threadIdx.x; np < hi; np += kThreads) {
-        const int j = (int)(np / nx), i = (int)(np - (long long)j * nx);
+        const int j = (int)((unsigned)np / (unsigned)nx), i = (int)np - j * nx;   // N < 2^31
         const double v = residual_cell<ND>(a, b, x, np, i, j, nx, ny, N);
         r[skew_slot(i, j, sw)] = v;
         acc = acc + v * v;
@@ -478,6 +504,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
         for (int q = 0; q < NSTAGE; q++) mbar_init(&stage_bar[threadIdx.x][q], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    const unsigned sbase = smem_u32(stage_mem);
+    const unsigned rup = smem_u32(&ring_up[fw][0]), rdn = smem_u32(&ring_dn[fw][0]);
     Stager<NSTAGE, PMAX> st;
     st.mem = stage_mem;
     st.base = fw * NSTAGE * PMAX * kBlock;
@@ -655,14 +683,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                         const int s = tau - soff;
                         const int i = s - 2 * lane;
                         const bool valid = row_ok && i >= 0 && i < nx;
+                        const int src = tau - 1 - kLag;
+                        double v = shfl_up_v(mine);
                         double cn[NL + 2], rvn = 0.0;
                         if (kk + 1 < kLag) {
 #pragma unroll
-                            for (int k = 0; k < NL + 2; k++) cn[k] = stage_mem[bo + k * kBlock + (kk + 1) * kLine];
-                            rvn = ring_up[fw][(rbase + (unsigned)(tau - kLag)) & (kRing - 1)];
+                            for (int k = 0; k < NL + 2; k++) cn[k] = lds_v(sbase + (unsigned)(bo + k * kBlock + (kk + 1) * kLine) * 8u);
+                            rvn = lds_v(rup + ((rbase + (unsigned)(tau - kLag)) & (kRing - 1)) * 8u);
                         }
-                        const int src = tau - 1 - kLag;
-                        double v = __shfl_up_sync(kFull, mine, 1);
                         if (lane == 0) v = (has_below && src >= 0) ? rv : 0.0;
                         a3 = a2; a2 = a1; a1 = v;
                         // w = -(r + dl2 w_W + dl3 w_SE + dl4 w_S [+ dl5 w_SW]) / dl1
@@ -737,14 +765,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                     const int s = Tmax - tau - soff;
                     const int i = s - 2 * lane;
                     const bool valid = row_ok && i >= 0 && i < nx;
+                    const int src = tau - 1 - kLag;
+                    double v = shfl_down_v(mine);
                     double cn[NU + 1], rvn = 0.0;
                     if (kk + 1 < kLag) {
 #pragma unroll
-                        for (int k = 0; k < NU + 1; k++) cn[k] = stage_mem[bo + k * kBlock + (kLag - 2 - kk) * kLine];
-                        rvn = ring_dn[fw][(rbase + (unsigned)(tau - kLag)) & (kRing - 1)];
+                        for (int k = 0; k < NU + 1; k++) cn[k] = lds_v(sbase + (unsigned)(bo + k * kBlock + (kLag - 2 - kk) * kLine) * 8u);
+                        rvn = lds_v(rdn + ((rbase + (unsigned)(tau - kLag)) & (kRing - 1)) * 8u);
                     }
-                    const int src = tau - 1 - kLag;
-                    double v = __shfl_down_sync(kFull, mine, 1);
                     if (lane == 31) v = (has_above && src >= 0) ? rv : 0.0;
                     a3 = a2; a2 = a1; a1 = v;
                     // z = w - du1 z_E - du2 z_NW - du3 z_N [- du4 z_NE]; E = own previous
@@ -860,7 +888,8 @@ static cudaError_t launch_nd(const MsiLaunch &L, int nsys, cudaStream_t st)
     bool aligned = L.dev == nullptr;
     for (int k = 0; k < nsys && aligned; k++) aligned = ((uintptr_t)L.s[k].ws % 16) == 0;
     const bool room = L.ws_cap == 0 || L.ws_cap >= msi_cluster_work_doubles(ND, L.nx, L.ny);
-    if (aligned && room) {
+    const bool small = (long long)L.nx * L.ny < (1LL << 31);   // 32-bit cell indices in the passes
+    if (aligned && room && small) {
         // fewest wavefront warps per CTA (one SM per warp) whose cluster fits
         bool fits = false;
         cudaError_t e = launch_cluster<ND, 1, 4>(L, nsys, st, &fits);
