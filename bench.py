@@ -327,7 +327,7 @@ def run_ours(args):
             "e2e": {"value": e2e, "unit": "cell-updates/s", "h2d_bytes_per_step": nbytes,
                     "d2h_bytes_per_step": nbytes},
             "gpu_launches": launches,
-            "roofline": {"kernel": "k_msi<5> (MSI5 factorisation + fb2d5 iterations, one CTA)",
+            "roofline": {"kernel": "k_msi_c<5,1,4> (MSI5 factorisation + fb2d5 iterations, one cluster)",
                          "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind,
                          "traffic": traffic, "algorithmic_bytes_per_launch": alg,

@@ -71,7 +71,9 @@ int m2d_msi5_solve_it(const int *nx, const int *ny, const int *nitm, const doubl
  * live in GPU memory (CUDA Fortran / OpenACC data, or another library):
  * nd = 9 or 5; d_a, d_b, d_x device pointers in the layout above; d_work a
  * caller-allocated device buffer of m2d_msi_workspace_doubles(nd,nx,ny)
- * doubles; `stream` a cudaStream_t (NULL: the default stream).  The call is
+ * doubles (16-byte aligned, as cudaMalloc returns it, for the cluster kernel;
+ * otherwise the slower one-CTA kernel runs); `stream` a cudaStream_t (NULL:
+ * the default stream).  The call is
  * asynchronous: the iteration count is written to the device int *d_nit
  * (may be NULL) when the solve completes on `stream`. */
 long m2d_msi_workspace_doubles(int nd, int nx, int ny);

@@ -409,34 +409,33 @@ __device__ __forceinline__ void lu_cell(const double (&cb)[ND], double alpha, co
 
 // A (plane-major, cell order) -> wavefront-major planes for the factorisation's
 // bulk copies: line (w, s) lane l holds cell (s - 2 l, 32 w + l).  A CTA
-// transposes a tile of 32 rows x (kSkewTile + 62) cells through shared memory
-// into kSkewTile lines; cells outside the grid become zeros.
+// transposes one plane's tile of 32 rows x (kSkewTile + 62) cells through
+// shared memory into kSkewTile lines; cells outside the grid become zeros.
+// Grid: (line tiles, row groups, systems x ND planes).
 constexpr int kSkewTile = 64;
 template <int ND>
 __global__ void __launch_bounds__(256) k_skew_a(MsiLaunch L)
 {
     __shared__ double tile[32][kSkewTile + kSkewPad + 1];
-    const MsiSys S = L.s[blockIdx.z];
+    const int sys = blockIdx.z / ND, k = blockIdx.z - sys * ND;
+    const MsiSys S = L.s[sys];
     const int nx = L.nx, ny = L.ny;
     const long long N = (long long)nx * ny;
     const int NL = (ND == 9) ? 5 : 4, NU = (ND == 9) ? 4 : 3;
     const int SW = nx + kSkewPad;
     const long long PS = (long long)((ny + 31) / 32) * SW * kLine;
-    double *as = S.ws + (long long)(NL + NU + 3) * PS;
+    double *as = S.ws + (long long)(NL + NU + 3 + k) * PS;
     const int w = blockIdx.y, c0 = blockIdx.x * kSkewTile;
     constexpr int TW = kSkewTile + kSkewPad;
-    for (int k = 0; k < ND; k++) {
-        for (int idx = threadIdx.x; idx < 32 * TW; idx += blockDim.x) {
-            const int r = idx / TW, c = idx - r * TW;
-            const int i = c0 - kSkewPad + c, j = 32 * w + r;
-            tile[r][c] = (j < ny && i >= 0 && i < nx) ? PL(S.a, k + 1, (long long)j * nx + i) : 0.0;
-        }
-        __syncthreads();
-        for (int idx = threadIdx.x; idx < kSkewTile * 32; idx += blockDim.x) {
-            const int t = idx >> 5, l = idx & 31, s = c0 + t;
-            if (s < SW) as[(long long)k * PS + ((long long)w * SW + s) * kLine + l] = tile[l][t + kSkewPad - 2 * l];
-        }
-        __syncthreads();
+    for (int idx = threadIdx.x; idx < 32 * TW; idx += blockDim.x) {
+        const int r = idx / TW, c = idx - r * TW;
+        const int i = c0 - kSkewPad + c, j = 32 * w + r;
+        tile[r][c] = (j < ny && i >= 0 && i < nx) ? PL(S.a, k + 1, (long long)j * nx + i) : 0.0;
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < kSkewTile * 32; idx += blockDim.x) {
+        const int t = idx >> 5, l = idx & 31, s = c0 + t;
+        if (s < SW) as[((long long)w * SW + s) * kLine + l] = tile[l][t + kSkewPad - 2 * l];
     }
 }
 
@@ -872,7 +871,7 @@ static cudaError_t launch_cluster(const MsiLaunch &L, int nsys, cudaStream_t st,
     }
     *fits = true;
     // A into wavefront-major order first (all systems, whole GPU)
-    const dim3 sg((unsigned)((L.nx + kSkewPad + kSkewTile - 1) / kSkewTile), (unsigned)nwarps, (unsigned)nsys);
+    const dim3 sg((unsigned)((L.nx + kSkewPad + kSkewTile - 1) / kSkewTile), (unsigned)nwarps, (unsigned)(nsys * ND));
     k_skew_a<ND><<<sg, 256, 0, st>>>(L);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
