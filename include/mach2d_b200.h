@@ -90,6 +90,22 @@ int m2d_msi_solve_device_timed(int nd, int nx, int ny, int nitm, double tol,
                                double *d_work, void *stream, int *d_nit,
                                unsigned long long *d_times);
 
+/* No counterpart in the reference ("MSI_MIXED" in solvers_init).  The same
+ * MSI iteration with the factorisation and both sweeps in FP32: the residual
+ * r = A x - b, x, the norm and the stopping test |r| < tol |r0| stay FP64, so
+ * the iteration is FP64 iterative refinement preconditioned by the FP32
+ * incomplete LU and converges to the FP64 solution; it is not bitwise equal
+ * to m2d_msi9_solve.  Same arguments as m2d_msi9_solve_it / the device
+ * variant above; ny <= 1024 runs the FP32 cluster kernel, larger ny the FP64
+ * one-CTA kernel. */
+int m2d_msi9_solve_mixed(const int *nx, const int *ny, const int *nitm, const double *tol,
+                         const double *a, const double *b, double *x, int *nit);
+int m2d_msi5_solve_mixed(const int *nx, const int *ny, const int *nitm, const double *tol,
+                         const double *a, const double *b, double *x, int *nit);
+int m2d_msi_solve_device_mixed(int nd, int nx, int ny, int nitm, double tol, const double *d_a,
+                               const double *d_b, double *d_x, double *d_work, void *stream,
+                               int *d_nit);
+
 /* No counterpart in the reference.  The same device-resident solve for
  * callers that cannot allocate device memory when they solve: a host program
  * whose device memory is all owned by its own pool (an OpenACC or CUDA
@@ -264,7 +280,7 @@ typedef struct m2d_case {
     double Rg, gamma, mu, kappa;            /* CONSTANT thermophysical model */
     int itmmax, itpmax;
     double tolm, tolt;
-    int solver;                             /* 0 MSI, 1 TDMA */
+    int solver;                             /* 0 MSI, 1 TDMA, 2 MSI with FP32 factors and sweeps */
     int nitm_u, nitm_p;
     double tol_u, tol_p;
     int dtmodel;                            /* 0 RAMP, 1 SCARBOROUGH */

@@ -107,7 +107,7 @@ Fields empty_fields(int nx, int ny)
 }
 
 int msi_solve_host(int nd, const int *nx, const int *ny, const int *nitm, const double *tol,
-                   const double *a, const double *b, double *x, int *nit_out)
+                   const double *a, const double *b, double *x, int *nit_out, int prec = 0)
 {
     if (!dims_ok(nx, ny) || !nitm || !tol) return fail(ST_ARG, "msi: bad arguments");
     if (*ny > msi_max_ny()) return fail(ST_TOO_LARGE, "msi: ny exceeds m2d_msi_max_ny()");
@@ -116,6 +116,7 @@ int msi_solve_host(int nd, const int *nx, const int *ny, const int *nitm, const 
     MsiLaunch L;
     memset(&L, 0, sizeof L);
     L.nx = *nx; L.ny = *ny; L.nitm = *nitm; L.tol = *tol;
+    L.prec = prec;
     MsiSys &S = L.s[0];
     S.a = s.in(a, (size_t)nd * N);
     S.b = s.in(b, N);
@@ -161,6 +162,12 @@ int m2d_msi9_solve(const int *nx, const int *ny, const int *nitm, const double *
 int m2d_msi5_solve(const int *nx, const int *ny, const int *nitm, const double *tol,
                    const double *a, const double *b, double *x)
 { return msi_solve_host(5, nx, ny, nitm, tol, a, b, x, nullptr); }
+int m2d_msi9_solve_mixed(const int *nx, const int *ny, const int *nitm, const double *tol,
+                         const double *a, const double *b, double *x, int *nit)
+{ return msi_solve_host(9, nx, ny, nitm, tol, a, b, x, nit, 1); }
+int m2d_msi5_solve_mixed(const int *nx, const int *ny, const int *nitm, const double *tol,
+                         const double *a, const double *b, double *x, int *nit)
+{ return msi_solve_host(5, nx, ny, nitm, tol, a, b, x, nit, 1); }
 int m2d_msi9_solve_it(const int *nx, const int *ny, const int *nitm, const double *tol,
                       const double *a, const double *b, double *x, int *nit)
 { return msi_solve_host(9, nx, ny, nitm, tol, a, b, x, nit); }
@@ -180,11 +187,12 @@ long m2d_msi_workspace_doubles(int nd, int nx, int ny)
 // work_doubles covers at least the plain-layout kernel
 int m2d_msi_solve_device_ws(int nd, int nx, int ny, int nitm, double tol, const double *d_a,
                             const double *d_b, double *d_x, double *d_work, long work_doubles,
-                            void *stream, int *d_nit, unsigned long long *d_times)
+                            void *stream, int *d_nit, unsigned long long *d_times, int prec)
 {
     MsiLaunch L;
     memset(&L, 0, sizeof L);
     L.nx = nx; L.ny = ny; L.nitm = nitm; L.tol = tol;
+    L.prec = prec;
     MsiSys &S = L.s[0];
     S.a = d_a; S.b = d_b; S.x = d_x;
     S.ws = d_work;
@@ -204,7 +212,17 @@ int m2d_msi_solve_device(int nd, int nx, int ny, int nitm, double tol, const dou
         return fail(ST_ARG, "msi_solve_device: bad arguments");
     if (ny > msi_max_ny()) return fail(ST_TOO_LARGE, "msi_solve_device: ny exceeds m2d_msi_max_ny()");
     return m2d_msi_solve_device_ws(nd, nx, ny, nitm, tol, d_a, d_b, d_x, d_work,
-                                   m2d_msi_workspace_doubles(nd, nx, ny), stream, d_nit, nullptr);
+                                   m2d_msi_workspace_doubles(nd, nx, ny), stream, d_nit, nullptr, 0);
+}
+
+int m2d_msi_solve_device_mixed(int nd, int nx, int ny, int nitm, double tol, const double *d_a,
+                               const double *d_b, double *d_x, double *d_work, void *stream, int *d_nit)
+{
+    if ((nd != 9 && nd != 5) || nx < 4 || ny < 4 || !d_a || !d_b || !d_x || !d_work)
+        return fail(ST_ARG, "msi_solve_device_mixed: bad arguments");
+    if (ny > msi_max_ny()) return fail(ST_TOO_LARGE, "msi_solve_device_mixed: ny exceeds m2d_msi_max_ny()");
+    return m2d_msi_solve_device_ws(nd, nx, ny, nitm, tol, d_a, d_b, d_x, d_work,
+                                   m2d_msi_workspace_doubles(nd, nx, ny), stream, d_nit, nullptr, 1);
 }
 
 int m2d_msi_solve_device_timed(int nd, int nx, int ny, int nitm, double tol, const double *d_a,
@@ -215,7 +233,7 @@ int m2d_msi_solve_device_timed(int nd, int nx, int ny, int nitm, double tol, con
         return fail(ST_ARG, "msi_solve_device_timed: bad arguments");
     if (ny > msi_max_ny()) return fail(ST_TOO_LARGE, "msi_solve_device_timed: ny exceeds m2d_msi_max_ny()");
     return m2d_msi_solve_device_ws(nd, nx, ny, nitm, tol, d_a, d_b, d_x, d_work,
-                                   m2d_msi_workspace_doubles(nd, nx, ny), stream, d_nit, d_times);
+                                   m2d_msi_workspace_doubles(nd, nx, ny), stream, d_nit, d_times, 0);
 }
 
 static int tdma_host(int nd, const int *nx, const int *ny, const int *nitm, const double *a,

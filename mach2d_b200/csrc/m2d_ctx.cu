@@ -87,7 +87,7 @@ extern "C" int m2d_create(const m2d_case *c, int device, m2d_ctx **out)
     if (!c || !out) return ctx_fail(M2D_ERR_ARG, "m2d_create: null argument");
     *out = nullptr;
     if (c->nxr < 3 || c->nyr < 3) return ctx_fail(M2D_ERR_ARG, "m2d_create: need at least 3x3 real volumes");
-    if (c->solver == 0 && c->nyr + 2 > msi_max_ny()) return ctx_fail(M2D_ERR_TOO_LARGE, "m2d_create: ny exceeds m2d_msi_max_ny()");
+    if (c->solver != 1 && c->nyr + 2 > msi_max_ny()) return ctx_fail(M2D_ERR_TOO_LARGE, "m2d_create: ny exceeds m2d_msi_max_ny()");
     HostInstance h;
     int rc = build_instance(*c, h);
     if (rc) return ctx_fail(rc, "m2d_create: grid set-up failed");
@@ -194,17 +194,18 @@ static int solve9(m2d_ctx *x, int nsys, double *const *a, double *const *b, doub
                   const int *islot, const int *rslot)
 {
     const m2d_case &c = x->c;
-    if (c.solver == 0) {
+    if (c.solver != 1) {
         MsiLaunch L;
         memset(&L, 0, sizeof L);
         L.nx = x->nx; L.ny = x->ny; L.nitm = c.nitm_u; L.tol = c.tol_u;
+        L.prec = (c.solver == 2) ? 1 : 0;
         L.err = x->dint + I_ERR;
         for (int k = 0; k < nsys; k++) {
             L.s[k].a = a[k]; L.s[k].b = b[k]; L.s[k].x = v[k];
             L.s[k].ws = x->ws9[k];
             L.s[k].nit = x->dint + islot[k]; L.s[k].rr = x->dsc + rslot[k];
         }
-        KL(launch_msi(9, L, nsys, x->st), 1);
+        KL(launch_msi(9, L, nsys, x->st), 2);   // A transpose + solve
     } else {
         for (int k = 0; k < nsys; k++)
             KL(launch_tdma(9, x->nx, x->ny, c.nitm_u, a[k], b[k], v[k], x->P, x->Q, x->st), 4 * c.nitm_u);
@@ -215,15 +216,16 @@ static int solve9(m2d_ctx *x, int nsys, double *const *a, double *const *b, doub
 static int solve5(m2d_ctx *x)
 {
     const m2d_case &c = x->c;
-    if (c.solver == 0) {
+    if (c.solver != 1) {
         MsiLaunch L;
         memset(&L, 0, sizeof L);
         L.nx = x->nx; L.ny = x->ny; L.nitm = c.nitm_p; L.tol = c.tol_p;
+        L.prec = (c.solver == 2) ? 1 : 0;
         L.err = x->dint + I_ERR;
         L.s[0].a = x->f.ap; L.s[0].b = x->f.bp; L.s[0].x = x->f.pl;
         L.s[0].ws = x->ws5;
         L.s[0].nit = x->dint + I_NIT_P; L.s[0].rr = x->dsc + S_RR + 4;
-        KL(launch_msi(5, L, 1, x->st), 1);
+        KL(launch_msi(5, L, 1, x->st), 2);   // A transpose + solve
     } else {
         KL(launch_tdma(5, x->nx, x->ny, c.nitm_p, x->f.ap, x->f.bp, x->f.pl, x->P, x->Q, x->st), 4 * c.nitm_p);
     }

@@ -36,6 +36,7 @@
 // produces zeros, which is exactly the zero-neighbour rule of the general
 // formula, so results stay bitwise equal to the lexicographic reference loop.
 #include <cstdint>
+#include <type_traits>
 #include <cooperative_groups.h>
 #include "m2d_solvers.cuh"
 
@@ -128,10 +129,17 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned by
 // Ordered shared-memory loads and shuffles.  A sweep step's shuffle of the
 // previous step's result is its critical input; issued before the next
 // step's shared-memory loads, it does not queue behind them.
-__device__ __forceinline__ double lds_v(unsigned addr)
+template <typename T> __device__ __forceinline__ T lds_v(unsigned addr);
+template <> __device__ __forceinline__ double lds_v<double>(unsigned addr)
 {
     double v;
     asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(addr));
+    return v;
+}
+template <> __device__ __forceinline__ float lds_v<float>(unsigned addr)
+{
+    float v;
+    asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(addr));
     return v;
 }
 __device__ __forceinline__ double shfl_up_v(double x)
@@ -140,6 +148,18 @@ __device__ __forceinline__ double shfl_up_v(double x)
     asm volatile("{\n\t.reg .b32 lo, hi;\n\tmov.b64 {lo, hi}, %1;\n\t"
                  "shfl.sync.up.b32 lo, lo, 1, 0, -1;\n\tshfl.sync.up.b32 hi, hi, 1, 0, -1;\n\t"
                  "mov.b64 %0, {lo, hi};\n\t}" : "=d"(v) : "d"(x));
+    return v;
+}
+__device__ __forceinline__ float shfl_up_v(float x)
+{
+    float v;
+    asm volatile("shfl.sync.up.b32 %0, %1, 1, 0, -1;" : "=f"(v) : "f"(x));
+    return v;
+}
+__device__ __forceinline__ float shfl_down_v(float x)
+{
+    float v;
+    asm volatile("shfl.sync.down.b32 %0, %1, 1, 31, -1;" : "=f"(v) : "f"(x));
     return v;
 }
 __device__ __forceinline__ double shfl_down_v(double x)
@@ -191,10 +211,10 @@ __device__ __forceinline__ void fence_async_shared() { asm volatile("fence.proxy
 // Per wavefront warp: NSTAGE staging blocks of NP planes x kLag lines, one
 // mbarrier each.  issued/consumed count staged batches over all phases, so
 // block = count % NSTAGE and the mbarrier parity = (count / NSTAGE) & 1.
-template <int NSTAGE, int PMAX>
+template <typename TS, int NSTAGE, int PMAX>
 struct Stager {
-    double *mem;                 // the CTA's staging memory
-    int base;                    // this warp's area in it (doubles)
+    TS *mem;                     // the CTA's staging memory
+    int base;                    // this warp's area in it (elements)
     unsigned long long *bar;
     int issued, consumed;
     __device__ int block(int q) const { return base + q * PMAX * kBlock; }
@@ -202,18 +222,18 @@ struct Stager {
 
 // stage slot lines [s_lo, s_lo + kLag) of NP wavefront-major planes (lines
 // outside [0, sw) are not copied: every cell on them is invalid)
-template <int NP, int NSTAGE, int PMAX>
-__device__ __forceinline__ void stage_issue(Stager<NSTAGE, PMAX> &st, double *const *planes,
+template <int NP, typename TS, int NSTAGE, int PMAX>
+__device__ __forceinline__ void stage_issue(Stager<TS, NSTAGE, PMAX> &st, TS *const *planes,
                                             long long line0, int s_lo, int sw)
 {
     const int q = st.issued % NSTAGE;
     if ((threadIdx.x & 31) == 0) {
         fence_async_shared();   // earlier reads of this block precede the copies into it
         const int lo = max(s_lo, 0), hi = min(s_lo + kLag, sw);
-        const unsigned bytes = hi > lo ? (unsigned)(hi - lo) * kLine * 8u : 0u;
+        const unsigned bytes = hi > lo ? (unsigned)(hi - lo) * kLine * (unsigned)sizeof(TS) : 0u;
         mbar_arrive_tx(&st.bar[q], bytes * NP);
         if (bytes) {
-            double *dst = st.mem + st.block(q) + (lo - s_lo) * kLine;
+            TS *dst = st.mem + st.block(q) + (lo - s_lo) * kLine;
 #pragma unroll
             for (int p = 0; p < NP; p++)
                 bulk_g2s(dst + p * kBlock, planes[p] + (line0 + lo) * kLine, bytes, &st.bar[q]);
@@ -222,8 +242,8 @@ __device__ __forceinline__ void stage_issue(Stager<NSTAGE, PMAX> &st, double *co
     st.issued++;
 }
 // waits for the next staged batch; returns its block's offset in st.mem
-template <int NSTAGE, int PMAX>
-__device__ __forceinline__ int stage_wait(Stager<NSTAGE, PMAX> &st, bool &timed_out)
+template <typename TS, int NSTAGE, int PMAX>
+__device__ __forceinline__ int stage_wait(Stager<TS, NSTAGE, PMAX> &st, bool &timed_out)
 {
     const int q = st.consumed % NSTAGE;
     const unsigned parity = (unsigned)(st.consumed / NSTAGE) & 1u;
@@ -256,13 +276,14 @@ __device__ __forceinline__ void chan_slot_free(unsigned long long *empty, int n,
 {
     if (n >= kSlots) mbar_wait(&empty[n & (kSlots - 1)], (unsigned)(n / kSlots - 1) & 1u, timed_out);
 }
-// producer lane that staged the values: ship batch n (vals doubles)
-__device__ __forceinline__ void chan_send(unsigned ring_dst, unsigned full_dst, const double *out, int n, int vals)
+// producer lane that staged the values: ship batch n (vals elements)
+template <typename TS>
+__device__ __forceinline__ void chan_send(unsigned ring_dst, unsigned full_dst, const TS *out, int n, int vals)
 {
     const int slot = n & (kSlots - 1);
     fence_async_shared();   // the staged values become visible to the bulk copy
-    bulk_s2s(ring_dst + (unsigned)(slot * vals) * 8u, out + slot * vals, (unsigned)vals * 8u,
-             full_dst + (unsigned)slot * 8u);
+    bulk_s2s(ring_dst + (unsigned)(slot * vals) * (unsigned)sizeof(TS), out + slot * vals,
+             (unsigned)vals * (unsigned)sizeof(TS), full_dst + (unsigned)slot * 8u);
 }
 __device__ __forceinline__ void chan_release(unsigned empty_dst, int n)
 {
@@ -307,9 +328,9 @@ __device__ __forceinline__ double residual_cell(const double *__restrict__ a, co
 // x += z when z (wavefront-major) is given, then r = A x - b stored
 // wavefront-major.  Returns the cluster-wide sum of r^2, identical in every
 // thread.  Starts with a cluster barrier: every row's sweep must be final.
-template <int ND>
+template <int ND, typename TS>
 __device__ double cluster_residual(cg::cluster_group &cl, const double *__restrict__ a,
-                                   const double *__restrict__ b, double *x, const double *z, double *r,
+                                   const double *__restrict__ b, double *x, const TS *z, TS *r,
                                    int nx, int ny, int sw, double *red, double *part)
 {
     cl.sync();
@@ -321,7 +342,7 @@ __device__ double cluster_residual(cg::cluster_group &cl, const double *__restri
 #pragma unroll 8
         for (long long np = lo + threadIdx.x; np < hi; np += kThreads) {
             const int j = (int)((unsigned)np / (unsigned)nx), i = (int)np - j * nx;   // N < 2^31
-            x[np] = z[skew_slot(i, j, sw)] + x[np];
+            x[np] = (double)z[skew_slot(i, j, sw)] + x[np];
         }
         cl.sync();
     }
@@ -330,7 +351,7 @@ __device__ double cluster_residual(cg::cluster_group &cl, const double *__restri
     for (long long np = lo + threadIdx.x; np < hi; np += kThreads) {
         const int j = (int)((unsigned)np / (unsigned)nx), i = (int)np - j * nx;   // N < 2^31
         const double v = residual_cell<ND>(a, b, x, np, i, j, nx, ny, N);
-        r[skew_slot(i, j, sw)] = v;
+        r[skew_slot(i, j, sw)] = (TS)v;
         acc = acc + v * v;
     }
     fence_async_global();   // the forward sweep reads r with bulk copies
@@ -361,7 +382,7 @@ __device__ double cluster_residual(cg::cluster_group &cl, const double *__restri
 template <int ND, bool FAST>
 __device__ __forceinline__ void lu_cell(const double (&cb)[ND], double alpha, const double *mw,
                                         const double *a1, const double *a2, const double *a3, double *l,
-                                        double *u, bool &bad)
+                                        double *u, double &y1, bool &bad)
 {
     auto dv = [&](double n, double d) -> double { return FAST ? div_fast(n, d, bad) : n / d; };
     if (ND == 9) {
@@ -379,11 +400,13 @@ __device__ __forceinline__ void lu_cell(const double (&cb)[ND], double alpha, co
         const double n2 = b8 - l2 * mw[3] - alpha * phi4;
         if (FAST) {
             const double y = __drcp_rn(l1);
+            y1 = y;
             bad = bad || !range_ok(n0, l1) || !range_ok(n1, l1) || !range_ok(n2, l1) || !range_ok(b9, l1);
             u[0] = div_recip(n0, l1, y); u[1] = div_recip(n1, l1, y);
             u[2] = div_recip(n2, l1, y); u[3] = div_recip(b9, l1, y);
         } else {
             u[0] = n0 / l1; u[1] = n1 / l1; u[2] = n2 / l1; u[3] = b9 / l1;
+            y1 = __drcp_rn(l1);
         }
         l[0] = l1; l[1] = l2; l[2] = l3; l[3] = l4; l[4] = l5;
     } else {
@@ -398,22 +421,67 @@ __device__ __forceinline__ void lu_cell(const double (&cb)[ND], double alpha, co
         const double n2 = b5 - alpha * phi4;
         if (FAST) {
             const double y = __drcp_rn(l1);
+            y1 = y;
             bad = bad || !range_ok(n0, l1) || !range_ok(n1, l1) || !range_ok(n2, l1);
             u[0] = div_recip(n0, l1, y); u[1] = div_recip(n1, l1, y); u[2] = div_recip(n2, l1, y);
         } else {
             u[0] = n0 / l1; u[1] = n1 / l1; u[2] = n2 / l1;
+            y1 = __drcp_rn(l1);
         }
         l[0] = l1; l[1] = l2; l[2] = l3; l[3] = l4;
     }
 }
 
-// A (plane-major, cell order) -> wavefront-major planes for the factorisation's
-// bulk copies: line (w, s) lane l holds cell (s - 2 l, 32 w + l).  A CTA
-// transposes one plane's tile of 32 rows x (kSkewTile + 62) cells through
-// shared memory into kSkewTile lines; cells outside the grid become zeros.
-// Grid: (line tiles, row groups, systems x ND planes).
-constexpr int kSkewTile = 64;
+// The same factorisation step in FP32 for the mixed-precision solve.  Its
+// factors only precondition an FP64 iteration, so the operation order is
+// free: fused multiply-adds and approximate reciprocals; y1 = 1/l1.
 template <int ND>
+__device__ __forceinline__ void lu_cell_f(const float (&cb)[ND], float alpha, const float *mw,
+                                          const float *a1, const float *a2, const float *a3, float *l,
+                                          float *u, float &y1)
+{
+    if (ND == 9) {
+        const float b1 = cb[0], b2 = cb[1], b3 = cb[2], b4 = cb[3], b5 = cb[4];
+        const float b6 = cb[5], b7 = cb[6], b8 = cb[7], b9 = cb[8];
+        const float l5 = b1;
+        const float l4 = __fdividef(fmaf(-alpha * b3, a1[0], fmaf(-l5, a3[0], b2)), fmaf(-alpha * a2[0], a1[0], 1.0f));
+        const float l3 = fmaf(-l4, a2[0], b3);
+        const float l2 = __fdividef(fmaf(-2.0f * alpha * l5, a3[1], fmaf(-l5, a3[2], fmaf(-l4, a2[1], b4))),
+                                    fmaf(2.0f * alpha, mw[1], 1.0f));
+        const float phi1 = l3 * a1[0], phi2 = l5 * a3[1], phi3 = l3 * a1[3], phi4 = l2 * mw[1];
+        const float t = fmaf(-l5, a3[3], fmaf(-l4, a2[2], fmaf(-l3, a1[1], fmaf(-l2, mw[0], b5))));
+        const float l1 = fmaf(alpha, 2.0f * phi1 + phi2 + phi3 + 2.0f * phi4, t);
+        const float y = __fdividef(1.0f, l1);
+        u[0] = fmaf(-2.0f * alpha, phi1 + phi3, fmaf(-l4, a2[3], fmaf(-l3, a1[2], b6))) * y;
+        u[1] = fmaf(-l2, mw[2], b7) * y;
+        u[2] = fmaf(-alpha, phi4, fmaf(-l2, mw[3], b8)) * y;
+        u[3] = b9 * y;
+        y1 = y;
+        l[0] = l1; l[1] = l2; l[2] = l3; l[3] = l4; l[4] = l5;
+    } else {
+        const float b1 = cb[0], b2 = cb[1], b3 = cb[2], b4 = cb[3], b5 = cb[4];
+        const float l4 = __fdividef(b1, fmaf(-alpha * a2[0], a1[0], 1.0f));
+        const float l3 = -l4 * a2[0];
+        const float l2 = __fdividef(fmaf(-l4, a2[1], b2), fmaf(2.0f * alpha, mw[1], 1.0f));
+        const float phi1 = l3 * a1[0], phi4 = l2 * mw[1];
+        const float t = fmaf(-l4, a2[2], fmaf(-l3, a1[1], fmaf(-l2, mw[0], b3)));
+        const float l1 = fmaf(2.0f * alpha, phi1 + phi4, t);
+        const float y = __fdividef(1.0f, l1);
+        u[0] = fmaf(-2.0f * alpha, phi1, fmaf(-l3, a1[2], b4)) * y;
+        u[1] = -l2 * mw[2] * y;
+        u[2] = fmaf(-alpha, phi4, b5) * y;
+        y1 = y;
+        l[0] = l1; l[1] = l2; l[2] = l3; l[3] = l4;
+    }
+}
+
+// A (plane-major, cell order) -> wavefront-major planes of element type TS for
+// the factorisation's bulk copies: line (w, s) lane l holds cell
+// (s - 2 l, 32 w + l).  A CTA transposes one plane's tile of 32 rows x
+// (kSkewTile + 62) cells through shared memory into kSkewTile lines; cells
+// outside the grid become zeros.  Grid: (line tiles, row groups, systems x ND).
+constexpr int kSkewTile = 64;
+template <int ND, typename TS>
 __global__ void __launch_bounds__(256) k_skew_a(MsiLaunch L)
 {
     __shared__ double tile[32][kSkewTile + kSkewPad + 1];
@@ -424,7 +492,7 @@ __global__ void __launch_bounds__(256) k_skew_a(MsiLaunch L)
     const int NL = (ND == 9) ? 5 : 4, NU = (ND == 9) ? 4 : 3;
     const int SW = nx + kSkewPad;
     const long long PS = (long long)((ny + 31) / 32) * SW * kLine;
-    double *as = S.ws + (long long)(NL + NU + 3 + k) * PS;
+    TS *as = reinterpret_cast<TS *>(S.ws) + (long long)(NL + NU + 3 + k) * PS;
     const int w = blockIdx.y, c0 = blockIdx.x * kSkewTile;
     constexpr int TW = kSkewTile + kSkewPad;
     for (int idx = threadIdx.x; idx < 32 * TW; idx += blockDim.x) {
@@ -435,31 +503,38 @@ __global__ void __launch_bounds__(256) k_skew_a(MsiLaunch L)
     __syncthreads();
     for (int idx = threadIdx.x; idx < kSkewTile * 32; idx += blockDim.x) {
         const int t = idx >> 5, l = idx & 31, s = c0 + t;
-        if (s < SW) as[((long long)w * SW + s) * kLine + l] = tile[l][t + kSkewPad - 2 * l];
+        if (s < SW) as[((long long)w * SW + s) * kLine + l] = (TS)tile[l][t + kSkewPad - 2 * l];
     }
 }
 
-template <int ND, int WPC, int NSTAGE>
+// TS = double: the reference's FP64 algorithm, bitwise.  TS = float: the
+// factors and both sweeps in FP32 inside the FP64 iteration (residual, x,
+// norm and stopping test stay FP64): iterative refinement preconditioned by
+// the FP32 factorisation.
+template <int ND, int WPC, int NSTAGE, typename TS>
 __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
 {
+    constexpr bool EXACT = std::is_same<TS, double>::value;
     constexpr int NU = (ND == 9) ? 4 : 3;
     constexpr int NL = (ND == 9) ? 5 : 4;
     constexpr int PMAX = (ND > NL + 2) ? ND : NL + 2;   // planes staged per batch
     constexpr int DIAG = (ND == 9) ? 4 : 2;      // index of the main diagonal in a row of A
+    constexpr unsigned ES = sizeof(TS);
     // per wavefront warp of this CTA.  Consumer side: rings of values from the
     // neighbour warps and their "full" barriers; producer side: staging of the
     // values for the neighbours and the "empty" barriers the neighbours release.
-    __shared__ __align__(16) double ring_up[WPC][kRing * NU];   // from the warp below (LU, forward)
-    __shared__ __align__(16) double out_up[WPC][kRing * NU];    // for the warp above
-    __shared__ __align__(16) double ring_dn[WPC][kRing];        // from the warp above (backward)
-    __shared__ __align__(16) double out_dn[WPC][kRing];         // for the warp below
+    __shared__ __align__(16) TS ring_up[WPC][kRing * NU];   // from the warp below (LU, forward)
+    __shared__ __align__(16) TS out_up[WPC][kRing * NU];    // for the warp above
+    __shared__ __align__(16) TS ring_dn[WPC][kRing];        // from the warp above (backward)
+    __shared__ __align__(16) TS out_dn[WPC][kRing];         // for the warp below
     __shared__ unsigned long long full_up[WPC][kSlots], empty_up[WPC][kSlots];
     __shared__ unsigned long long full_dn[WPC][kSlots], empty_dn[WPC][kSlots];
     __shared__ unsigned long long stage_bar[WPC][NSTAGE];
-    __shared__ double lu_save[WPC][4 * NU][32];  // factorisation state at batch start
+    __shared__ TS lu_save[WPC][4 * NU][32];      // factorisation state at batch start
     __shared__ double red[kThreads];
     __shared__ double part[kMaxCluster + 1];
-    extern __shared__ __align__(128) double stage_mem[];   // WPC x NSTAGE x PMAX x kBlock
+    extern __shared__ __align__(128) double stage_raw[];   // WPC x NSTAGE x PMAX x kBlock elements
+    TS *stage_mem = reinterpret_cast<TS *>(stage_raw);
     cg::cluster_group cl = cg::this_cluster();
     const int C = (int)cl.num_blocks(), rank = (int)cl.block_rank();
     const int sys = blockIdx.x / C;
@@ -479,14 +554,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
     const int soff = (64 + kLag) * wg;            // step at which this warp's slot 0 comes up
     const double *__restrict__ a = S.a;
     double *x = S.x;
-    // wavefront-major planes: dl1..dlNL, du1..duNU, 1/dl1, residual, sweep
-    // result, then A (written by k_skew_a)
-    double *dlp = S.ws;
-    double *dup = dlp + NL * PS;
-    double *rl1 = dup + NU * PS;
-    double *rp = rl1 + PS;
-    double *wp = rp + PS;
-    double *asp = wp + PS;
+    // wavefront-major planes of TS: dl1..dlNL, du1..duNU, 1/dl1, residual,
+    // sweep result, then A (written by k_skew_a)
+    TS *dlp = reinterpret_cast<TS *>(S.ws);
+    TS *dup = dlp + NL * PS;
+    TS *rl1 = dup + NU * PS;
+    TS *rp = rl1 + PS;
+    TS *wp = rp + PS;
+    TS *asp = wp + PS;
     // a wavefront warp past the last row group (possible when WPC > 1) owns no
     // slots: it reads group 0 (values unused, all its cells are invalid) and
     // stores nothing
@@ -505,7 +580,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
     }
     const unsigned sbase = smem_u32(stage_mem);
     const unsigned rup = smem_u32(&ring_up[fw][0]), rdn = smem_u32(&ring_dn[fw][0]);
-    Stager<NSTAGE, PMAX> st;
+    Stager<TS, NSTAGE, PMAX> st;
     st.mem = stage_mem;
     st.base = fw * NSTAGE * PMAX * kBlock;
     st.bar = &stage_bar[fw][0];
@@ -535,30 +610,32 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
 
     // ---- incomplete LU (lu2d9 msi2d9-v03.f90:277-432, lu2d5 msi2d5-v03.f90:247-330)
     if (front) {
-        double *ap[ND];
+        TS *ap[ND];
 #pragma unroll
         for (int k = 0; k < ND; k++) ap[k] = asp + k * PS;
         for (int t = 0; t < NSTAGE - 1 && t < nbatch; t++) stage_issue<ND>(st, ap, line0, t * kLag - soff, SW);
-        double mw[NU], a1[NU], a2[NU], a3[NU];
+        TS mw[NU], a1[NU], a2[NU], a3[NU];
 #pragma unroll
-        for (int q = 0; q < NU; q++) { mw[q] = 0.0; a1[q] = 0.0; a2[q] = 0.0; a3[q] = 0.0; }
+        for (int q = 0; q < NU; q++) { mw[q] = 0; a1[q] = 0; a2[q] = 0; a3[q] = 0; }
         for (int b = 0; b < nbatch; b++) {
             const int tb = b * kLag;
             const int n = up_base + b;                          // global batch number on the channel
             const bool send = has_above && b <= nbatch - 2;   // the last batch is never read
-            if (has_below && b >= 1) chan_recv(&full_up[fw][0], n - 1, kLag * NU * 8, timed_out);
+            if (has_below && b >= 1) chan_recv(&full_up[fw][0], n - 1, kLag * NU * ES, timed_out);
             if (send) chan_slot_free(&empty_up[fw][0], n, timed_out);
             const int bo = stage_wait(st, timed_out) + lane;
             if (b + NSTAGE - 1 < nbatch) stage_issue<ND>(st, ap, line0, (b + NSTAGE - 1) * kLag - soff, SW);
+            if (EXACT) {
 #pragma unroll
-            for (int q = 0; q < NU; q++) {
-                lu_save[fw][q][lane] = mw[q]; lu_save[fw][NU + q][lane] = a1[q];
-                lu_save[fw][2 * NU + q][lane] = a2[q]; lu_save[fw][3 * NU + q][lane] = a3[q];
+                for (int q = 0; q < NU; q++) {
+                    lu_save[fw][q][lane] = mw[q]; lu_save[fw][NU + q][lane] = a1[q];
+                    lu_save[fw][2 * NU + q][lane] = a2[q]; lu_save[fw][3 * NU + q][lane] = a3[q];
+                }
             }
             const unsigned rbase = (unsigned)up_base * kLag;
             bool bad = false;
 #pragma unroll
-            for (int pass = 0; pass < 2; pass++) {
+            for (int pass = 0; pass < (EXACT ? 2 : 1); pass++) {
                 // pass 0: fast divisions; pass 1 (only if some cell of pass 0
                 // may differ from IEEE division): the batch again from its
                 // start state with IEEE division
@@ -576,41 +653,45 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                     const int s = tau - soff;
                     const int i = s - 2 * lane;
                     const bool valid = row_ok && i >= 0 && i < nx;
-                    double cb[ND];
+                    TS cb[ND];
 #pragma unroll
                     for (int k = 0; k < ND; k++)
-                        cb[k] = valid ? stage_mem[bo + k * kBlock + kk * kLine] : (k == DIAG ? 1.0 : 0.0);
+                        cb[k] = valid ? stage_mem[bo + k * kBlock + kk * kLine] : (TS)(k == DIAG ? 1 : 0);
                     const int src = tau - 1 - kLag;
                     const unsigned rs = (rbase + (unsigned)src) & (kRing - 1);
 #pragma unroll
                     for (int q = 0; q < NU; q++) {
-                        double v = __shfl_up_sync(kFull, mw[q], 1);
-                        const double r = ring_up[fw][rs * NU + q];
-                        if (lane == 0) v = (has_below && src >= 0) ? r : 0.0;
+                        TS v = __shfl_up_sync(kFull, mw[q], 1);
+                        const TS r = ring_up[fw][rs * NU + q];
+                        if (lane == 0) v = (has_below && src >= 0) ? r : (TS)0;
                         a3[q] = a2[q]; a2[q] = a1[q]; a1[q] = v;
                     }
                     // an invalid cell sees a unit row: all its divisions are by 1
                     // and its outputs are replaced by zeros below
-                    const double alpha = (valid && i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2) ? 0.5 : 0.0;
-                    double l[NL], u[NU];
-                    if (pass == 0) {
-                        bool bc = false;
-                        lu_cell<ND, true>(cb, alpha, mw, a1, a2, a3, l, u, bc);
-                        bad = bad || (valid && bc);
+                    const TS alpha = (valid && i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2) ? (TS)0.5 : (TS)0;
+                    TS l[NL], u[NU], y;
+                    if constexpr (EXACT) {
+                        if (pass == 0) {
+                            bool bc = false;
+                            lu_cell<ND, true>(cb, alpha, mw, a1, a2, a3, l, u, y, bc);
+                            bad = bad || (valid && bc);
+                        } else {
+                            bool unused = false;
+                            lu_cell<ND, false>(cb, alpha, mw, a1, a2, a3, l, u, y, unused);
+                        }
                     } else {
-                        bool unused = false;
-                        lu_cell<ND, false>(cb, alpha, mw, a1, a2, a3, l, u, unused);
+                        lu_cell_f<ND>(cb, alpha, mw, a1, a2, a3, l, u, y);
                     }
-                    if (valid && (!(fabs(l[0]) > 0.0) || !isfinite(l[0]))) bad_pivot = true;
+                    if (valid && (!(fabs((double)l[0]) > 0.0) || !isfinite((double)l[0]))) bad_pivot = true;
 #pragma unroll
-                    for (int q = 0; q < NU; q++) u[q] = valid ? u[q] : 0.0;
+                    for (int q = 0; q < NU; q++) u[q] = valid ? u[q] : (TS)0;
                     if (has_rows && s >= 0 && s < SW) {
-                        const double y = __drcp_rn(l[0]);   // forward sweep's reciprocal pivot
+                        // y = 1/dl1 (RN for FP64), the forward sweep's reciprocal pivot
 #pragma unroll
-                        for (int k = 0; k < NL; k++) SK(dlp + k * PS, s) = valid ? l[k] : 0.0;
+                        for (int k = 0; k < NL; k++) SK(dlp + k * PS, s) = valid ? l[k] : (TS)0;
 #pragma unroll
                         for (int q = 0; q < NU; q++) SK(dup + q * PS, s) = u[q];
-                        SK(rl1, s) = valid ? y : 0.0;
+                        SK(rl1, s) = valid ? y : (TS)0;
                     }
 #pragma unroll
                     for (int q = 0; q < NU; q++) mw[q] = u[q];
@@ -632,7 +713,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
     stamp(L, rank, 1);
 
     // ---- fb2d9 / fb2d5 (msi2d9-v03.f90:42-262, msi2d5-v03.f90:42-233)
-    const double rr0 = cluster_residual<ND>(cl, a, S.b, x, nullptr, rp, nx, ny, SW, red, part);
+    const double rr0 = cluster_residual<ND, TS>(cl, a, S.b, x, nullptr, rp, nx, ny, SW, red, part);
     stamp(L, rank, 2);
     const double gammarp = L.tol * sqrt(rr0);
     const int cap = (L.nitm > 0) ? L.nitm : kMaxIterUnbounded;
@@ -643,27 +724,27 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
         // forward: L w = -r.  Staged planes {r, dl1..dlNL, 1/dl1}; step kk of
         // a batch is line kk of its block
         if (front) {
-            double *fp[NL + 2];
+            TS *fp[NL + 2];
             fp[0] = rp;
 #pragma unroll
             for (int k = 0; k < NL; k++) fp[k + 1] = dlp + k * PS;
             fp[NL + 1] = rl1;
             for (int t = 0; t < NSTAGE - 1 && t < nbatch; t++) stage_issue<NL + 2>(st, fp, line0, t * kLag - soff, SW);
-            double mine = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+            TS mine = 0, a1 = 0, a2 = 0, a3 = 0;
             for (int b = 0; b < nbatch; b++) {
                 const int tb = b * kLag;
                 const int n = up_base + b;
                 const bool send = has_above && b <= nbatch - 2;
-                if (has_below && b >= 1) chan_recv(&full_up[fw][0], n - 1, kLag * 8, timed_out);
+                if (has_below && b >= 1) chan_recv(&full_up[fw][0], n - 1, kLag * ES, timed_out);
                 if (send) chan_slot_free(&empty_up[fw][0], n, timed_out);
                 const int bo = stage_wait(st, timed_out) + lane;
                 if (b + NSTAGE - 1 < nbatch) stage_issue<NL + 2>(st, fp, line0, (b + NSTAGE - 1) * kLag - soff, SW);
-                const double m0 = mine, b1 = a1, b2 = a2, b3 = a3;   // state at batch start
-                const unsigned rbase = (unsigned)up_base * kLag;       // ring position of step 0
+                const TS m0 = mine, b1 = a1, b2 = a2, b3 = a3;   // state at batch start
+                const unsigned rbase = (unsigned)up_base * kLag;   // ring position of step 0
                 bool bad = false;
-                double ob[kLag];   // results of the batch, stored after its last step
-    #pragma unroll
-            for (int pass = 0; pass < 2; pass++) {
+                TS ob[kLag];   // results of the batch, stored after its last step
+#pragma unroll
+                for (int pass = 0; pass < (EXACT ? 2 : 1); pass++) {
                     if (pass == 1) {
                         // some quotient of pass 0 may differ from IEEE division:
                         // the batch again from its start state with IEEE division
@@ -672,7 +753,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                     }
                     // c: staged coefficients of the current step, rv: ring value
                     // (lane 0's south-east neighbour); both loaded one step ahead
-                    double c[NL + 2], rv;
+                    TS c[NL + 2], rv;
 #pragma unroll
                     for (int k = 0; k < NL + 2; k++) c[k] = stage_mem[bo + k * kBlock];
                     rv = ring_up[fw][(rbase + (unsigned)(tb - 1 - kLag)) & (kRing - 1)];
@@ -683,27 +764,34 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                         const int i = s - 2 * lane;
                         const bool valid = row_ok && i >= 0 && i < nx;
                         const int src = tau - 1 - kLag;
-                        double v = shfl_up_v(mine);
-                        double cn[NL + 2], rvn = 0.0;
+                        TS v = shfl_up_v(mine);
+                        TS cn[NL + 2], rvn = 0;
                         if (kk + 1 < kLag) {
 #pragma unroll
-                            for (int k = 0; k < NL + 2; k++) cn[k] = lds_v(sbase + (unsigned)(bo + k * kBlock + (kk + 1) * kLine) * 8u);
-                            rvn = lds_v(rup + ((rbase + (unsigned)(tau - kLag)) & (kRing - 1)) * 8u);
+                            for (int k = 0; k < NL + 2; k++)
+                                cn[k] = lds_v<TS>(sbase + (unsigned)(bo + k * kBlock + (kk + 1) * kLine) * ES);
+                            rvn = lds_v<TS>(rup + ((rbase + (unsigned)(tau - kLag)) & (kRing - 1)) * ES);
                         }
-                        if (lane == 0) v = (has_below && src >= 0) ? rv : 0.0;
+                        if (lane == 0) v = (has_below && src >= 0) ? rv : (TS)0;
                         a3 = a2; a2 = a1; a1 = v;
                         // w = -(r + dl2 w_W + dl3 w_SE + dl4 w_S [+ dl5 w_SW]) / dl1
-                        double num;
-                        if (ND == 9) num = c[0] + c[2] * mine + c[3] * a1 + c[4] * a2 + c[5] * a3;
-                        else num = c[0] + c[2] * mine + c[3] * a1 + c[4] * a2;
-                        double wv;
-                        if (pass == 0) {
-                            wv = -div_recip(num, c[1], c[NL + 1]);
-                            bad = bad || (valid && !range_ok(num, c[1]));
+                        TS wv;
+                        if constexpr (EXACT) {
+                            double num;
+                            if (ND == 9) num = c[0] + c[2] * mine + c[3] * a1 + c[4] * a2 + c[5] * a3;
+                            else num = c[0] + c[2] * mine + c[3] * a1 + c[4] * a2;
+                            if (pass == 0) {
+                                wv = -div_recip(num, c[1], c[NL + 1]);
+                                bad = bad || (valid && !range_ok(num, c[1]));
+                            } else {
+                                wv = -(num / c[1]);
+                            }
                         } else {
-                            wv = -(num / c[1]);
+                            float num = fmaf(c[4], a2, fmaf(c[3], a1, fmaf(c[2], mine, c[0])));
+                            if (ND == 9) num = fmaf(c[5], a3, num);
+                            wv = -num * c[NL + 1];
                         }
-                        wv = valid ? wv : 0.0;
+                        wv = valid ? wv : (TS)0;
                         ob[kk] = wv;
                         mine = wv;
                         if (lane == 31 && send) out_up[fw][(rbase + (unsigned)tau) & (kRing - 1)] = wv;
@@ -735,18 +823,18 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
         // its block.  Staged planes {w, du1..duNU}
         if (front) {
             const int Tmax = (nx - 1) + 2 * (ny - 1) + kLag * (NWG - 1);
-            double *bp[NU + 1];
+            TS *bp[NU + 1];
             bp[0] = wp;
 #pragma unroll
             for (int k = 0; k < NU; k++) bp[k + 1] = dup + k * PS;
             for (int t = 0; t < NSTAGE - 1 && t < nbatch; t++)
                 stage_issue<NU + 1>(st, bp, line0, Tmax - (t * kLag + kLag - 1) - soff, SW);
-            double mine = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+            TS mine = 0, a1 = 0, a2 = 0, a3 = 0;
             for (int b = 0; b < nbatch; b++) {
                 const int tb = b * kLag;
                 const int n = dn_base + b;
                 const bool send = has_below && b <= nbatch - 2;
-                if (has_above && b >= 1) chan_recv(&full_dn[fw][0], n - 1, kLag * 8, timed_out);
+                if (has_above && b >= 1) chan_recv(&full_dn[fw][0], n - 1, kLag * ES, timed_out);
                 if (send) chan_slot_free(&empty_dn[fw][0], n, timed_out);
                 const int bo = stage_wait(st, timed_out) + lane;
                 if (b + NSTAGE - 1 < nbatch)
@@ -754,7 +842,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                 const unsigned rbase = (unsigned)dn_base * kLag;
                 // c: staged {w, du} of the current step, rv: ring value (lane
                 // 31's north-west neighbour); both loaded one step ahead
-                double c[NU + 1], rv, ob[kLag];
+                TS c[NU + 1], rv, ob[kLag];
 #pragma unroll
                 for (int k = 0; k < NU + 1; k++) c[k] = stage_mem[bo + k * kBlock + (kLag - 1) * kLine];
                 rv = ring_dn[fw][(rbase + (unsigned)(tb - 1 - kLag)) & (kRing - 1)];
@@ -765,20 +853,26 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                     const int i = s - 2 * lane;
                     const bool valid = row_ok && i >= 0 && i < nx;
                     const int src = tau - 1 - kLag;
-                    double v = shfl_down_v(mine);
-                    double cn[NU + 1], rvn = 0.0;
+                    TS v = shfl_down_v(mine);
+                    TS cn[NU + 1], rvn = 0;
                     if (kk + 1 < kLag) {
 #pragma unroll
-                        for (int k = 0; k < NU + 1; k++) cn[k] = lds_v(sbase + (unsigned)(bo + k * kBlock + (kLag - 2 - kk) * kLine) * 8u);
-                        rvn = lds_v(rdn + ((rbase + (unsigned)(tau - kLag)) & (kRing - 1)) * 8u);
+                        for (int k = 0; k < NU + 1; k++)
+                            cn[k] = lds_v<TS>(sbase + (unsigned)(bo + k * kBlock + (kLag - 2 - kk) * kLine) * ES);
+                        rvn = lds_v<TS>(rdn + ((rbase + (unsigned)(tau - kLag)) & (kRing - 1)) * ES);
                     }
-                    if (lane == 31) v = (has_above && src >= 0) ? rv : 0.0;
+                    if (lane == 31) v = (has_above && src >= 0) ? rv : (TS)0;
                     a3 = a2; a2 = a1; a1 = v;
                     // z = w - du1 z_E - du2 z_NW - du3 z_N [- du4 z_NE]; E = own previous
-                    double z;
-                    if (ND == 9) z = c[0] - c[1] * mine - c[2] * a1 - c[3] * a2 - c[4] * a3;
-                    else z = c[0] - c[1] * mine - c[2] * a1 - c[3] * a2;
-                    z = valid ? z : 0.0;
+                    TS z;
+                    if constexpr (EXACT) {
+                        if (ND == 9) z = c[0] - c[1] * mine - c[2] * a1 - c[3] * a2 - c[4] * a3;
+                        else z = c[0] - c[1] * mine - c[2] * a1 - c[3] * a2;
+                    } else {
+                        z = fmaf(-c[3], a2, fmaf(-c[2], a1, fmaf(-c[1], mine, c[0])));
+                        if (ND == 9) z = fmaf(-c[4], a3, z);
+                    }
+                    z = valid ? z : (TS)0;
                     ob[kk] = z;
                     mine = z;
                     if (lane == 0 && send) out_dn[fw][(rbase + (unsigned)tau) & (kRing - 1)] = z;
@@ -803,7 +897,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
         dn_base += nbatch - 1;
         if (nit == 1) stamp(L, rank, 4);
         // var = z + var, then the new residual
-        rr = cluster_residual<ND>(cl, a, S.b, x, wp, rp, nx, ny, SW, red, part);
+        rr = cluster_residual<ND, TS>(cl, a, S.b, x, wp, rp, nx, ny, SW, red, part);
         if (nit == 1) stamp(L, rank, 5);
         if (sqrt(rr) < gammarp) break;
         if (nit == cap) {
@@ -829,25 +923,25 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
 
 bool msi_warp_supported(int ny) { return ny <= 1024; }
 
-template <int ND, int WPC, int NSTAGE>
+template <int ND, int WPC, int NSTAGE, typename TS>
 static size_t stage_bytes()
 {
     constexpr int NL = (ND == 9) ? 5 : 4;
     constexpr int PMAX = (ND > NL + 2) ? ND : NL + 2;
-    return (size_t)WPC * NSTAGE * PMAX * kBlock * sizeof(double);
+    return (size_t)WPC * NSTAGE * PMAX * kBlock * sizeof(TS);
 }
 
 // launches one cluster per system if the cluster shape can be scheduled;
 // *fits = false (and nothing launched) otherwise
-template <int ND, int WPC, int NSTAGE>
+template <int ND, int WPC, int NSTAGE, typename TS>
 static cudaError_t launch_cluster(const MsiLaunch &L, int nsys, cudaStream_t st, bool *fits)
 {
     *fits = false;
     const int nwarps = (L.ny + 31) / 32;
     const int C = (nwarps + WPC - 1) / WPC;
     if (C > kMaxCluster) return cudaSuccess;
-    auto kern = k_msi_c<ND, WPC, NSTAGE>;
-    const size_t smem = stage_bytes<ND, WPC, NSTAGE>();
+    auto kern = k_msi_c<ND, WPC, NSTAGE, TS>;
+    const size_t smem = stage_bytes<ND, WPC, NSTAGE, TS>();
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -872,36 +966,40 @@ static cudaError_t launch_cluster(const MsiLaunch &L, int nsys, cudaStream_t st,
     *fits = true;
     // A into wavefront-major order first (all systems, whole GPU)
     const dim3 sg((unsigned)((L.nx + kSkewPad + kSkewTile - 1) / kSkewTile), (unsigned)nwarps, (unsigned)(nsys * ND));
-    k_skew_a<ND><<<sg, 256, 0, st>>>(L);
+    k_skew_a<ND, TS><<<sg, 256, 0, st>>>(L);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     return cudaLaunchKernelEx(&cfg, kern, L);
 }
 
-template <int ND>
-static cudaError_t launch_nd(const MsiLaunch &L, int nsys, cudaStream_t st)
+template <int ND, typename TS>
+static cudaError_t launch_nd(const MsiLaunch &L, int nsys, cudaStream_t st, bool *done)
 {
     // the bulk copies need 16-byte aligned scratch (systems given through a
     // device array cannot be checked here) and the wavefront-major layout
     // must fit in the scratch
+    *done = false;
     bool aligned = L.dev == nullptr;
     for (int k = 0; k < nsys && aligned; k++) aligned = ((uintptr_t)L.s[k].ws % 16) == 0;
     const bool room = L.ws_cap == 0 || L.ws_cap >= msi_cluster_work_doubles(ND, L.nx, L.ny);
     const bool small = (long long)L.nx * L.ny < (1LL << 31);   // 32-bit cell indices in the passes
-    if (aligned && room && small) {
-        // fewest wavefront warps per CTA (one SM per warp) whose cluster fits
-        bool fits = false;
-        cudaError_t e = launch_cluster<ND, 1, 4>(L, nsys, st, &fits);
-        if (e != cudaSuccess || fits) return e;
-        e = launch_cluster<ND, 2, 2>(L, nsys, st, &fits);
-        if (e != cudaSuccess || fits) return e;
-    }
-    return launch_msi_generic(ND, L, nsys, st);
+    if (!(aligned && room && small)) return cudaSuccess;
+    // fewest wavefront warps per CTA (one SM per warp) whose cluster fits
+    cudaError_t e = launch_cluster<ND, 1, 4, TS>(L, nsys, st, done);
+    if (e != cudaSuccess || *done) return e;
+    return launch_cluster<ND, 2, 2, TS>(L, nsys, st, done);
 }
 
 cudaError_t launch_msi_warp(int nd, const MsiLaunch &L, int nsys, cudaStream_t st)
 {
-    return nd == 9 ? launch_nd<9>(L, nsys, st) : launch_nd<5>(L, nsys, st);
+    bool done = false;
+    cudaError_t e;
+    if (L.prec == 1)
+        e = nd == 9 ? launch_nd<9, float>(L, nsys, st, &done) : launch_nd<5, float>(L, nsys, st, &done);
+    else
+        e = nd == 9 ? launch_nd<9, double>(L, nsys, st, &done) : launch_nd<5, double>(L, nsys, st, &done);
+    if (e != cudaSuccess || done) return e;
+    return launch_msi_generic(nd, L, nsys, st);
 }
 
 }  // namespace m2d

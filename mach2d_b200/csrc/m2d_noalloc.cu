@@ -38,7 +38,7 @@ double *g_scratch_addr[kMaxDevices] = {nullptr};
 extern void m2d_set_last_error_msg(const char *);
 extern "C" int m2d_msi_solve_device_ws(int nd, int nx, int ny, int nitm, double tol, const double *d_a,
                                    const double *d_b, double *d_x, double *d_work, long work_doubles,
-                                   void *stream, int *d_nit, unsigned long long *d_times);
+                                   void *stream, int *d_nit, unsigned long long *d_times, int prec);
 
 extern "C" long m2d_msi_noalloc_max_cells(int nd)
 {
@@ -92,5 +92,5 @@ extern "C" int m2d_msi_solve_device_noalloc(int nd, int nx, int ny, int nitm, do
         work = g_scratch_addr[dev];
     }
     return m2d_msi_solve_device_ws(nd, nx, ny, nitm, tol, d_a, d_b, d_x, work, kNoallocScratchDoubles, stream,
-                                   d_nit, nullptr);
+                                   d_nit, nullptr, 0);
 }

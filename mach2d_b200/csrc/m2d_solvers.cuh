@@ -39,6 +39,8 @@ struct MsiLaunch {
                                // start, after LU, after r0, first forward, first backward,
                                // first residual, end
     size_t ws_cap;             // doubles each ws holds; 0 = at least msi_work_doubles()
+    int prec;                  // 0: FP64 throughout (bitwise reference); 1: FP32 factors and
+                               // sweeps inside the FP64 iteration (cluster kernel only)
 };
 
 // Largest ny the one-CTA wavefront kernel accepts (its shared-memory ring

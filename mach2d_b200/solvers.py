@@ -1,7 +1,8 @@
 """Linear-solver plug-ins with the interface of src/solvers/.
 
 `solvers_init` mirrors src/solvers/mod_solvers.f90:17-87 (selection by
-"MSI" / "TDMA", unknown option is an error); each class mirrors
+"MSI" / "TDMA", unknown option is an error; "MSI_MIXED" is this library's
+FP32-sweep variant); each class mirrors
 class_solver_*%init / %solve (src/solvers/mod_solver_msi.f90,
 mod_solver_tdma.f90).  `solve(a, b, sol)` updates `sol` in place like the
 Fortran `intent(inout)` argument.  a is a (k, nx*ny) float64 array whose row
@@ -37,6 +38,23 @@ class ClassSolverMSI5d(ClassSolverMSI9d):
     ndiag = 5
 
 
+class ClassSolverMSIMixed9d(ClassSolverMSI9d):
+    """No counterpart in the reference: MSI whose factorisation and sweeps run
+    in FP32 inside the FP64 iteration (m2d_msi9_solve_mixed)."""
+
+    def solve(self, a, b, sol):
+        import ctypes
+        nit = ctypes.c_int(0)
+        call("m2d_msi9_solve_mixed" if self.ndiag == 9 else "m2d_msi5_solve_mixed",
+             self.nx, self.ny, self.nitm, self.tol, _mat(a, self.ndiag, self.nx * self.ny),
+             _vec(b), _vec(sol), nit)
+        self.nit = nit.value
+
+
+class ClassSolverMSIMixed5d(ClassSolverMSIMixed9d):
+    ndiag = 5
+
+
 class ClassSolverTDMA9d:
     """class_solver_tdma9d (src/solvers/mod_solver_tdma.f90:76-100)."""
 
@@ -65,6 +83,9 @@ def solvers_init(nx, ny, ksolver, nitm_u, nitm_p, tol_u, tol_p):
                 ClassSolverMSI9d().init(nx, ny, nitm_u, tol_u))
     if k == "TDMA":
         return ClassSolverTDMA5d().init(nx, ny, nitm_p), ClassSolverTDMA9d().init(nx, ny, nitm_u)
+    if k == "MSI_MIXED":
+        return (ClassSolverMSIMixed5d().init(nx, ny, nitm_p, tol_p),
+                ClassSolverMSIMixed9d().init(nx, ny, nitm_u, tol_u))
     raise ValueError(f"solvers_init: Unkown option: {k}")
 
 
