@@ -230,6 +230,23 @@ int m2d_check_mass_conservation(const int *nx, const int *ny, const double *dt,
     const double *roa, const double *ron, const double *roe, const double *Uce,
     const double *Vcn, double *res);                                               /* :1833-1880 */
 
+/* ---- Baldwin-Lomax eddy viscosity: src/equations/blomax.f90 -------------
+ * set/get_blomax_coefficients (:25-62), initialize_blomax (:67-80; the
+ * vorticity metrics of :83-115 are evaluated inside the kernel, so this only
+ * checks its arguments), get_eddy_viscosity_blomax (:285-395: vtp at the real
+ * volumes, ghost entries left as passed), get_eddy_viscosity_fictitious
+ * (:397-490).  The reference never calls the model from its main loop. */
+int m2d_set_blomax_coefficients(const double *kappa, const double *Aop, const double *alpha,
+                                const double *Ccp, const double *Ckleb, const double *Cwk);
+int m2d_get_blomax_coefficients(double *kappa, double *Aop, double *alpha, double *Ccp,
+                                double *Ckleb, double *Cwk);
+int m2d_initialize_blomax(const int *nx, const int *ny, const double *x, const double *y);
+int m2d_get_eddy_viscosity_blomax(const int *nx, const int *ny, const double *x, const double *y,
+    const double *xp, const double *yp, const double *xk, const double *yk, const double *Jp,
+    const double *Jn, const double *vln, const double *ro, const double *ron, const double *u,
+    const double *v, double *vtp);
+int m2d_get_eddy_viscosity_fictitious(const int *nx, const int *ny, double *phi);
+
 /* ---- internal-flow plug-in: src/user/internal_flow/mod_intflow.f90 ------- */
 int m2d_intflow_set_bcu(const int *nx, const int *ny, const int *modvis, const double *x,
     const double *xp, const double *xk, const double *yk, const double *u, const double *v,

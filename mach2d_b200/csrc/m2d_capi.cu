@@ -11,6 +11,7 @@
 #include <vector>
 #include "m2d_fields.cuh"
 #include "m2d_solvers.cuh"
+#include "m2d_blomax.cuh"
 #include "../../include/mach2d_b200.h"
 
 static thread_local std::string g_last_error;
@@ -695,6 +696,60 @@ int m2d_intflow_time_cycle_update(const int *nx, const int *ny, const double *x,
     Params q; memset(&q, 0, sizeof q);
     q.gamma = *gamma; q.Rg = *Rg; q.p0 = *P0; q.T0 = *T0;
     return s.finish(launch_inlet_update(f, q, 0));
+}
+
+/* ---- Baldwin-Lomax eddy viscosity: src/equations/blomax.f90 ------------- */
+static m2d::BlConst g_blomax;   // the module's coefficients (blomax.f90:5-10)
+
+int m2d_set_blomax_coefficients(const double *kappa, const double *Aop, const double *alpha,
+                                const double *Ccp, const double *Ckleb, const double *Cwk)
+{
+    if (!kappa || !Aop || !alpha || !Ccp || !Ckleb || !Cwk) return fail(ST_ARG, "set_blomax_coefficients: null argument");
+    g_blomax.kappa = *kappa; g_blomax.Aop = *Aop; g_blomax.alpha = *alpha;
+    g_blomax.Ccp = *Ccp; g_blomax.Ckleb = *Ckleb; g_blomax.Cwk = *Cwk;
+    return ST_OK;
+}
+
+int m2d_get_blomax_coefficients(double *kappa, double *Aop, double *alpha, double *Ccp, double *Ckleb,
+                                double *Cwk)
+{
+    if (!kappa || !Aop || !alpha || !Ccp || !Ckleb || !Cwk) return fail(ST_ARG, "get_blomax_coefficients: null argument");
+    *kappa = g_blomax.kappa; *Aop = g_blomax.Aop; *alpha = g_blomax.alpha;
+    *Ccp = g_blomax.Ccp; *Ckleb = g_blomax.Ckleb; *Cwk = g_blomax.Cwk;
+    return ST_OK;
+}
+
+int m2d_initialize_blomax(const int *nx, const int *ny, const double *x, const double *y)
+{
+    CHK;
+    if (!x || !y) return fail(ST_ARG, "initialize_blomax: null argument");
+    return ST_OK;   // the vorticity metrics are evaluated inside the kernel
+}
+
+int m2d_get_eddy_viscosity_blomax(const int *nx, const int *ny, const double *x, const double *y,
+    const double *xp, const double *yp, const double *xk, const double *yk, const double *Jp,
+    const double *Jn, const double *vln, const double *ro, const double *ron, const double *u,
+    const double *v, double *vtp)
+{
+    CHK;
+    if (*ny < 5) return fail(ST_ARG, "get_eddy_viscosity_blomax: ny < 5");
+    Stage s; size_t N = ND_;
+    const double *dx = s.in(x, N), *dy = s.in(y, N), *dxp = s.in(xp, N), *dyp = s.in(yp, N);
+    const double *dxk = s.in(xk, N), *dyk = s.in(yk, N), *dJp = s.in(Jp, N), *dJn = s.in(Jn, N);
+    const double *dvln = s.in(vln, N), *dro = s.in(ro, N), *dron = s.in(ron, N);
+    const double *du = s.in(u, N), *dv = s.in(v, N);
+    double *dvtp = s.inout(vtp, N);
+    if (s.status) return s.status;
+    return s.finish(launch_blomax(*nx, *ny, g_blomax, dx, dy, dxp, dyp, dxk, dyk, dJp, dJn, dvln, dro, dron,
+                                  du, dv, dvtp, 0));
+}
+
+int m2d_get_eddy_viscosity_fictitious(const int *nx, const int *ny, double *phi)
+{
+    CHK; Stage s; size_t N = ND_;
+    double *d = s.inout(phi, N);
+    if (s.status) return s.status;
+    return s.finish(launch_blomax_fictitious(*nx, *ny, d, 0));
 }
 
 }  // extern "C"

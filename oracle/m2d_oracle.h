@@ -257,6 +257,16 @@ int  orc_iterate(orc_state *s, orc_report *rep);
 long orc_field(orc_state *s, const char *name, double **ptr);
 double orc_scalar(const orc_state *s, const char *name);
 
+/* ---- Baldwin-Lomax: src/equations/blomax.f90 (blomax.c) ---------------- */
+void orc_set_blomax_coefficients(double kappa, double Aop, double alpha, double Ccp, double Ckleb,
+                                 double Cwk);
+/* work: 9 (ny-2) doubles */
+void orc_get_eddy_viscosity_blomax(int nx, int ny, const double *x, const double *y, const double *xp,
+                                   const double *yp, const double *xk, const double *yk, const double *Jp,
+                                   const double *Jn, const double *vln, const double *ro, const double *ron,
+                                   const double *u, const double *v, double *vtp, double *work);
+void orc_get_eddy_viscosity_fictitious(int nx, int ny, double *phi);
+
 #ifdef __cplusplus
 }
 #endif

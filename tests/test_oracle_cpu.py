@@ -108,3 +108,32 @@ def test_total_enthalpy_is_conserved_for_euler():
     interior[1:-1, 1:-1] = True
     h = cp * T + (u * u + v * v) / 2
     assert np.max(np.abs(h.reshape(ny, nx)[interior] / H - 1)) < 1e-13
+
+
+def _cartesian_column_case(nx=12, ny=30):
+    """Uniform Cartesian grid (unit Jacobian metrics) with a wall at the north."""
+    xs = np.arange(nx, dtype=float) * 0.01
+    ys = np.arange(ny, dtype=float) * 0.001
+    X, Y = np.meshgrid(xs, ys)                       # corners (NE corner of each volume)
+    xp, yp = X - 0.005, Y - 0.0005
+    f = dict(x=X.reshape(-1).copy(), y=Y.reshape(-1).copy(), xp=xp.reshape(-1).copy(),
+             yp=yp.reshape(-1).copy(), xk=np.full(nx * ny, 0.01), yk=np.zeros(nx * ny),
+             Jp=np.full(nx * ny, 1.0 / (0.01 * 0.001)), Jn=np.full(nx * ny, 1.0 / (0.01 * 0.001)),
+             vln=np.full(nx * ny, 1.8e-5), ro=np.full(nx * ny, 1.2), ron=np.full(nx * ny, 1.2),
+             v=np.zeros(nx * ny))
+    return nx, ny, f
+
+
+def test_blomax_oracle_zero_for_uniform_flow_positive_for_shear():
+    from _oracle import call as orc
+    nx, ny, f = _cartesian_column_case()
+    keys = ("x", "y", "xp", "yp", "xk", "yk", "Jp", "Jn", "vln", "ro", "ron", "u", "v")
+    f["u"] = np.full(nx * ny, 50.0)
+    vt = np.zeros(nx * ny)
+    orc("get_eddy_viscosity_blomax", nx, ny, *[f[k] for k in keys], vt, np.zeros(9 * (ny - 2)))
+    assert np.all(vt == 0.0)
+    d = (f["y"].reshape(ny, nx)[ny - 2:ny - 1, :] - f["yp"].reshape(ny, nx)).clip(0) + 1e-5
+    f["u"] = (50.0 * np.tanh(d / 0.005)).reshape(-1).copy()
+    orc("get_eddy_viscosity_blomax", nx, ny, *[f[k] for k in keys], vt, np.zeros(9 * (ny - 2)))
+    real = vt.reshape(ny, nx)[1:-1, 1:-1]
+    assert np.all(real >= 0.0) and np.max(real) > 0.0
