@@ -37,13 +37,15 @@ HBM_FALLBACK_GBS = 6650.0
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nxr", type=int, default=NXR)
     ap.add_argument("--nyr", type=int, default=NYR)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch", type=int, default=8,
+                    help="instances of the same workload for the batch throughput figure (0: skip)")
     return ap.parse_args()
 
 
@@ -310,6 +312,23 @@ def run_ours(args):
         except Exception:
             traffic = None
 
+    batch = None
+    if world == 1 and args.batch > 0:
+        from mach2d_b200.simplec import Batch
+        b = Batch([make_case(args.nxr, args.nyr) for _ in range(args.batch)], device=local)
+        b.iterate(max(1, args.warmup))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        bsteps = max(3, args.steps // 2)
+        b.iterate(bsteps)
+        torch.cuda.synchronize()
+        bdt = time.perf_counter() - t0
+        batch = {"instances": args.batch, "steps": bsteps,
+                 "value": args.batch * bsteps * args.nxr * args.nyr / bdt, "unit": "cell-updates/s",
+                 "timing": "host wall clock around m2d_batch_iterate with device synchronisation",
+                 "note": "independent instances of the same workload, one context and stream each"}
+        b.close()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, nsamp, secs = cpu_sample(args, args.cpu_seconds)
@@ -333,6 +352,7 @@ def run_ours(args):
                          "traffic": traffic, "algorithmic_bytes_per_launch": alg,
                          "launch_ms": avg_ms, "iterations_per_launch": nit},
             "cpu_baseline": cpu,
+            "batch": batch,
             "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)

@@ -338,6 +338,23 @@ int m2d_integrals(m2d_ctx *ctx, double *fmi, double *fme, double *Fd, double *Cd
 int m2d_ctx_stream(const m2d_ctx *ctx, void **stream);
 int m2d_ctx_field_device(m2d_ctx *ctx, const char *name, double **dptr, long *n);
 
+/* ---- batches of instances (no counterpart in the reference) ------------
+ * n independent nozzle instances on one GPU, each a full context with its
+ * own stream.  m2d_batch_iterate runs `iters` outer iterations of every
+ * instance with `workers` host threads (<= 0: min(n, 16)), so that several
+ * instances have kernels in flight at once; reps[k] (may be NULL) receives
+ * instance k's last report.  An instance whose iteration fails stops there
+ * (m2d_batch_status); the call returns the first failure.  Each instance's
+ * results equal those of running it alone.  m2d_batch_ctx gives an
+ * instance's context for fields and integrals. */
+typedef struct m2d_batch m2d_batch;
+int m2d_batch_create(const m2d_case *cases, int n, int device, int workers, m2d_batch **out);
+int m2d_batch_size(const m2d_batch *b, int *n);
+int m2d_batch_ctx(m2d_batch *b, int k, m2d_ctx **ctx);
+int m2d_batch_iterate(m2d_batch *b, int iters, m2d_report *reps);
+int m2d_batch_status(const m2d_batch *b, int k, int *status);
+int m2d_batch_destroy(m2d_batch *b);
+
 #ifdef __cplusplus
 }
 #endif

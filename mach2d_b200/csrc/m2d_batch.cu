@@ -1,0 +1,113 @@
+// m2d_batch.cu -- many nozzle instances advanced together on one GPU.
+//
+// No counterpart in the reference (one instance per process there).  Each
+// instance is a full context (own arena and non-blocking stream), so
+// instances never share device state.  A single instance keeps at most the
+// two MSI9 clusters busy (ny/32 SMs each), leaving most of the 148 SMs idle;
+// a batch runs W host worker threads, each advancing its share of the
+// instances, so up to W instances have kernels in flight at once.  Results
+// of every instance are bitwise identical to running it alone.
+#include <string>
+#include <thread>
+#include <vector>
+#include "../../include/mach2d_b200.h"
+
+extern void m2d_set_last_error_msg(const char *);
+
+struct m2d_batch {
+    std::vector<m2d_ctx *> ctx;
+    std::vector<int> status;   // first non-zero status of each instance (it stops there)
+    int workers = 1;
+};
+
+extern "C" int m2d_batch_create(const m2d_case *cases, int n, int device, int workers, m2d_batch **out)
+{
+    if (!cases || n < 1 || !out) {
+        m2d_set_last_error_msg("m2d_batch_create: bad arguments");
+        return M2D_ERR_ARG;
+    }
+    *out = nullptr;
+    m2d_batch *b = new m2d_batch;
+    b->workers = workers > 0 ? workers : (n < 16 ? n : 16);
+    if (b->workers > n) b->workers = n;
+    b->ctx.assign(n, nullptr);
+    b->status.assign(n, M2D_OK);
+    for (int k = 0; k < n; k++) {
+        const int rc = m2d_create(&cases[k], device, &b->ctx[k]);
+        if (rc != M2D_OK) {
+            const std::string msg = std::string("m2d_batch_create: instance ") + std::to_string(k) + ": " +
+                                    m2d_last_error();
+            for (int q = 0; q < k; q++) m2d_destroy(b->ctx[q]);
+            delete b;
+            m2d_set_last_error_msg(msg.c_str());
+            return rc;
+        }
+    }
+    *out = b;
+    return M2D_OK;
+}
+
+extern "C" int m2d_batch_size(const m2d_batch *b, int *n)
+{
+    if (!b || !n) return M2D_ERR_ARG;
+    *n = (int)b->ctx.size();
+    return M2D_OK;
+}
+
+extern "C" int m2d_batch_ctx(m2d_batch *b, int k, m2d_ctx **ctx)
+{
+    if (!b || !ctx || k < 0 || k >= (int)b->ctx.size()) return M2D_ERR_ARG;
+    *ctx = b->ctx[k];
+    return M2D_OK;
+}
+
+extern "C" int m2d_batch_iterate(m2d_batch *b, int iters, m2d_report *reps)
+{
+    if (!b || iters < 0) {
+        m2d_set_last_error_msg("m2d_batch_iterate: bad arguments");
+        return M2D_ERR_ARG;
+    }
+    const int n = (int)b->ctx.size(), W = b->workers;
+    std::vector<std::string> msg(n);
+    auto work = [&](int w) {
+        for (int it = 0; it < iters; it++) {
+            for (int k = w; k < n; k += W) {
+                if (b->status[k] != M2D_OK) continue;
+                m2d_report r;
+                const int rc = m2d_iterate(b->ctx[k], &r);
+                if (reps) reps[k] = r;
+                if (rc != M2D_OK) {
+                    b->status[k] = rc;
+                    msg[k] = m2d_last_error();
+                }
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int w = 1; w < W; w++) pool.emplace_back(work, w);
+    work(0);
+    for (auto &t : pool) t.join();
+    for (int k = 0; k < n; k++) {
+        if (b->status[k] != M2D_OK) {
+            const std::string m = std::string("instance ") + std::to_string(k) + ": " + msg[k];
+            m2d_set_last_error_msg(m.c_str());
+            return b->status[k];
+        }
+    }
+    return M2D_OK;
+}
+
+extern "C" int m2d_batch_status(const m2d_batch *b, int k, int *status)
+{
+    if (!b || !status || k < 0 || k >= (int)b->ctx.size()) return M2D_ERR_ARG;
+    *status = b->status[k];
+    return M2D_OK;
+}
+
+extern "C" int m2d_batch_destroy(m2d_batch *b)
+{
+    if (!b) return M2D_OK;
+    for (m2d_ctx *c : b->ctx) m2d_destroy(c);
+    delete b;
+    return M2D_OK;
+}

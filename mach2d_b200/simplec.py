@@ -155,3 +155,65 @@ class Simplec:
         if name in ("Tbn", "Tbs"):
             return self.nx
         return N
+
+
+class _BorrowedSimplec(Simplec):
+    """A view of one instance of a Batch (the batch owns the context)."""
+
+    def __init__(self, ctx, nx, ny, case):
+        self.case = case
+        self._ctx = ctx
+        self.nx, self.ny = nx, ny
+
+    def close(self):
+        self._ctx = ctypes.c_void_p()
+
+
+class Batch:
+    """Many nozzle instances on one GPU (m2d_batch_*): each a full context on
+    its own stream, advanced together by `workers` host threads."""
+
+    def __init__(self, cases, device=0, workers=0):
+        self.cases = list(cases)
+        n = len(self.cases)
+        arr = (Case * n)(*self.cases)
+        self._b = ctypes.c_void_p()
+        L = lib()
+        L.m2d_batch_create.argtypes = [ctypes.POINTER(Case), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                       ctypes.POINTER(ctypes.c_void_p)]
+        check(L.m2d_batch_create(arr, n, int(device), int(workers), ctypes.byref(self._b)))
+        L.m2d_batch_ctx.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+        L.m2d_dims.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+        self.instances = []
+        for k in range(n):
+            c = ctypes.c_void_p()
+            check(L.m2d_batch_ctx(self._b, k, ctypes.byref(c)))
+            nx, ny = ctypes.c_int(), ctypes.c_int()
+            check(L.m2d_dims(c, ctypes.byref(nx), ctypes.byref(ny)))
+            self.instances.append(_BorrowedSimplec(c, nx.value, ny.value, self.cases[k]))
+
+    def __len__(self):
+        return len(self.instances)
+
+    def iterate(self, iters=1):
+        """Runs `iters` outer iterations of every instance; returns the last
+        report of each."""
+        n = len(self.instances)
+        reps = (Report * n)()
+        L = lib()
+        L.m2d_batch_iterate.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(Report)]
+        check(L.m2d_batch_iterate(self._b, int(iters), reps))
+        return list(reps)
+
+    def close(self):
+        if self._b:
+            for s in self.instances:
+                s.close()
+            lib().m2d_batch_destroy(self._b)
+            self._b = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

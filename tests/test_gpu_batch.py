@@ -1,0 +1,68 @@
+"""Batches of nozzle instances (m2d_batch_*): no counterpart in the reference.
+
+Each instance is a full context on its own stream, so the batch must give
+every instance exactly the results it gets when run alone (same kernels, same
+order of operations), whatever the number of host workers; and a failing
+instance must stop alone without disturbing the others.
+"""
+import numpy as np
+import pytest
+
+from mach2d_b200 import M2DError
+from mach2d_b200.simplec import Batch, Simplec, euler_cosine_case, n01_case
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("u", "v", "p", "T", "ro", "Uce", "Vcn")
+REPORT = ("it", "dt", "norm", "normpl", "rmass", "fmi", "fme", "Fd", "itp_used")
+
+
+def _cases():
+    # uneven grids and operating points, as in the batched workload
+    return [euler_cosine_case(64, 32, p0=8.0e5, T0=900.0),
+            euler_cosine_case(96, 40, Rin=2.2, Rout=1.6),
+            n01_case(),
+            euler_cosine_case(130, 48, Lc=1.5, Ld=3.0, p0=2.0e6, T0=1200.0),
+            euler_cosine_case(48, 32)]
+
+
+@pytest.mark.parametrize("workers", [1, 3, 0])
+def test_batch_instances_equal_solo_runs(workers):
+    iters = 12
+    b = Batch(_cases(), workers=workers)
+    reps = b.iterate(iters)
+    for k, case in enumerate(_cases()):
+        solo = Simplec(case)
+        for _ in range(iters):
+            r = solo.iterate()
+        for c in REPORT:
+            assert getattr(reps[k], c) == getattr(r, c), (k, c)
+        for f in FIELDS:
+            assert np.array_equal(b.instances[k].field(f), solo.field(f)), (k, f)
+        assert b.instances[k].integrals()[3] == solo.integrals()[3]
+        solo.close()
+    b.close()
+
+
+def test_batch_failure_stays_in_its_instance():
+    b = Batch(_cases()[:3], workers=2)
+    b.iterate(1)
+    g = b.instances[2]                                  # the N01 deck
+    u = g.field("u")
+    u[g.nx * 5 + 7] = np.nan
+    g.set_field("u", u)
+    with pytest.raises(M2DError) as e:
+        b.iterate(3)
+    assert e.value.code == 3 and "instance 2" in str(e.value)
+    import ctypes
+    from mach2d_b200._lib import lib
+    st = ctypes.c_int()
+    for k, want in ((0, 0), (1, 0), (2, 3)):
+        lib().m2d_batch_status(b._b, k, ctypes.byref(st))
+        assert st.value == want, (k, st.value)
+    reps = None
+    with pytest.raises(M2DError):
+        reps = b.iterate(2)                             # instance 2 stays stopped, others go on
+    assert reps is None
+    assert b.instances[0].scalar("it") == 6 and b.instances[1].scalar("it") == 6
+    b.close()
