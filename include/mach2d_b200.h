@@ -280,9 +280,56 @@ int m2d_intflow_time_cycle_update(const int *nx, const int *ny, const double *x,
     const double *P0, const double *T0, double *uin, double *vin, double *pin, double *Tin,
     double *Mw, double *plin, double *pina, double *p);
 
+/* ---- thermophysical properties: src/thermophysical/ ----------------------
+ * The gas-mixture model (class_thermophysical_mixture,
+ * mod_class_thermophysical_mixture.f90): cp(T) from 5-coefficient
+ * polynomials per species (below / above 1000 K), mu(T) and k(T) from
+ * exp(a ln T + b/T + c/T^2 + d) per species combined by Wilke's rule.
+ * m2d_mixture_init (init, :56-224) takes the species of the mixture
+ * (fractions <= 1e-8 are skipped, as the reference does): base 0 = molar,
+ * 1 = mass fractions; Mi in kg/mol; cpi ngs x 10, mui and kpi ngs x 8,
+ * species-major, in the database's coefficient order.  It fills Xi, Yi, Ri
+ * and Rg = Ru / Mg, and returns M2D_ERR_ARG if the fractions do not sum to 1
+ * within 10 epsilon.  The field routines below take the mixture in place of
+ * the reference's thermomodel pointer. */
+#define M2D_MAX_SPECIES 8
+typedef struct m2d_mixture {
+    int ngs;                                         /* gaseous species */
+    double Rg;                                       /* J/(kg K) */
+    double Xi[M2D_MAX_SPECIES], Yi[M2D_MAX_SPECIES]; /* molar and mass fractions */
+    double Mi[M2D_MAX_SPECIES], Ri[M2D_MAX_SPECIES]; /* kg/mol, Ru/Mi */
+    double cpi[M2D_MAX_SPECIES][10];
+    double mui[M2D_MAX_SPECIES][8];
+    double kpi[M2D_MAX_SPECIES][8];
+} m2d_mixture;
+int m2d_mixture_init(int base, int ngs, const double *fractions, const double *Mi,
+                     const double *cpi, const double *mui, const double *kpi, m2d_mixture *out);
+/* point values: cp, mu, kp, gm (mixture functions :227-272); NULL outputs skipped */
+int m2d_mixture_eval(const m2d_mixture *mix, double T, double *cp, double *mu, double *kp,
+                     double *gm);
+/* mod_thermophysical.f90 field routines (:79-509) and the boundary averages
+ * of src/util/mod_field_operations.f90:1-110 (get_north/south/east/west_
+ * boundary_field in one call) */
+int m2d_set_cp(const m2d_mixture *mix, const int *nx, const int *ny, const double *Tbn,
+    const double *Tbs, const double *Tbe, const double *Tbw, const double *T, double *cp);
+int m2d_set_gamma(const int *nx, const int *ny, const double *Rg, const double *cp, double *gcp);
+int m2d_set_laminar_viscosity_at_nodes(const m2d_mixture *mix, const int *nx, const int *ny,
+    const double *T, double *vlp);
+int m2d_set_thermal_conductivity_at_nodes(const m2d_mixture *mix, const int *nx, const int *ny,
+    const double *T, double *kp);
+int m2d_get_laminar_viscosity_at_faces(const m2d_mixture *mix, const int *nx, const int *ny,
+    const double *Tbn, const double *Tbs, const double *Tbe, const double *Tbw,
+    const double *vlp, double *vle, double *vln);
+int m2d_get_thermal_conductivity_at_faces(const m2d_mixture *mix, const int *nx, const int *ny,
+    const double *Tbn, const double *Tbs, const double *Tbe, const double *Tbw,
+    const double *kp, double *ke, double *kn);
+int m2d_get_boundary_fields(const int *nx, const int *ny, const double *F, double *Fbn,
+    double *Fbs, double *Fbe, double *Fbw);
+
 /* ===================== 2. device-resident SIMPLEC context =================
  * Mirrors the set-up and the `it` loop body of src/mach2d_main.f90:25-445 for
- * internal flow with constant thermophysical properties. */
+ * internal flow, with the CONSTANT (ktm = 0) or MIXTURE (ktm = 1)
+ * thermophysical model. */
 
 typedef struct m2d_case {
     int geom;                               /* 0: C01 cosine nozzle, 1: N01 nozzle */

@@ -71,7 +71,7 @@ def call(name, *args):
             v = ctypes.c_double(float(a))
             keep.append(v)
             conv.append(ctypes.byref(v))
-        elif isinstance(a, ctypes._SimpleCData):
+        elif isinstance(a, (ctypes._SimpleCData, ctypes.Structure)):
             conv.append(ctypes.byref(a))
         else:
             raise TypeError(f"unsupported argument {type(a)}")

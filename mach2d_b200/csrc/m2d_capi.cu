@@ -12,6 +12,8 @@
 #include "m2d_fields.cuh"
 #include "m2d_solvers.cuh"
 #include "m2d_blomax.cuh"
+#include "m2d_thermo.cuh"
+#include <cmath>
 #include "../../include/mach2d_b200.h"
 
 static thread_local std::string g_last_error;
@@ -751,5 +753,133 @@ int m2d_get_eddy_viscosity_fictitious(const int *nx, const int *ny, double *phi)
     if (s.status) return s.status;
     return s.finish(launch_blomax_fictitious(*nx, *ny, d, 0));
 }
+
+/* ---- thermophysical model: src/thermophysical/ ------------------------- */
+static const m2d_mixture *mixture_in(Stage &s, const m2d_mixture *h)
+{
+    if (!h) { s.status = s.status ? s.status : ST_ARG; m2d_set_last_error_msg("null mixture"); return nullptr; }
+    double *d = s.alloc(sizeof(m2d_mixture) / sizeof(double) + 1);
+    if (d && cudaMemcpy(d, h, sizeof(m2d_mixture), cudaMemcpyHostToDevice) != cudaSuccess) s.status = ST_CUDA;
+    return (const m2d_mixture *)d;
+}
+
+int m2d_mixture_init(int base, int ngs, const double *fractions, const double *Mi, const double *cpi,
+                     const double *mui, const double *kpi, m2d_mixture *out)
+{
+    // class_thermophysical_mixture%init, mod_class_thermophysical_mixture.f90:56-224
+    if (!fractions || !Mi || !cpi || !mui || !kpi || !out || ngs < 1 || (base != 0 && base != 1))
+        return fail(ST_ARG, "mixture_init: bad arguments");
+    m2d_mixture m;
+    memset(&m, 0, sizeof m);
+    const double Ru = 8.31451000e+00;
+    for (int k = 0; k < ngs; k++) {
+        if (!(fractions[k] > 1.0e-8)) continue;          // species below 1e-8 are left out
+        if (m.ngs == M2D_MAX_SPECIES) return fail(ST_ARG, "mixture_init: more than 8 species");
+        const int q = m.ngs++;
+        (base == 0 ? m.Xi : m.Yi)[q] = fractions[k];
+        m.Mi[q] = Mi[k];
+        for (int c = 0; c < 10; c++) m.cpi[q][c] = cpi[k * 10 + c];
+        for (int c = 0; c < 8; c++) { m.mui[q][c] = mui[k * 8 + c]; m.kpi[q][c] = kpi[k * 8 + c]; }
+    }
+    if (m.ngs == 0) return fail(ST_ARG, "mixture_init: no species");
+    double sum = 0.0;
+    for (int q = 0; q < m.ngs; q++) sum = sum + (base == 0 ? m.Xi[q] : m.Yi[q]);
+    if (std::fabs(1.0 - sum) > 2.220446049250313e-16 * 10.0)
+        return fail(ST_ARG, "mixture_init: the fractions do not sum to one");
+    double Mg = 0.0;
+    if (base == 0) {
+        for (int q = 0; q < m.ngs; q++) Mg = Mg + m.Xi[q] * m.Mi[q];
+        for (int q = 0; q < m.ngs; q++) m.Yi[q] = m.Xi[q] * m.Mi[q] / Mg;
+    } else {
+        double t = 0.0;
+        for (int q = 0; q < m.ngs; q++) t = t + m.Yi[q] / m.Mi[q];
+        for (int q = 0; q < m.ngs; q++) m.Xi[q] = (m.Yi[q] / m.Mi[q]) / t;
+        for (int q = 0; q < m.ngs; q++) Mg = Mg + m.Xi[q] * m.Mi[q];
+    }
+    for (int q = 0; q < m.ngs; q++) m.Ri[q] = Ru / m.Mi[q];
+    m.Rg = Ru / Mg;
+    *out = m;
+    return ST_OK;
+}
+
+int m2d_mixture_eval(const m2d_mixture *mix, double T, double *cp, double *mu, double *kp, double *gm)
+{
+    if (!mix) return fail(ST_ARG, "mixture_eval: null mixture");
+    if (cp) *cp = m2d::mix_cp(*mix, T);
+    if (mu) *mu = m2d::mix_mu(*mix, T);
+    if (kp) *kp = m2d::mix_kp(*mix, T);
+    if (gm) *gm = m2d::mix_gm(*mix, T);
+    return ST_OK;
+}
+
+int m2d_get_boundary_fields(const int *nx, const int *ny, const double *F, double *Fbn, double *Fbs,
+                            double *Fbe, double *Fbw)
+{
+    CHK; Stage s; size_t N = ND_, X = (size_t)*nx, Y = (size_t)*ny;
+    const double *dF = s.in(F, N);
+    double *dn = s.inout(Fbn, X), *ds = s.inout(Fbs, X), *de = s.inout(Fbe, Y), *dw = s.inout(Fbw, Y);
+    if (s.status) return s.status;
+    return s.finish(launch_boundary_fields(*nx, *ny, dF, dn, ds, de, dw, 0));
+}
+
+int m2d_set_cp(const m2d_mixture *mix, const int *nx, const int *ny, const double *Tbn,
+    const double *Tbs, const double *Tbe, const double *Tbw, const double *T, double *cp)
+{
+    CHK; Stage s; size_t N = ND_, X = (size_t)*nx, Y = (size_t)*ny;
+    const m2d_mixture *dm = mixture_in(s, mix);
+    const double *dn = s.in(Tbn, X), *ds = s.in(Tbs, X), *de = s.in(Tbe, Y), *dw = s.in(Tbw, Y), *dT = s.in(T, N);
+    double *dcp = s.inout(cp, N);
+    if (s.status) return s.status;
+    return s.finish(launch_set_cp(*nx, *ny, dm, dn, ds, de, dw, dT, dcp, 0));
+}
+
+int m2d_set_gamma(const int *nx, const int *ny, const double *Rg, const double *cp, double *gcp)
+{
+    CHK;
+    if (!Rg) return fail(ST_ARG, "set_gamma: null Rg");
+    Stage s; size_t N = ND_;
+    const double *dcp = s.in(cp, N);
+    double *dg = s.inout(gcp, N);
+    if (s.status) return s.status;
+    return s.finish(launch_set_gamma(*nx, *ny, *Rg, dcp, dg, 0));
+}
+
+static int transport_nodes(const m2d_mixture *mix, const int *nx, const int *ny, bool visc, const double *T,
+                           double *phip)
+{
+    CHK; Stage s; size_t N = ND_;
+    const m2d_mixture *dm = mixture_in(s, mix);
+    const double *dT = s.in(T, N);
+    double *dp = s.inout(phip, N);
+    if (s.status) return s.status;
+    return s.finish(launch_transport_nodes(*nx, *ny, dm, visc, dT, dp, 0));
+}
+int m2d_set_laminar_viscosity_at_nodes(const m2d_mixture *mix, const int *nx, const int *ny,
+    const double *T, double *vlp)
+{ return transport_nodes(mix, nx, ny, true, T, vlp); }
+int m2d_set_thermal_conductivity_at_nodes(const m2d_mixture *mix, const int *nx, const int *ny,
+    const double *T, double *kp)
+{ return transport_nodes(mix, nx, ny, false, T, kp); }
+
+static int transport_faces(const m2d_mixture *mix, const int *nx, const int *ny, bool visc, const double *Tbn,
+                           const double *Tbs, const double *Tbe, const double *Tbw, const double *phip,
+                           double *phie, double *phin)
+{
+    CHK; Stage s; size_t N = ND_, X = (size_t)*nx, Y = (size_t)*ny;
+    const m2d_mixture *dm = mixture_in(s, mix);
+    const double *dn = s.in(Tbn, X), *ds = s.in(Tbs, X), *de = s.in(Tbe, Y), *dw = s.in(Tbw, Y);
+    const double *dp = s.in(phip, N);
+    double *dpe = s.inout(phie, N), *dpn = s.inout(phin, N);
+    if (s.status) return s.status;
+    return s.finish(launch_transport_faces(*nx, *ny, dm, visc, dn, ds, de, dw, dp, dpe, dpn, 0));
+}
+int m2d_get_laminar_viscosity_at_faces(const m2d_mixture *mix, const int *nx, const int *ny,
+    const double *Tbn, const double *Tbs, const double *Tbe, const double *Tbw,
+    const double *vlp, double *vle, double *vln)
+{ return transport_faces(mix, nx, ny, true, Tbn, Tbs, Tbe, Tbw, vlp, vle, vln); }
+int m2d_get_thermal_conductivity_at_faces(const m2d_mixture *mix, const int *nx, const int *ny,
+    const double *Tbn, const double *Tbs, const double *Tbe, const double *Tbw,
+    const double *kp, double *ke, double *kn)
+{ return transport_faces(mix, nx, ny, false, Tbn, Tbs, Tbe, Tbw, kp, ke, kn); }
 
 }  // extern "C"

@@ -267,6 +267,32 @@ void orc_get_eddy_viscosity_blomax(int nx, int ny, const double *x, const double
                                    const double *u, const double *v, double *vtp, double *work);
 void orc_get_eddy_viscosity_fictitious(int nx, int ny, double *phi);
 
+/* ---- thermophysical model (thermo.c): mod_class_thermophysical_mixture.f90,
+ *      mod_thermophysical.f90, mod_field_operations.f90.  orc_mixture has
+ *      the layout of the library's m2d_mixture. */
+#define ORC_MAX_SPECIES 8
+typedef struct orc_mixture {
+    int ngs;
+    double Rg;
+    double Xi[ORC_MAX_SPECIES], Yi[ORC_MAX_SPECIES], Mi[ORC_MAX_SPECIES], Ri[ORC_MAX_SPECIES];
+    double cpi[ORC_MAX_SPECIES][10], mui[ORC_MAX_SPECIES][8], kpi[ORC_MAX_SPECIES][8];
+} orc_mixture;
+int orc_mixture_init(int base, int ngs, const double *fractions, const double *Mi, const double *cpi,
+                     const double *mui, const double *kpi, orc_mixture *out);
+double orc_mix_cp(const orc_mixture *m, double T);
+double orc_mix_mu(const orc_mixture *m, double T);
+double orc_mix_kp(const orc_mixture *m, double T);
+double orc_mix_gm(const orc_mixture *m, double T);
+void orc_get_boundary_fields(int nx, int ny, const double *F, double *Fbn, double *Fbs, double *Fbe,
+                             double *Fbw);
+void orc_set_cp(const orc_mixture *m, int nx, int ny, const double *Tbn, const double *Tbs, const double *Tbe,
+                const double *Tbw, const double *T, double *cp);
+void orc_set_gamma(int nx, int ny, double Rg, const double *cp, double *gcp);
+/* visc = 1: laminar viscosity; 0: thermal conductivity */
+void orc_transport_nodes(const orc_mixture *m, int nx, int ny, int visc, const double *T, double *phip);
+void orc_transport_faces(const orc_mixture *m, int nx, int ny, int visc, const double *Tbn, const double *Tbs,
+                         const double *Tbe, const double *Tbw, const double *p, double *pe, double *pn);
+
 #ifdef __cplusplus
 }
 #endif
