@@ -341,7 +341,7 @@ typedef struct m2d_case {
     int coord, modvis;
     double beta;
     double p0, T0, Twall;                   /* Tnbc: Twall <= 0 means adiabatic */
-    double Rg, gamma, mu, kappa;            /* CONSTANT thermophysical model */
+    double Rg, gamma, mu, kappa;            /* CONSTANT thermophysical model (ktm = 0) */
     int itmmax, itpmax;
     double tolm, tolt;
     int solver;                             /* 0 MSI, 1 TDMA, 2 MSI with FP32 factors and sweeps */
@@ -351,6 +351,8 @@ typedef struct m2d_case {
     double dt1, dt2; int it1, it2;
     double h0, mincc, maxcc;
     int nan_policy;                         /* max() with the NaN of at = 0: 0 drop, 1 propagate */
+    int ktm;                                /* 0 CONSTANT, 1 MIXTURE (thermophysical_initialization) */
+    m2d_mixture mix;                        /* ktm = 1: the gas mixture (m2d_mixture_init) */
 } m2d_case;
 
 typedef struct m2d_report {

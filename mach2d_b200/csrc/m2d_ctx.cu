@@ -11,6 +11,7 @@
 #include "m2d_fields.cuh"
 #include "m2d_setup.h"
 #include "m2d_solvers.cuh"
+#include "m2d_thermo.cuh"
 
 using namespace m2d;
 
@@ -34,6 +35,7 @@ struct m2d_ctx {
     double *ws9[2], *ws5, *P, *Q, *part;
     double *dsc = nullptr;
     int *dint = nullptr;
+    m2d_mixture *dmix = nullptr;   // device copy of c.mix (ktm = 1)
     double *hsc = nullptr;   // pinned mirror of dsc
     int *hint = nullptr;     // pinned mirror of dint
     double dt = 0, norm = 0, normpl = 0, rmass = 0, p_avg = 0;
@@ -82,12 +84,38 @@ static double *plane_ptr(m2d_ctx *x, const char *name, long *n)
     return nullptr;
 }
 
+// cp, and for Navier-Stokes vlp, kp and their face values, from T and the
+// boundary temperatures (src/mach2d_main.f90:112-149); with `boundary` the
+// boundary temperatures are first taken as face averages of T
+static cudaError_t mixture_properties(m2d_ctx *x, bool boundary)
+{
+    Fields &f = x->f;
+    const int nx = x->nx, ny = x->ny;
+    cudaStream_t st = x->st;
+    cudaError_t e = cudaSuccess;
+    if (boundary) e = launch_boundary_fields(nx, ny, f.T, f.Tbn, f.Tbs, f.Tbe, f.Tbw, st);
+    if (e == cudaSuccess) e = launch_set_cp(nx, ny, x->dmix, f.Tbn, f.Tbs, f.Tbe, f.Tbw, f.T, f.cp, st);
+    if (e == cudaSuccess && x->c.modvis == 1) {
+        e = launch_transport_nodes(nx, ny, x->dmix, true, f.T, f.vlp, st);
+        if (e == cudaSuccess) e = launch_transport_nodes(nx, ny, x->dmix, false, f.T, f.kp, st);
+        if (e == cudaSuccess)
+            e = launch_transport_faces(nx, ny, x->dmix, true, f.Tbn, f.Tbs, f.Tbe, f.Tbw, f.vlp, f.vle, f.vln, st);
+        if (e == cudaSuccess)
+            e = launch_transport_faces(nx, ny, x->dmix, false, f.Tbn, f.Tbs, f.Tbe, f.Tbw, f.kp, f.ke, f.kn, st);
+    }
+    if (boundary) x->launches += 3 + (x->c.modvis == 1 ? 4 : 0);   // counted inside m2d_iterate only
+    return e;
+}
+
 extern "C" int m2d_create(const m2d_case *c, int device, m2d_ctx **out)
 {
     if (!c || !out) return ctx_fail(M2D_ERR_ARG, "m2d_create: null argument");
     *out = nullptr;
     if (c->nxr < 3 || c->nyr < 3) return ctx_fail(M2D_ERR_ARG, "m2d_create: need at least 3x3 real volumes");
     if (c->solver != 1 && c->nyr + 2 > msi_max_ny()) return ctx_fail(M2D_ERR_TOO_LARGE, "m2d_create: ny exceeds m2d_msi_max_ny()");
+    if (c->ktm != 0 && c->ktm != 1) return ctx_fail(M2D_ERR_ARG, "m2d_create: ktm must be 0 (CONSTANT) or 1 (MIXTURE)");
+    if (c->ktm == 1 && (c->mix.ngs < 1 || c->mix.ngs > M2D_MAX_SPECIES || !(c->mix.Rg > 0.0)))
+        return ctx_fail(M2D_ERR_ARG, "m2d_create: ktm = 1 needs a mixture from m2d_mixture_init");
     HostInstance h;
     int rc = build_instance(*c, h);
     if (rc) return ctx_fail(rc, "m2d_create: grid set-up failed");
@@ -105,7 +133,8 @@ extern "C" int m2d_create(const m2d_case *c, int device, m2d_ctx **out)
     const size_t nplanes = h.planes().size();
     const size_t strips = (size_t)9 * h.ny + 2 * (size_t)h.nx + 64;
     const size_t solver = 2 * msi_work_doubles(9, h.nx, h.ny) + msi_work_doubles(5, h.nx, h.ny) + 2 * N + 3 * 32;
-    const size_t total = nplanes * N + 32 * N + strips + solver + (size_t)red_parts() + 64 + S_COUNT;
+    const size_t mixd = (sizeof(m2d_mixture) + sizeof(double) - 1) / sizeof(double);
+    const size_t total = nplanes * N + 32 * N + strips + solver + (size_t)red_parts() + 64 + S_COUNT + mixd;
     e = cudaMalloc(&x->arena, total * sizeof(double));
     if (e != cudaSuccess) { cudaStreamDestroy(x->st); delete x; m2d_set_last_error(e, "cudaMalloc", __FILE__, __LINE__); return M2D_ERR_NOMEM; }
     cudaMemsetAsync(x->arena, 0, total * sizeof(double), x->st);
@@ -129,6 +158,7 @@ extern "C" int m2d_create(const m2d_case *c, int device, m2d_ctx **out)
     x->part = take((size_t)red_parts() + 8);
     x->dsc = take(S_COUNT);
     x->dint = (int *)take(I_COUNT);
+    x->dmix = (m2d_mixture *)take(mixd);
     if ((size_t)(cur - x->arena) > total) { m2d_destroy(x); return ctx_fail(M2D_ERR_NOMEM, "m2d_create: arena overflow"); }
     e = cudaMallocHost(&x->hsc, S_COUNT * sizeof(double));
     if (e == cudaSuccess) e = cudaMallocHost(&x->hint, I_COUNT * sizeof(int));
@@ -148,12 +178,16 @@ extern "C" int m2d_create(const m2d_case *c, int device, m2d_ctx **out)
             {f.Tbs, &h.Tbs}};
         for (auto &s : sv)
             if (e == cudaSuccess) e = cudaMemcpyAsync(s.d, s.v->data(), s.v->size() * sizeof(double), cudaMemcpyHostToDevice, x->st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(x->dmix, &c->mix, sizeof(m2d_mixture), cudaMemcpyHostToDevice, x->st);
+        // get_cp_mu_kappa_initialization for the MIXTURE model
+        // (mod_thermophysical.f90:560-589), from the initial T and Tbn..Tbw
+        if (e == cudaSuccess && c->ktm == 1) e = mixture_properties(x, false);
         if (e == cudaSuccess) e = cudaStreamSynchronize(x->st);
         if (e != cudaSuccess) { m2d_destroy(x); m2d_set_last_error(e, "upload", __FILE__, __LINE__); return M2D_ERR_CUDA; }
     }
     Params &q = x->q;
     memset(&q, 0, sizeof q);
-    q.modvis = c->modvis; q.coord = c->coord; q.beta = c->beta; q.Rg = c->Rg; q.gamma = c->gamma;
+    q.modvis = c->modvis; q.coord = c->coord; q.beta = c->beta; q.Rg = h.Rg; q.gamma = h.gamma;
     q.p0 = c->p0; q.T0 = c->T0; q.Cpref = h.Cpref; q.Href = h.Href; q.Twall = c->Twall;
     x->Href = h.Href; x->Cpref = h.Cpref; x->fm1D = h.fm1D; x->Fd1D = h.Fd1D; x->Fpv1D = h.Fpv1D;
     x->Sg = h.Sg; x->dt = h.dt0;
@@ -262,6 +296,7 @@ extern "C" int m2d_iterate(m2d_ctx *x, m2d_report *rep)
     TRY(cudaMemsetAsync(x->dint, 0, I_COUNT * sizeof(int), st));
     KL(launch_backup(f, st), 1);
     KL(launch_inlet_update(f, q, st), 1);
+    if (c.ktm == 1) TRY(mixture_properties(x, true));
     {
         RedArgs r = red(x, RED_SUM_REAL); r.x = f.p;
         KL(launch_reduce(r, x->part, x->dsc + S_PSUM, st), 2);
@@ -331,7 +366,9 @@ extern "C" int m2d_iterate(m2d_ctx *x, m2d_report *rep)
         r.ron = f.ron; r.roe = f.roe; r.Uce = f.Uce; r.Vcn = f.Vcn; r.dt = q.dt;
         KL(launch_reduce(r, x->part, x->dsc + S_RMASS, st), 2);
     }
-    const bool h_conservation = (c.modvis == 0);   // constant properties only in this build
+    // T from total-enthalpy conservation for Euler with constant properties
+    // only (src/mach2d_main.f90:357-359); otherwise the energy equation
+    const bool h_conservation = (c.modvis == 0 && c.ktm == 0);
     if (h_conservation) {
         KL(launch_T_from_H(f, x->Href, x->Cpref, st), 2);
     } else {

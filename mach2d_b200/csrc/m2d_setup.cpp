@@ -9,6 +9,7 @@
 //   metrics, radius   src/grid/mod_grid.f90:237-723
 //   initial guess     src/user/internal_flow/mod_intflow.f90:1240-1557
 #include "m2d_setup.h"
+#include "m2d_thermo.cuh"
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -283,13 +284,20 @@ int build_instance(const m2d_case &c, HostInstance &h)
     for (int j = 2; j <= ny - 1; j++) { h.fbe[I(1, j)] = 1.0; h.fbe[I(nx - 1, j)] = 1.0; }
     for (int i = 2; i <= nx - 1; i++) { h.fbn[I(i, ny - 1)] = 1.0; h.fbn[I(i, 1)] = 1.0; }
 
-    // reference values (intflow_init, mod_intflow.f90:72-100, CONSTANT model)
-    h.Rg = c.Rg; h.gamma = c.gamma;
-    h.Cpref = c.gamma * c.Rg / (c.gamma - 1.0);
+    // reference values: thermophysical_initialization (mod_thermophysical.f90:20-75)
+    // and intflow_init (mod_intflow.f90:72-100); the internal-flow routines take
+    // gamma = gm(T0) (:1121, :1186)
+    if (c.ktm == 1) {
+        h.Rg = c.mix.Rg; h.gamma = m2d::mix_gm(c.mix, c.T0);
+        h.Cpref = m2d::mix_cp(c.mix, c.T0);
+    } else {
+        h.Rg = c.Rg; h.gamma = c.gamma;
+        h.Cpref = c.gamma * c.Rg / (c.gamma - 1.0);
+    }
     h.Href = h.Cpref * c.T0;
 
     // quasi-1D isentropic initial guess, mod_intflow.f90:1240-1488
-    const double pi = std::acos(-1.0), po = c.p0, T0 = c.T0, gm = c.gamma, Rg = c.Rg, Sg = h.Sg;
+    const double pi = std::acos(-1.0), po = c.p0, T0 = c.T0, gm = h.gamma, Rg = h.Rg, Sg = h.Sg;
     h.fm1D = po * Sg * std::sqrt(gm / (Rg * T0) * std::pow(2.0 / (gm + 1.0), (gm + 1.0) / (gm - 1.0)));
     int ig = 1;
     for (int i = 2; i <= nx - 1; i++)
@@ -413,9 +421,10 @@ int build_instance(const m2d_case &c, HostInstance &h)
     h.Tbs = h.T1D;
     h.Tbn = h.T1D;
     h.Tbe.assign(ny, h.T1D[nx - 2]);
-    // constant properties (get_cp_mu_kappa_initialization)
-    std::fill(h.cp.begin(), h.cp.end(), h.Cpref);
-    if (c.modvis == 1) {
+    // constant properties (get_cp_mu_kappa_initialization); the MIXTURE model's
+    // fields are computed on the device by m2d_create from T and Tbn..Tbw
+    if (c.ktm != 1) std::fill(h.cp.begin(), h.cp.end(), h.Cpref);
+    if (c.modvis == 1 && c.ktm != 1) {
         std::fill(h.vlp.begin(), h.vlp.end(), c.mu); std::fill(h.vle.begin(), h.vle.end(), c.mu);
         std::fill(h.vln.begin(), h.vln.end(), c.mu); std::fill(h.kp.begin(), h.kp.end(), c.kappa);
         std::fill(h.ke.begin(), h.ke.end(), c.kappa); std::fill(h.kn.begin(), h.kn.end(), c.kappa);

@@ -2,6 +2,7 @@
 // (src/thermophysical/mod_class_thermophysical_mixture.f90) and the field
 // routines of src/thermophysical/mod_thermophysical.f90.
 #pragma once
+#include <cmath>
 #include <cuda_runtime.h>
 #include "../../include/mach2d_b200.h"
 

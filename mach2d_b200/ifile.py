@@ -4,9 +4,12 @@ A data line is `value & name & description`; any other line is a comment.
 `case_from_decks` maps a parameters deck plus a geometry deck onto the
 m2d_case of the device-resident iteration (src/mod_mach2d_data.f90:186-233,
 src/grid/mod_grid.f90:44-75, src/solvers/mod_solvers.f90:17-87,
-src/tstepper/mod_tstepper*.f90, mod_class_thermophysical_constant.f90).
+src/tstepper/mod_tstepper*.f90, src/thermophysical/mod_thermophysical.f90:20-75).
 """
+import os
+
 from .simplec import Case
+from .thermo import mixture_from_files
 
 
 def parse(path, delimiter="&"):
@@ -26,11 +29,24 @@ def fnum(s):
     return float(s.replace("d", "e").replace("D", "e"))
 
 
-def case_from_decks(params_path, geometry_path):
+def _resolve(path, base_dir):
+    """A deck names its data files relative to the directory the solver runs
+    in (./mach2d_input/...): try the current directory, then base_dir."""
+    if os.path.isabs(path) or os.path.exists(path):
+        return path
+    return os.path.join(base_dir, path)
+
+
+def case_from_decks(params_path, geometry_path, base_dir=None):
+    """base_dir: where the deck's relative data-file paths start (default:
+    the parent of the deck's own directory)."""
     p = parse(params_path)
     g = parse(geometry_path)
-    if p.get("thermo_model", "").strip() != "CONSTANT":
-        raise ValueError("only the CONSTANT thermophysical model is supported")
+    if base_dir is None:
+        base_dir = os.path.dirname(os.path.dirname(os.path.abspath(params_path)))
+    model = p.get("thermo_model", "").strip()
+    if model not in ("CONSTANT", "MIXTURE"):
+        raise ValueError(f"thermophysical_initialization: Unknown opton: {model}")
     if int(p["kflow"]) != 1:
         raise ValueError("only internal flow (kflow = 1) is supported")
     nmf, nmd = int(p["nmf"]), int(p["nmd"])
@@ -71,4 +87,9 @@ def case_from_decks(params_path, geometry_path):
     c.it1, c.it2 = int(p["it1"]), int(p["it2"])
     c.h0, c.mincc, c.maxcc = fnum(p["h0"]), fnum(p["mincc"]), fnum(p["maxcc"])
     c.nan_policy = 0
+    c.ktm = 0
+    if model == "MIXTURE":
+        c.ktm = 1
+        c.mix = mixture_from_files(_resolve(p["thermo_mix_parameters"].strip(), base_dir),
+                                   _resolve(p["thermo_mix_database"].strip(), base_dir))
     return c

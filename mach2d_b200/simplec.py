@@ -6,6 +6,7 @@ import ctypes
 import numpy as np
 
 from ._lib import check, lib
+from .thermo import Mixture
 
 
 class Case(ctypes.Structure):
@@ -26,11 +27,19 @@ class Case(ctypes.Structure):
         ("tol_u", ctypes.c_double), ("tol_p", ctypes.c_double), ("dtmodel", ctypes.c_int),
         ("dt1", ctypes.c_double), ("dt2", ctypes.c_double), ("it1", ctypes.c_int),
         ("it2", ctypes.c_int), ("h0", ctypes.c_double), ("mincc", ctypes.c_double),
-        ("maxcc", ctypes.c_double), ("nan_policy", ctypes.c_int),
+        ("maxcc", ctypes.c_double), ("nan_policy", ctypes.c_int), ("ktm", ctypes.c_int),
+        ("mix", Mixture),
     ]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_}
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "mix"}
+        if self.ktm == 1:
+            m = self.mix
+            n = m.ngs
+            d["mix"] = {"ngs": n, "Rg": m.Rg, "Xi": list(m.Xi)[:n], "Yi": list(m.Yi)[:n],
+                        "Mi": list(m.Mi)[:n], "cpi": [list(r) for r in m.cpi][:n],
+                        "mui": [list(r) for r in m.mui][:n], "kpi": [list(r) for r in m.kpi][:n]}
+        return d
 
 
 class Report(ctypes.Structure):

@@ -82,3 +82,29 @@ def read_species_database(path, names):
     mui = np.array([species[n]["ID_VL"][:4] + species[n]["ID_VU"][:4] for n in names])
     kpi = np.array([species[n]["ID_KL"][:4] + species[n]["ID_KU"][:4] for n in names])
     return Mi, cpi, mui, kpi
+
+
+def read_mixture_parameters(path):
+    """(base, names, fractions) from a file in the reference's
+    thermo_parameters.txt format: the base (0 molar, 1 mass) on the first
+    line, then `fraction name` lines up to one named END
+    (mod_class_thermophysical_mixture.f90:78-170)."""
+    with open(path) as fh:
+        lines = [ln.split() for ln in fh if ln.strip()]
+    base = int(float(lines[0][0]))
+    names, fr = [], []
+    for parts in lines[1:]:
+        if parts[1] == "END":
+            break
+        fr.append(float(parts[0].replace("D", "E").replace("d", "e")))
+        names.append(parts[1])
+    return base, names, fr
+
+
+def mixture_from_files(parameters_path, database_path):
+    """The MIXTURE model of class_thermophysical_mixture%init from its two
+    input files; species whose fraction is <= 1e-8 are left out."""
+    base, names, fr = read_mixture_parameters(parameters_path)
+    keep = [k for k, f in enumerate(fr) if f > 1e-8]
+    Mi, cpi, mui, kpi = read_species_database(database_path, [names[k] for k in keep])
+    return mixture_init(base, [fr[k] for k in keep], Mi, cpi, mui, kpi)

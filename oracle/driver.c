@@ -79,11 +79,19 @@ orc_state *orc_create(const orc_case *c)
     double **v2[] = {&s->M1D, &s->p1D, &s->T1D, &s->u1D};
     for (int k = 0; k < 4; k++) *v2[k] = (double *)calloc((size_t)nx, sizeof(double));
 
-    /* thermophysical_initialization + intflow_init (constant model) */
-    s->ktm = 0;
-    s->Rg = c->Rg; s->gamma = c->gamma;
+    /* thermophysical_initialization (mod_thermophysical.f90:20-75) + intflow_init
+     * (mod_intflow.f90:72-100); the internal-flow routines take gamma = gm(T0)
+     * (:1121, :1186) */
+    s->ktm = c->ktm;
     s->Tref = c->T0;
-    s->Cpref = c->gamma * c->Rg / (c->gamma - 1.0);
+    if (c->ktm == 1) {
+        s->Rg = c->mix.Rg;
+        s->gamma = orc_mix_gm(&c->mix, c->T0);
+        s->Cpref = orc_mix_cp(&c->mix, s->Tref);
+    } else {
+        s->Rg = c->Rg; s->gamma = c->gamma;
+        s->Cpref = c->gamma * c->Rg / (c->gamma - 1.0);
+    }
     s->Href = s->Cpref * s->Tref;
 
     /* grid_create (nmf = nmd: the finest grid is the desired grid) */
@@ -107,7 +115,7 @@ orc_state *orc_create(const orc_case *c)
     /* intflow_initial_conditions -> get_initial_guess (mod_intflow.f90:1240-1488) */
     {
         const double pi = acos(-1.0);
-        double po = c->p0, T0 = c->T0, gamma = c->gamma, Rg = c->Rg, Sg = s->Sg;
+        double po = c->p0, T0 = c->T0, gamma = s->gamma, Rg = s->Rg, Sg = s->Sg;
         s->fm1D = orc_get_isentropic_mass_flow(po, T0, gamma, Rg, Sg);
         int ig = orc_get_ig(nx, ny, s->y);
         for (int i = 2; i <= nx - 1; i++) {
@@ -181,13 +189,23 @@ orc_state *orc_create(const orc_case *c)
         memcpy(s->Tbn, s->T1D, (size_t)nx * sizeof(double));
         for (int j = 0; j < ny; j++) s->Tbe[j] = V1(s->T1D, nx - 1);
     }
-    /* get_cp_mu_kappa_initialization (constant model) */
-    for (size_t k = 0; k < N; k++) s->cp[k] = s->Cpref;
-    if (c->modvis == 1)
-        for (size_t k = 0; k < N; k++) {
-            s->vlp[k] = c->mu; s->vle[k] = c->mu; s->vln[k] = c->mu;
-            s->kp[k] = c->kappa; s->ke[k] = c->kappa; s->kn[k] = c->kappa;
+    /* get_cp_mu_kappa_initialization (mod_thermophysical.f90:514-591) */
+    if (c->ktm == 1) {
+        orc_set_cp(&c->mix, nx, ny, s->Tbn, s->Tbs, s->Tbe, s->Tbw, s->T, s->cp);
+        if (c->modvis == 1) {
+            orc_transport_nodes(&c->mix, nx, ny, 1, s->T, s->vlp);
+            orc_transport_nodes(&c->mix, nx, ny, 0, s->T, s->kp);
+            orc_transport_faces(&c->mix, nx, ny, 1, s->Tbn, s->Tbs, s->Tbe, s->Tbw, s->vlp, s->vle, s->vln);
+            orc_transport_faces(&c->mix, nx, ny, 0, s->Tbn, s->Tbs, s->Tbe, s->Tbw, s->kp, s->ke, s->kn);
         }
+    } else {
+        for (size_t k = 0; k < N; k++) s->cp[k] = s->Cpref;
+        if (c->modvis == 1)
+            for (size_t k = 0; k < N; k++) {
+                s->vlp[k] = c->mu; s->vle[k] = c->mu; s->vln[k] = c->mu;
+                s->kp[k] = c->kappa; s->ke[k] = c->kappa; s->kn[k] = c->kappa;
+            }
+    }
     /* first time step */
     if (c->dtmodel == 1) s->dt = orc_tstepper_dt0_scarborough(nx, ny, s->Jp, s->u, s->v);
     else s->dt = orc_tstepper_dt_ramp(0, c->dt1, c->dt2, c->it1, c->it2);
@@ -224,6 +242,17 @@ int orc_iterate(orc_state *s, orc_report *rep)
     orc_get_uin_vin_pin_Tin_Mw(nx, ny, s->gamma, s->Rg, c->p0, c->T0, s->u, s->uin, s->vin,
                                s->pin, s->Tin, s->Mw);
     orc_get_plin_and_p_fictitious(nx, ny, s->x, s->xp, s->pina, s->pin, s->plin, s->p);
+    /* temperature-dependent properties, src/mach2d_main.f90:112-149 */
+    if (s->ktm == 1) {
+        orc_get_boundary_fields(nx, ny, s->T, s->Tbn, s->Tbs, s->Tbe, s->Tbw);
+        orc_set_cp(&c->mix, nx, ny, s->Tbn, s->Tbs, s->Tbe, s->Tbw, s->T, s->cp);
+        if (modvis == 1) {
+            orc_transport_nodes(&c->mix, nx, ny, 1, s->T, s->vlp);
+            orc_transport_nodes(&c->mix, nx, ny, 0, s->T, s->kp);
+            orc_transport_faces(&c->mix, nx, ny, 1, s->Tbn, s->Tbs, s->Tbe, s->Tbw, s->vlp, s->vle, s->vln);
+            orc_transport_faces(&c->mix, nx, ny, 0, s->Tbn, s->Tbs, s->Tbe, s->Tbw, s->kp, s->ke, s->kn);
+        }
+    }
     /* get_average(p) */
     {
         double a = 0.0;

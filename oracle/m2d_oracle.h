@@ -214,6 +214,15 @@ double orc_tstepper_dt_scarborough(int nx, int ny, double dt, const double *au,
     double maxcc, int nan_policy);
 double orc_tstepper_dt_ramp(int it, double dt1, double dt2, int it1, int it2);
 
+/* gas mixture (thermo.c); the layout of the library's m2d_mixture */
+#define ORC_MAX_SPECIES 8
+typedef struct orc_mixture {
+    int ngs;
+    double Rg;
+    double Xi[ORC_MAX_SPECIES], Yi[ORC_MAX_SPECIES], Mi[ORC_MAX_SPECIES], Ri[ORC_MAX_SPECIES];
+    double cpi[ORC_MAX_SPECIES][10], mui[ORC_MAX_SPECIES][8], kpi[ORC_MAX_SPECIES][8];
+} orc_mixture;
+
 /* ---- driver: src/mach2d_main.f90:25-445 --------------------------------- */
 typedef struct orc_case {
     /* geometry: 0 = C01 cosine nozzle, 1 = N01 */
@@ -237,6 +246,8 @@ typedef struct orc_case {
     double dt1, dt2; int it1, it2;
     double h0, mincc, maxcc;
     int nan_policy;
+    int ktm;               /* 0 = CONSTANT, 1 = MIXTURE */
+    orc_mixture mix;       /* ktm = 1 */
 } orc_case;
 
 typedef struct orc_report {
@@ -270,13 +281,6 @@ void orc_get_eddy_viscosity_fictitious(int nx, int ny, double *phi);
 /* ---- thermophysical model (thermo.c): mod_class_thermophysical_mixture.f90,
  *      mod_thermophysical.f90, mod_field_operations.f90.  orc_mixture has
  *      the layout of the library's m2d_mixture. */
-#define ORC_MAX_SPECIES 8
-typedef struct orc_mixture {
-    int ngs;
-    double Rg;
-    double Xi[ORC_MAX_SPECIES], Yi[ORC_MAX_SPECIES], Mi[ORC_MAX_SPECIES], Ri[ORC_MAX_SPECIES];
-    double cpi[ORC_MAX_SPECIES][10], mui[ORC_MAX_SPECIES][8], kpi[ORC_MAX_SPECIES][8];
-} orc_mixture;
 int orc_mixture_init(int base, int ngs, const double *fractions, const double *Mi, const double *cpi,
                      const double *mui, const double *kpi, orc_mixture *out);
 double orc_mix_cp(const orc_mixture *m, double T);

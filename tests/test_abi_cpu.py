@@ -3,6 +3,7 @@ every entry point include/mach2d_b200.h declares, rejects bad arguments
 without touching the device, and the host-side mirrors behave like the
 reference's (solver factory, deck reader)."""
 import ctypes
+import json
 import os
 import subprocess
 
@@ -77,3 +78,30 @@ def test_deck_reader_maps_a_reference_style_deck(tmp_path):
 
 def test_package_points_at_in_tree_library():
     assert os.path.dirname(mach2d_b200.LIB_PATH) == os.path.join(ROOT, "mach2d_b200")
+
+
+REF_INPUT = "/root/reference/mach2d_input"
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_INPUT), reason="reference input decks not present")
+def test_deck_reader_builds_the_mixture_of_a_reference_mixture_deck():
+    """parametersNozzleNSPTV.txt selects thermo_model = MIXTURE; its species
+    come from thermo_parameters.txt and thermo_database.csv."""
+    from mach2d_b200.ifile import case_from_decks
+    from mach2d_b200.thermo import mixture_init
+    c = case_from_decks(os.path.join(REF_INPUT, "parametersNozzleNSPTV.txt"),
+                        os.path.join(REF_INPUT, "geometry_n01.txt"), base_dir=os.path.dirname(REF_INPUT))
+    assert (c.ktm, c.modvis, c.mix.ngs) == (1, 1, 3)
+    d = json.load(open(os.path.join(ROOT, "tests", "golden", "air_species.json")))
+    m = mixture_init(d["base"], d["fractions"], d["Mi"], d["cpi"], d["mui"], d["kpi"])
+    assert bytes(m) == bytes(c.mix)
+
+
+def test_air_fixture_gives_air_properties():
+    from mach2d_b200.thermo import mixture_eval, mixture_init
+    d = json.load(open(os.path.join(ROOT, "tests", "golden", "air_species.json")))
+    m = mixture_init(d["base"], d["fractions"], d["Mi"], d["cpi"], d["mui"], d["kpi"])
+    cp, mu, kp, gm = mixture_eval(m, 300.0)
+    assert m.Rg == pytest.approx(287.0, rel=1e-4)
+    assert cp == pytest.approx(1004.5, rel=2e-3) and gm == pytest.approx(1.400, rel=1e-3)
+    assert mu == pytest.approx(1.85e-5, rel=2e-2) and kp == pytest.approx(0.0262, rel=3e-2)

@@ -78,6 +78,39 @@ def test_navier_stokes_constant_properties():
     _compare_runs(euler_cosine_case(24, 12, modvis=1, Twall=900.0), 12)
 
 
+def _air():
+    from mach2d_b200.thermo import mixture_init
+    d = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "air_species.json")))
+    return mixture_init(d["base"], d["fractions"], d["Mi"], d["cpi"], d["mui"], d["kpi"])
+
+
+PROPS = ("cp", "vlp", "vle", "vln", "kp", "ke", "kn")
+
+
+def test_mixture_initial_properties():
+    """get_cp_mu_kappa_initialization with the MIXTURE model: cp bitwise,
+    mu and k (device exp/log) to 1e-12."""
+    case = euler_cosine_case(30, 14, modvis=1, Twall=900.0, ktm=1, mix=_air())
+    g, o = Simplec(case), OracleCase(case)
+    assert g.scalar("Cpref") == o.scalar("Cpref") and g.scalar("Href") == o.scalar("Href")
+    assert np.array_equal(g.field("cp"), o.field("cp"))
+    for f in PROPS[1:]:
+        fg, fo = g.field(f), o.field(f)
+        assert np.max(np.abs(fg - fo)) <= 1e-12 * np.max(np.abs(fo)), f
+
+
+def test_mixture_euler():
+    # ktm = 1, modvis = 0: cp(T) every iteration and the energy equation for T
+    _compare_runs(euler_cosine_case(24, 12, ktm=1, mix=_air()), 12,
+                  fields=("u", "v", "p", "T", "ro", "cp", "roe", "ron"))
+
+
+def test_mixture_navier_stokes():
+    # ktm = 1, modvis = 1: cp, mu and k at nodes and faces every iteration
+    _compare_runs(euler_cosine_case(24, 12, modvis=1, Twall=900.0, ktm=1, mix=_air()), 12,
+                  fields=("u", "v", "p", "T", "ro") + PROPS)
+
+
 def test_tdma_solver_path():
     _compare_runs(n01_case(solver=1, nitm_u=3, nitm_p=5), 15)
 

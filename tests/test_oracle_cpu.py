@@ -137,3 +137,52 @@ def test_blomax_oracle_zero_for_uniform_flow_positive_for_shear():
     orc("get_eddy_viscosity_blomax", nx, ny, *[f[k] for k in keys], vt, np.zeros(9 * (ny - 2)))
     real = vt.reshape(ny, nx)[1:-1, 1:-1]
     assert np.all(real >= 0.0) and np.max(real) > 0.0
+
+
+def _constant_species_mixture(Rg, gamma, mu, kappa):
+    """One species whose cp, mu and k do not depend on T: cp/R = gamma/(gamma-1),
+    mu = exp(ln(mu 1e7)) 1e-7, k = exp(ln(k 1e4)) 1e-4."""
+    from mach2d_b200.thermo import mixture_init
+    Mi = 8.31451 / Rg
+    c = gamma / (gamma - 1.0)
+    cpi = [c, 0, 0, 0, 0, c, 0, 0, 0, 0]
+    lm, lk = math.log(mu * 1e7), math.log(kappa * 1e4)
+    return mixture_init(0, [1.0], [Mi], cpi, [0, 0, 0, lm, 0, 0, 0, lm], [0, 0, 0, lk, 0, 0, 0, lk])
+
+
+def test_mixture_with_constant_species_matches_constant_model():
+    """The MIXTURE path of the driver (properties recomputed every iteration,
+    src/mach2d_main.f90:112-149) reduces to the CONSTANT one when the species'
+    properties do not depend on T: same run to rounding."""
+    base = euler_cosine_case(20, 10, modvis=1, Twall=900.0)
+    mix = _constant_species_mixture(base.Rg, base.gamma, base.mu, base.kappa)
+    var = euler_cosine_case(20, 10, modvis=1, Twall=900.0, ktm=1, mix=mix)
+    a, b = OracleCase(base), OracleCase(var)
+    assert abs(b.scalar("Cpref") / a.scalar("Cpref") - 1) < 1e-14
+    for _ in range(8):
+        ra, rb = a.iterate()[1], b.iterate()[1]
+        assert ra.itp_used == rb.itp_used
+        assert abs(rb.norm / ra.norm - 1) < 1e-9
+    for f in ("u", "v", "p", "T"):
+        fa, fb = a.field(f), b.field(f)
+        assert np.max(np.abs(fa - fb)) <= 1e-9 * np.max(np.abs(fa)), f
+    assert np.max(np.abs(b.field("vle")[b.field("vle") != 0] / base.mu - 1)) < 1e-13
+
+
+def test_mixture_euler_solves_the_energy_equation():
+    """ktm = 1 with modvis = 0: T comes from the energy equation (no H
+    conservation), cp follows T, and the run stays finite."""
+    d = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "air_species.json")))
+    from mach2d_b200.thermo import mixture_eval, mixture_init
+    mix = mixture_init(d["base"], d["fractions"], d["Mi"], d["cpi"], d["mui"], d["kpi"])
+    o = OracleCase(euler_cosine_case(20, 10, ktm=1, mix=mix))
+    assert o.scalar("Cpref") == mixture_eval(mix, 1000.0)[0]      # Cpref = cp(T0)
+    for _ in range(10):
+        rc, rep = o.iterate()
+        assert rc == 0 and np.isfinite(rep.norm)
+    T, cp = o.field("T"), o.field("cp")
+    nx, ny = o.nx, o.ny
+    real = np.zeros((ny, nx), bool)
+    real[1:-1, 1:-1] = True
+    real = real.reshape(-1)
+    assert np.std(cp[real]) > 0 and np.all((T[real] > 200) & (T[real] < 1100))
