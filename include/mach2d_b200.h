@@ -402,6 +402,68 @@ int m2d_batch_size(const m2d_batch *b, int *n);
 int m2d_batch_ctx(m2d_batch *b, int k, m2d_ctx **ctx);
 int m2d_batch_iterate(m2d_batch *b, int iters, m2d_report *reps);
 int m2d_batch_status(const m2d_batch *b, int k, int *status);
+
+/* ===================== 3. learned p' preconditioner ======================
+ * No counterpart in the reference.  A 4-level U-Net (3x3 convolutions with
+ * 16/32/64/128 channels, GELU, 2x2 mean pooling, nearest upsampling with
+ * skip concatenation, 1x1 head; BF16 weights and activations, FP32
+ * accumulation) maps 11 planes of a p' system to a p' correction.
+ * Images are H x W (multiples of 8), pixel (y, x) = real cell (x+2, y+2).
+ * Parameters (FP32 master copy, m2d_unet_param_count() floats): per
+ * convolution in network order -- enc0 (16->16, 16->16), enc1 (16->32,
+ * 32->32), enc2 (32->64, 64->64), bottleneck (64->128, 128->128), dec2
+ * (192->64, 64->64), dec1 (96->32, 32->32), dec0 (48->16, 16->16) --
+ * W[cout][9][cin] (tap = 3 dy + dx) then b[cout]; last the head's 16
+ * weights and bias.  The input layer's channels 11..15 see zeros.
+ * All data pointers are device pointers; calls are asynchronous on `stream`
+ * unless they return host values. */
+typedef struct m2d_unet m2d_unet;
+long m2d_unet_param_count(void);
+/* bmax images per call at most; allocates activations, gradients and Adam state */
+int m2d_unet_create(int bmax, int H, int W, int device, m2d_unet **out);
+int m2d_unet_destroy(m2d_unet *net);
+int m2d_unet_shape(const m2d_unet *net, int *bmax, int *H, int *W);
+/* host FP32 parameters in and out (set also resets the Adam state) */
+int m2d_unet_set_params(m2d_unet *net, const float *host, long n);
+int m2d_unet_get_params(m2d_unet *net, float *host, long n);
+int m2d_unet_get_grads(m2d_unet *net, float *host, long n);
+/* d_in: [nimg][11][H][W] FP32 planes; d_out: [nimg][H][W] FP32 */
+int m2d_unet_forward(m2d_unet *net, int nimg, const float *d_in, float *d_out, void *stream);
+/* forward, loss = scale * sum mask (out - target)^2 (mask may be NULL), and
+ * backward into the gradients (zeroed first); *loss (host, may be NULL)
+ * receives the loss after a stream synchronisation */
+int m2d_unet_loss_grad(m2d_unet *net, int nimg, const float *d_in, const float *d_target,
+                       const float *d_mask, float scale, float *loss, void *stream);
+/* one Adam step on the master parameters, then their BF16 copies */
+int m2d_unet_adam(m2d_unet *net, float lr, float beta1, float beta2, float eps, void *stream);
+
+/* p' system <-> images.  d_a: 5 planes (S, W, P, E, N), d_stats: 16 doubles.
+ * Features: r/(aP sigma) with sigma the RMS of r/aP, the nine coefficient
+ * planes over aP (SW, S, SE, W, P, E, NW, N, NE; corners zero), and the
+ * standardised log Jp.  apply: x_out = x + sigma y.  target: t = delta /
+ * sigma and mask = 1 on real cells.  residual5: r = b - A x on real cells,
+ * *d_rr = |r|^2 (may be NULL). */
+int m2d_residual5(int nx, int ny, const double *d_a, const double *d_b, const double *d_x,
+                  double *d_r, double *d_rr, void *stream);
+int m2d_pprime_features(int nx, int ny, int H, int W, const double *d_a, const double *d_r,
+                        const double *d_Jp, float *d_feat, double *d_stats, void *stream);
+int m2d_pprime_apply(int nx, int ny, int H, int W, const float *d_y, const double *d_stats,
+                     const double *d_x, double *d_xout, void *stream);
+int m2d_pprime_target(int nx, int ny, int H, int W, const double *d_delta, const double *d_stats,
+                      float *d_t, float *d_mask, void *stream);
+/* Flexible pressure-correction solve of the 5-diagonal p' system: the
+ * network's correction is kept only when it lowers |b - A x|; the MSI
+ * iteration (prec 0 FP64, 1 FP32 sweeps) then runs with its stopping test
+ * relative to the residual before the correction, and is skipped when the
+ * correction alone meets it.  d_work: m2d_msi_workspace_doubles(5, nx, ny). */
+typedef struct m2d_learned_report {
+    int accepted;          /* 1: the network's correction was kept */
+    double r0, r1;         /* |r| before and after the correction */
+    int nit;               /* MSI iterations that followed */
+} m2d_learned_report;
+int m2d_pprime_solve_learned(m2d_unet *net, int nx, int ny, int nitm, double tol,
+                             const double *d_a, const double *d_b, double *d_x, const double *d_Jp,
+                             double *d_work, int prec, void *stream, m2d_learned_report *rep);
 int m2d_batch_destroy(m2d_batch *b);
 
 #ifdef __cplusplus

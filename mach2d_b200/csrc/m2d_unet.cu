@@ -1,0 +1,1018 @@
+// m2d_unet.cu -- the learned p' preconditioner: a 4-level U-Net (channels
+// 16/32/64/128, 3x3 convolutions, GELU, BF16 weights and activations, FP32
+// accumulation) with hand-written forward, backward and Adam kernels.
+// No counterpart in the reference: it maps (p' residual, the nine
+// coefficient planes, the Jacobian) to a p' correction that the flexible
+// pressure-correction solve (m2d_pprime_solve_learned) tries before the MSI
+// iteration, keeping plain MSI as the fallback and the judge.
+//
+// Layout: activations are pixel-major (NHWC), a pixel's channels contiguous,
+// so the K slice of one 3x3 tap is one 32-byte row per 16 channels.  Images
+// are the real cells of the p' system (pixel (y, x) = cell (x+2, y+2)),
+// zero-padded to multiples of 8.  Every convolution is an implicit GEMM
+// (M = 8x16 pixel tile, N = output channels, K = 9 taps x input channels)
+// on the tensor cores (mma.sync m16n8k16 BF16 -> FP32) from shared-memory
+// tiles read with ldmatrix; the halo tile is XOR-swizzled so that the eight
+// rows of every ldmatrix fall in distinct banks.
+#include <cuda_bf16.h>
+#include <cmath>
+#include <cstring>
+#include <vector>
+#include "m2d_common.cuh"
+#include "../../include/mach2d_b200.h"
+
+using bf16 = __nv_bfloat16;
+
+void m2d_set_last_error_msg(const char *);
+
+namespace {
+
+constexpr int kLevels = 4;
+constexpr int kChan[kLevels] = {16, 32, 64, 128};
+constexpr int kInPlanes = 11;     // residual, 9 coefficients, Jacobian
+constexpr int kInChan = 16;       // padded to the MMA K step
+constexpr int kConvs = 14;
+
+// ---------------------------------------------------------------- PTX helpers
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void ldsm_x4(uint32_t addr, uint32_t (&r)[4])
+{
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(addr));
+}
+__device__ __forceinline__ void ldsm_x4_t(uint32_t addr, uint32_t (&r)[4])
+{
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(addr));
+}
+__device__ __forceinline__ void mma_bf16(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1)
+{
+    asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
+                 "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+                 : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+                 : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// GELU, tanh form: 0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3)))
+__device__ __forceinline__ float gelu(float x)
+{
+    const float u = 0.7978845608028654f * (x + 0.044715f * x * x * x);
+    return 0.5f * x * (1.0f + tanhf(u));
+}
+__device__ __forceinline__ float gelu_grad(float x)
+{
+    const float u = 0.7978845608028654f * (x + 0.044715f * x * x * x);
+    const float t = tanhf(u);
+    return 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * 0.7978845608028654f * (1.0f + 3.0f * 0.044715f * x * x);
+}
+
+// ------------------------------------------------------------- convolution
+// Halo tile of one 8x16 pixel tile: 10 x 18 pixels x 16 channels (32 B per
+// pixel); the two 16-byte halves of pixel hp are swapped when bit 2 of hp is
+// set, which puts any 8 consecutive pixels in distinct banks.
+constexpr int kTileH = 8, kTileW = 16, kHaloW = kTileW + 2, kHaloPix = (kTileH + 2) * kHaloW;
+constexpr int kWRow = 304;        // bytes per output channel of a weight chunk (9 x 32 + 16 pad)
+
+__device__ __forceinline__ int halo_off(int hp, int half) { return hp * 32 + ((half ^ ((hp >> 2) & 1)) << 4); }
+
+struct ConvArgs {
+    const bf16 *x; int ldx;        // input view (channel 0 of the slice), channel stride
+    const bf16 *w;                 // [cout][9][cin]
+    const float *bias;             // [cout] or null
+    float *z;                      // pre-activation [pixel][cout], or null
+    bf16 *y; int ldy;              // activation view, or null
+    float *yf; int ldyf;           // FP32 output view (input gradients), or null
+    int accumulate;                // yf += result
+    int act;                       // 1: y = gelu(result)
+    int nimg, H, W, cin, cout;
+};
+
+template <int NT>
+__global__ void __launch_bounds__(128) k_conv3x3(ConvArgs a)
+{
+    __shared__ __align__(128) unsigned char s_halo[kHaloPix * 32];
+    __shared__ __align__(128) unsigned char s_w[NT * kWRow];
+    const int tilesx = (a.W + kTileW - 1) / kTileW;
+    const int ty0 = (blockIdx.x / tilesx) * kTileH, tx0 = (blockIdx.x % tilesx) * kTileW;
+    const int co0 = blockIdx.y * NT;
+    const int img = blockIdx.z;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float acc[2][NT / 8][4];
+#pragma unroll
+    for (int m = 0; m < 2; m++)
+#pragma unroll
+        for (int n = 0; n < NT / 8; n++) acc[m][n][0] = acc[m][n][1] = acc[m][n][2] = acc[m][n][3] = 0.f;
+    const uint32_t sh = smem_u32(s_halo), sw = smem_u32(s_w);
+    for (int c0 = 0; c0 < a.cin; c0 += 16) {
+        for (int q = threadIdx.x; q < kHaloPix * 2; q += 128) {
+            const int hp = q >> 1, h = q & 1;
+            const int hy = hp / kHaloW, hx = hp - hy * kHaloW;
+            const int gy = ty0 + hy - 1, gx = tx0 + hx - 1;
+            uint4 v = make_uint4(0, 0, 0, 0);
+            if (gy >= 0 && gy < a.H && gx >= 0 && gx < a.W)
+                v = *reinterpret_cast<const uint4 *>(a.x + ((long long)(img * a.H + gy) * a.W + gx) * a.ldx + c0 + h * 8);
+            *reinterpret_cast<uint4 *>(s_halo + halo_off(hp, h)) = v;
+        }
+        for (int q = threadIdx.x; q < NT * 18; q += 128) {
+            const int n = q / 18, r = q - n * 18, tap = r >> 1, h = r & 1;
+            const uint4 v = *reinterpret_cast<const uint4 *>(a.w + ((long long)(co0 + n) * 9 + tap) * a.cin + c0 + h * 8);
+            *reinterpret_cast<uint4 *>(s_w + n * kWRow + tap * 32 + h * 16) = v;
+        }
+        __syncthreads();
+#pragma unroll 1
+        for (int tap = 0; tap < 9; tap++) {
+            const int dy = tap / 3, dx = tap - dy * 3;
+            uint32_t af[2][4];
+#pragma unroll
+            for (int mt = 0; mt < 2; mt++) {
+                const int col = (lane & 7) + ((lane >> 3) & 1) * 8, half = lane >> 4;
+                const int hp = (warp * 2 + mt + dy) * kHaloW + col + dx;
+                ldsm_x4(sh + halo_off(hp, half), af[mt]);
+            }
+#pragma unroll
+            for (int np = 0; np < NT / 16; np++) {
+                const int n = np * 16 + (lane & 7) + (lane >> 4) * 8, kh = (lane >> 3) & 1;
+                uint32_t bfr[4];
+                ldsm_x4(sw + n * kWRow + tap * 32 + kh * 16, bfr);
+#pragma unroll
+                for (int mt = 0; mt < 2; mt++) {
+                    mma_bf16(acc[mt][2 * np], af[mt], bfr[0], bfr[1]);
+                    mma_bf16(acc[mt][2 * np + 1], af[mt], bfr[2], bfr[3]);
+                }
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+        for (int nt = 0; nt < NT / 8; nt++)
+#pragma unroll
+            for (int hh = 0; hh < 2; hh++) {
+                const int gy = ty0 + warp * 2 + mt, gx = tx0 + (lane >> 2) + hh * 8;
+                if (gy >= a.H || gx >= a.W) continue;
+                const long long p = (long long)(img * a.H + gy) * a.W + gx;
+                const int co = co0 + nt * 8 + (lane & 3) * 2;
+                float v0 = acc[mt][nt][hh * 2], v1 = acc[mt][nt][hh * 2 + 1];
+                if (a.bias) { v0 += a.bias[co]; v1 += a.bias[co + 1]; }
+                if (a.z) *reinterpret_cast<float2 *>(a.z + p * a.cout + co) = make_float2(v0, v1);
+                if (a.yf) {
+                    float2 *d = reinterpret_cast<float2 *>(a.yf + p * a.ldyf + co);
+                    if (a.accumulate) { const float2 o = *d; v0 += o.x; v1 += o.y; }
+                    *d = make_float2(v0, v1);
+                }
+                if (a.y) {
+                    if (a.act) { v0 = gelu(v0); v1 = gelu(v1); }
+                    *reinterpret_cast<__nv_bfloat162 *>(a.y + p * a.ldy + co) = __floats2bfloat162_rn(v0, v1);
+                }
+            }
+}
+
+// dW[co][tap][ci] += sum over pixels of dZ[p][co] X[p + tap offset][ci]:
+// a GEMM with M = output channels (64 per CTA, 16 per warp), N = 9 taps x 16
+// input channels, K = pixels (16 per step, one tile row).  Both operands come
+// from pixel-major tiles through ldmatrix.trans.
+struct WgradArgs {
+    const bf16 *x; int ldx;        // layer input view
+    const bf16 *dz;                // [pixel][cout]
+    float *dw;                     // [cout][9][cin], accumulated with atomics
+    int nimg, H, W, cin, cout;
+};
+
+__global__ void __launch_bounds__(128) k_conv3x3_wgrad(WgradArgs a)
+{
+    __shared__ __align__(128) unsigned char s_dz[kTileH * kTileW * 128];   // 128 pixels x 64 channels
+    __shared__ __align__(128) unsigned char s_halo[kHaloPix * 32];
+    const int c0 = blockIdx.x * 16, co0 = blockIdx.y * 64;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wco = warp * 16;
+    const bool active = co0 + wco < a.cout;
+    float acc[18][4];
+#pragma unroll
+    for (int n = 0; n < 18; n++) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.f;
+    const int tilesx = (a.W + kTileW - 1) / kTileW, tilesy = (a.H + kTileH - 1) / kTileH;
+    const int ntiles = a.nimg * tilesx * tilesy;
+    const uint32_t sd = smem_u32(s_dz), sh = smem_u32(s_halo);
+    for (int t = blockIdx.z; t < ntiles; t += gridDim.z) {
+        const int img = t / (tilesx * tilesy), tt = t - img * tilesx * tilesy;
+        const int ty0 = (tt / tilesx) * kTileH, tx0 = (tt % tilesx) * kTileW;
+        for (int q = threadIdx.x; q < kTileH * kTileW * 8; q += 128) {
+            const int pl = q >> 3, s = q & 7;
+            const int gy = ty0 + (pl >> 4), gx = tx0 + (pl & 15);
+            uint4 v = make_uint4(0, 0, 0, 0);
+            if (gy < a.H && gx < a.W && co0 + s * 8 < a.cout)
+                v = *reinterpret_cast<const uint4 *>(a.dz + ((long long)(img * a.H + gy) * a.W + gx) * a.cout + co0 + s * 8);
+            *reinterpret_cast<uint4 *>(s_dz + pl * 128 + ((s ^ (pl & 7)) << 4)) = v;
+        }
+        for (int q = threadIdx.x; q < kHaloPix * 2; q += 128) {
+            const int hp = q >> 1, h = q & 1;
+            const int hy = hp / kHaloW, hx = hp - hy * kHaloW;
+            const int gy = ty0 + hy - 1, gx = tx0 + hx - 1;
+            uint4 v = make_uint4(0, 0, 0, 0);
+            if (gy >= 0 && gy < a.H && gx >= 0 && gx < a.W)
+                v = *reinterpret_cast<const uint4 *>(a.x + ((long long)(img * a.H + gy) * a.W + gx) * a.ldx + c0 + h * 8);
+            *reinterpret_cast<uint4 *>(s_halo + halo_off(hp, h)) = v;
+        }
+        __syncthreads();
+        if (active) {
+#pragma unroll 1
+            for (int yy = 0; yy < kTileH; yy++) {
+                uint32_t af[4];
+                {
+                    const int mi = lane >> 3, r = lane & 7;
+                    const int pl = yy * 16 + r + 8 * (mi >> 1);
+                    const int seg = (wco + (mi & 1) * 8) >> 3;
+                    ldsm_x4_t(sd + pl * 128 + ((seg ^ (pl & 7)) << 4), af);
+                }
+#pragma unroll
+                for (int tap = 0; tap < 9; tap++) {
+                    const int dy = tap / 3, dx = tap - dy * 3;
+                    const int mi = lane >> 3, r = lane & 7;
+                    const int hp = (yy + dy) * kHaloW + r + 8 * (mi & 1) + dx;
+                    uint32_t bfr[4];
+                    ldsm_x4_t(sh + halo_off(hp, mi >> 1), bfr);
+                    mma_bf16(acc[tap * 2], af, bfr[0], bfr[1]);
+                    mma_bf16(acc[tap * 2 + 1], af, bfr[2], bfr[3]);
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (!active) return;
+#pragma unroll
+    for (int n = 0; n < 18; n++) {
+        const int tap = n >> 1, ci = c0 + (n & 1) * 8 + (lane & 3) * 2;
+#pragma unroll
+        for (int hh = 0; hh < 2; hh++) {
+            const int co = co0 + wco + (lane >> 2) + hh * 8;
+            if (co >= a.cout) continue;
+            float *d = a.dw + ((long long)co * 9 + tap) * a.cin + ci;
+            atomicAdd(d, acc[n][hh * 2]);
+            atomicAdd(d + 1, acc[n][hh * 2 + 1]);
+        }
+    }
+}
+
+// dZ = bf16(dA * gelu'(Z)); db[c] += sum of dZ over pixels (before rounding)
+__global__ void k_gelu_bwd(long long npix, int cout, const float *dA, int lda, const float *z, bf16 *dz, float *db)
+{
+    __shared__ float s_db[128];
+    for (int c = threadIdx.x; c < cout; c += blockDim.x) s_db[c] = 0.f;
+    __syncthreads();
+    const long long n = npix * cout;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const long long p = e / cout;
+        const int c = (int)(e - p * cout);
+        const float g = dA[p * lda + c] * gelu_grad(z[e]);
+        dz[e] = __float2bfloat16_rn(g);
+        atomicAdd(&s_db[c], g);
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < cout; c += blockDim.x) atomicAdd(&db[c], s_db[c]);
+}
+
+// 2x2 mean (outputs rounded to bf16) and its adjoint (added into dX)
+__global__ void k_pool(int nimg, int H, int W, int C, const bf16 *x, int ldx, bf16 *y)
+{
+    const int Ho = H / 2, Wo = W / 2;
+    const long long n = (long long)nimg * Ho * Wo * C;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const long long p = e / C;
+        const int c = (int)(e - p * C);
+        const int img = (int)(p / ((long long)Ho * Wo));
+        const int r = (int)(p - (long long)img * Ho * Wo), yo = r / Wo, xo = r - yo * Wo;
+        const long long q = ((long long)img * H + 2 * yo) * W + 2 * xo;
+        const float s = __bfloat162float(x[q * ldx + c]) + __bfloat162float(x[(q + 1) * ldx + c]) +
+                        __bfloat162float(x[(q + W) * ldx + c]) + __bfloat162float(x[(q + W + 1) * ldx + c]);
+        y[e] = __float2bfloat16_rn(0.25f * s);
+    }
+}
+__global__ void k_pool_bwd(int nimg, int H, int W, int C, const float *dy, float *dx, int lddx)
+{
+    const long long n = (long long)nimg * H * W * C;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const long long p = e / C;
+        const int c = (int)(e - p * C);
+        const int img = (int)(p / ((long long)H * W));
+        const int r = (int)(p - (long long)img * H * W), yy = r / W, xx = r - yy * W;
+        const long long q = ((long long)img * (H / 2) + yy / 2) * (W / 2) + xx / 2;
+        dx[p * lddx + c] += 0.25f * dy[q * C + c];
+    }
+}
+// nearest 2x upsampling into a channel slice, and its adjoint
+__global__ void k_up(int nimg, int Ho, int Wo, int C, const bf16 *x, bf16 *y, int ldy)
+{
+    const long long n = (long long)nimg * Ho * Wo * C;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const long long p = e / C;
+        const int c = (int)(e - p * C);
+        const int img = (int)(p / ((long long)Ho * Wo));
+        const int r = (int)(p - (long long)img * Ho * Wo), yy = r / Wo, xx = r - yy * Wo;
+        const long long q = ((long long)img * (Ho / 2) + yy / 2) * (Wo / 2) + xx / 2;
+        y[p * ldy + c] = x[q * C + c];
+    }
+}
+__global__ void k_up_bwd(int nimg, int Hi, int Wi, int C, const float *dy, int lddy, float *dx)
+{
+    const int Ho = Hi * 2, Wo = Wi * 2;
+    const long long n = (long long)nimg * Hi * Wi * C;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const long long p = e / C;
+        const int c = (int)(e - p * C);
+        const int img = (int)(p / ((long long)Hi * Wi));
+        const int r = (int)(p - (long long)img * Hi * Wi), yy = r / Wi, xx = r - yy * Wi;
+        const long long q = ((long long)img * Ho + 2 * yy) * Wo + 2 * xx;
+        dx[e] = dy[q * lddy + c] + dy[(q + 1) * lddy + c] + dy[(q + Wo) * lddy + c] + dy[(q + Wo + 1) * lddy + c];
+    }
+}
+
+// planar FP32 input [img][11][H][W] -> pixel-major bf16 with 16 channels
+__global__ void k_pack_input(int nimg, int H, int W, const float *in, bf16 *x)
+{
+    const long long n = (long long)nimg * H * W;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+        const int img = (int)(p / ((long long)H * W));
+        const long long r = p - (long long)img * H * W;
+        __align__(16) bf16 v[kInChan];
+#pragma unroll
+        for (int c = 0; c < kInChan; c++)
+            v[c] = __float2bfloat16_rn(c < kInPlanes ? in[((long long)img * kInPlanes + c) * H * W + r] : 0.f);
+        uint4 *d = reinterpret_cast<uint4 *>(x + p * kInChan);
+        d[0] = reinterpret_cast<const uint4 *>(v)[0];
+        d[1] = reinterpret_cast<const uint4 *>(v)[1];
+    }
+}
+
+// 1x1 head: out = sum_c U[p][c] wh[c] + bh
+__global__ void k_head(long long npix, const bf16 *u, const float *wh, float *out)
+{
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += (long long)gridDim.x * blockDim.x) {
+        float s = 0.f;
+#pragma unroll
+        for (int c = 0; c < 16; c++) s += __bfloat162float(u[p * 16 + c]) * wh[c];
+        out[p] = s + wh[16];
+    }
+}
+// loss = scale * sum mask (out - t)^2, dout = 2 scale mask (out - t)
+__global__ void k_loss(long long npix, const float *out, const float *t, const float *mask, float scale, float *dout,
+                       float *loss)
+{
+    float s = 0.f;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += (long long)gridDim.x * blockDim.x) {
+        const float m = mask ? mask[p] : 1.f;
+        const float d = (out[p] - t[p]) * m;
+        s += d * d;
+        dout[p] = 2.f * scale * d;
+    }
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(loss, s * scale);
+}
+// head adjoint: dU[p][c] = dout[p] wh[c]; dwh[c] += sum dout U; dbh += sum dout
+__global__ void k_head_bwd(long long npix, const bf16 *u, const float *wh, const float *dout, float *du, float *dwh)
+{
+    float g[17];
+#pragma unroll
+    for (int c = 0; c < 17; c++) g[c] = 0.f;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += (long long)gridDim.x * blockDim.x) {
+        const float d = dout[p];
+#pragma unroll
+        for (int c = 0; c < 16; c++) {
+            du[p * 16 + c] = d * wh[c];
+            g[c] += d * __bfloat162float(u[p * 16 + c]);
+        }
+        g[16] += d;
+    }
+#pragma unroll
+    for (int c = 0; c < 17; c++) {
+        float v = g[c];
+        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0) atomicAdd(&dwh[c], v);
+    }
+}
+
+__global__ void k_adam(long long n, float *p, const float *g, float *m, float *v, float lr, float b1, float b2,
+                       float eps, float c1, float c2)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.f - b1) * gi;
+        const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+        m[i] = mi; v[i] = vi;
+        p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    }
+}
+// bf16 copies of one layer's weights: W [cout][9][cin] and the adjoint
+// kernel WT [cin][9][cout] with the taps reversed
+__global__ void k_sync_weights(int cin, int cout, const float *w, bf16 *wb, bf16 *wt)
+{
+    const int n = cout * 9 * cin;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        const int co = e / (9 * cin), r = e - co * 9 * cin, tap = r / cin, ci = r - tap * cin;
+        const bf16 v = __float2bfloat16_rn(w[e]);
+        wb[e] = v;
+        wt[((long long)ci * 9 + (8 - tap)) * cout + co] = v;
+    }
+}
+
+inline unsigned grid_for(long long n, int block = 256)
+{
+    long long g = (n + block - 1) / block;
+    if (g > 148LL * 16) g = 148LL * 16;
+    return (unsigned)(g < 1 ? 1 : g);
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ network
+struct ConvLayer {
+    int cin, cout, level;
+    long long woff, boff;      // offsets into the FP32 parameter array
+    bf16 *wb = nullptr, *wt = nullptr;
+    // forward views
+    const bf16 *x = nullptr; int ldx = 0;
+    bf16 *y = nullptr; int ldy = 0;
+    float *z = nullptr;
+    // backward views: gradient of the output (FP32, same layout as y) and of the input
+    float *dy = nullptr; int lddy = 0;
+    float *dx = nullptr; int lddx = 0;   // null: input gradient not needed
+};
+
+struct m2d_unet {
+    int device = 0, bmax = 0, H = 0, W = 0;
+    long long P[kLevels];
+    long long nparam = 0;
+    float *params = nullptr, *grads = nullptr, *adam_m = nullptr, *adam_v = nullptr;
+    std::vector<void *> allocs;
+    ConvLayer L[kConvs];
+    bf16 *in0 = nullptr, *D[3] = {}, *pooled[3] = {}, *U[3] = {}, *e3b = nullptr;
+    float *out = nullptr, *dout = nullptr, *dU0 = nullptr, *loss = nullptr;
+    float *dD[3] = {}, *dpool[3] = {};
+    bf16 *dz = nullptr;
+    int adam_step = 0;
+    // scratch of the flexible p' solve (one image)
+    float *feat = nullptr, *yout = nullptr;
+    double *r = nullptr, *x1 = nullptr, *stats = nullptr;
+    int *nit = nullptr;
+};
+
+namespace {
+
+int unet_fail(int code, const char *msg)
+{
+    m2d_set_last_error_msg(msg);
+    return code;
+}
+
+template <typename T>
+T *dalloc(m2d_unet *n, long long count, cudaError_t &e)
+{
+    void *p = nullptr;
+    if (e == cudaSuccess) e = cudaMalloc(&p, (size_t)count * sizeof(T));
+    if (e == cudaSuccess) { n->allocs.push_back(p); e = cudaMemset(p, 0, (size_t)count * sizeof(T)); }
+    return (T *)p;
+}
+
+cudaError_t launch_conv(int nimg, int H, int W, const bf16 *x, int ldx, const bf16 *w, int cin, int cout,
+                        const float *bias, float *z, bf16 *y, int ldy, float *yf, int ldyf, int accumulate, int act,
+                        cudaStream_t st)
+{
+    ConvArgs a;
+    a.x = x; a.ldx = ldx; a.w = w; a.bias = bias; a.z = z; a.y = y; a.ldy = ldy; a.yf = yf; a.ldyf = ldyf;
+    a.accumulate = accumulate; a.act = act; a.nimg = nimg; a.H = H; a.W = W; a.cin = cin; a.cout = cout;
+    const unsigned tiles = (unsigned)(((H + kTileH - 1) / kTileH) * ((W + kTileW - 1) / kTileW));
+    if (cout % 64 == 0) k_conv3x3<64><<<dim3(tiles, cout / 64, nimg), 128, 0, st>>>(a);
+    else if (cout % 32 == 0) k_conv3x3<32><<<dim3(tiles, cout / 32, nimg), 128, 0, st>>>(a);
+    else k_conv3x3<16><<<dim3(tiles, cout / 16, nimg), 128, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_wgrad(int nimg, int H, int W, const bf16 *x, int ldx, const bf16 *dz, float *dw, int cin, int cout,
+                         cudaStream_t st)
+{
+    WgradArgs a;
+    a.x = x; a.ldx = ldx; a.dz = dz; a.dw = dw; a.nimg = nimg; a.H = H; a.W = W; a.cin = cin; a.cout = cout;
+    const int ntiles = nimg * ((H + kTileH - 1) / kTileH) * ((W + kTileW - 1) / kTileW);
+    const int cx = cin / 16, cy = (cout + 63) / 64;
+    int z = (148 * 4 + cx * cy - 1) / (cx * cy);
+    if (z > ntiles) z = ntiles;
+    if (z < 1) z = 1;
+    k_conv3x3_wgrad<<<dim3(cx, cy, z), 128, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+extern "C" long m2d_unet_param_count(void)
+{
+    // conv layers in network order (input channels, output channels)
+    static const int io[kConvs][2] = {{16, 16}, {16, 16}, {16, 32}, {32, 32}, {32, 64}, {64, 64}, {64, 128},
+                                      {128, 128}, {192, 64}, {64, 64}, {96, 32}, {32, 32}, {48, 16}, {16, 16}};
+    long n = 0;
+    for (auto &l : io) n += (long)l[1] * 9 * l[0] + l[1];
+    return n + 17;
+}
+
+extern "C" int m2d_unet_create(int bmax, int H, int W, int device, m2d_unet **out)
+{
+    if (!out || bmax < 1 || H < 8 || W < 8 || H % 8 || W % 8)
+        return unet_fail(M2D_ERR_ARG, "m2d_unet_create: need batch >= 1 and H, W multiples of 8");
+    *out = nullptr;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) { m2d_set_last_error(e, "cudaSetDevice", __FILE__, __LINE__); return M2D_ERR_CUDA; }
+    m2d_unet *n = new m2d_unet();
+    n->device = device; n->bmax = bmax; n->H = H; n->W = W;
+    for (int l = 0; l < kLevels; l++) n->P[l] = (long long)bmax * (H >> l) * (W >> l);
+    static const int io[kConvs][3] = {{16, 16, 0}, {16, 16, 0}, {16, 32, 1}, {32, 32, 1}, {32, 64, 2}, {64, 64, 2},
+                                      {64, 128, 3}, {128, 128, 3}, {192, 64, 2}, {64, 64, 2}, {96, 32, 1}, {32, 32, 1},
+                                      {48, 16, 0}, {16, 16, 0}};
+    long long off = 0;
+    for (int k = 0; k < kConvs; k++) {
+        ConvLayer &c = n->L[k];
+        c.cin = io[k][0]; c.cout = io[k][1]; c.level = io[k][2];
+        c.woff = off; off += (long long)c.cout * 9 * c.cin;
+        c.boff = off; off += c.cout;
+    }
+    n->nparam = off + 17;     // head: 16 weights + bias
+    const long long *P = n->P;
+    n->params = dalloc<float>(n, n->nparam, e);
+    n->grads = dalloc<float>(n, n->nparam, e);
+    n->adam_m = dalloc<float>(n, n->nparam, e);
+    n->adam_v = dalloc<float>(n, n->nparam, e);
+    for (int k = 0; k < kConvs; k++) {
+        ConvLayer &c = n->L[k];
+        c.wb = dalloc<bf16>(n, (long long)c.cout * 9 * c.cin, e);
+        c.wt = dalloc<bf16>(n, (long long)c.cout * 9 * c.cin, e);
+        c.z = dalloc<float>(n, P[c.level] * c.cout, e);
+    }
+    // activations: D[l] = [up from level l+1 | skip of level l]
+    const int dch[3] = {48, 96, 192}, upch[3] = {32, 64, 128};
+    n->in0 = dalloc<bf16>(n, P[0] * 16, e);
+    for (int l = 0; l < 3; l++) {
+        n->D[l] = dalloc<bf16>(n, P[l] * dch[l], e);
+        n->pooled[l] = dalloc<bf16>(n, P[l + 1] * kChan[l], e);
+        n->U[l] = dalloc<bf16>(n, P[l] * kChan[l], e);
+        n->dD[l] = dalloc<float>(n, P[l] * dch[l], e);
+        n->dpool[l] = dalloc<float>(n, P[l + 1] * kChan[l], e);
+    }
+    n->e3b = dalloc<bf16>(n, P[3] * 128, e);
+    bf16 *ea[4], *da[3];
+    float *dea[4], *dda[3], *dU[3], *de3b;
+    for (int l = 0; l < 4; l++) { ea[l] = dalloc<bf16>(n, P[l] * kChan[l], e); dea[l] = dalloc<float>(n, P[l] * kChan[l], e); }
+    for (int l = 0; l < 3; l++) {
+        da[l] = dalloc<bf16>(n, P[l] * kChan[l], e); dda[l] = dalloc<float>(n, P[l] * kChan[l], e);
+        dU[l] = dalloc<float>(n, P[l] * kChan[l], e);
+    }
+    de3b = dalloc<float>(n, P[3] * 128, e);
+    n->out = dalloc<float>(n, P[0], e);
+    n->dout = dalloc<float>(n, P[0], e);
+    n->loss = dalloc<float>(n, 1, e);
+    n->dz = dalloc<bf16>(n, P[0] * 16 > P[3] * 128 ? P[0] * 16 : P[3] * 128, e);
+    n->dU0 = dU[0];
+    const long long cells = (long long)(H + 2) * (W + 2);
+    n->feat = dalloc<float>(n, (long long)kInPlanes * H * W, e);
+    n->yout = dalloc<float>(n, (long long)H * W, e);
+    n->r = dalloc<double>(n, cells, e);
+    n->x1 = dalloc<double>(n, cells, e);
+    n->stats = dalloc<double>(n, 16, e);
+    n->nit = dalloc<int>(n, 4, e);
+    if (e != cudaSuccess) {
+        m2d_set_last_error(e, "m2d_unet_create: allocation", __FILE__, __LINE__);
+        m2d_unet_destroy(n);
+        return M2D_ERR_NOMEM;
+    }
+    // wiring (see the file comment for the level structure)
+    auto enc = [&](int k1, int l, const bf16 *xin, int ldxin, float *dxin) {
+        ConvLayer &a = n->L[k1], &b = n->L[k1 + 1];
+        a.x = xin; a.ldx = ldxin; a.y = ea[l]; a.ldy = kChan[l]; a.dy = dea[l]; a.lddy = kChan[l];
+        a.dx = dxin; a.lddx = a.cin;
+        b.x = ea[l]; b.ldx = kChan[l]; b.dx = dea[l]; b.lddx = kChan[l];
+        if (l < 3) {
+            b.y = n->D[l] + upch[l]; b.ldy = dch[l]; b.dy = n->dD[l] + upch[l]; b.lddy = dch[l];
+        } else {
+            b.y = n->e3b; b.ldy = 128; b.dy = de3b; b.lddy = 128;
+        }
+    };
+    enc(0, 0, n->in0, 16, nullptr);
+    enc(2, 1, n->pooled[0], 16, n->dpool[0]);
+    enc(4, 2, n->pooled[1], 32, n->dpool[1]);
+    enc(6, 3, n->pooled[2], 64, n->dpool[2]);
+    auto dec = [&](int k1, int l) {
+        ConvLayer &a = n->L[k1], &b = n->L[k1 + 1];
+        a.x = n->D[l]; a.ldx = dch[l]; a.y = da[l]; a.ldy = kChan[l]; a.dy = dda[l]; a.lddy = kChan[l];
+        a.dx = n->dD[l]; a.lddx = dch[l];
+        b.x = da[l]; b.ldx = kChan[l]; b.y = n->U[l]; b.ldy = kChan[l]; b.dy = dU[l]; b.lddy = kChan[l];
+        b.dx = dda[l]; b.lddx = kChan[l];
+    };
+    dec(8, 2);
+    dec(10, 1);
+    dec(12, 0);
+    *out = n;
+    return M2D_OK;
+}
+
+extern "C" int m2d_unet_destroy(m2d_unet *n)
+{
+    if (!n) return M2D_OK;
+    cudaSetDevice(n->device);
+    cudaDeviceSynchronize();
+    for (void *p : n->allocs) cudaFree(p);
+    delete n;
+    return M2D_OK;
+}
+
+static cudaError_t sync_weights(m2d_unet *n, cudaStream_t st)
+{
+    for (int k = 0; k < kConvs; k++) {
+        ConvLayer &c = n->L[k];
+        k_sync_weights<<<grid_for((long long)c.cout * 9 * c.cin), 256, 0, st>>>(c.cin, c.cout, n->params + c.woff, c.wb, c.wt);
+    }
+    return cudaGetLastError();
+}
+
+extern "C" int m2d_unet_set_params(m2d_unet *n, const float *host, long count)
+{
+    if (!n || !host || count != n->nparam) return unet_fail(M2D_ERR_ARG, "m2d_unet_set_params: size mismatch");
+    cudaSetDevice(n->device);
+    cudaError_t e = cudaMemcpy(n->params, host, (size_t)count * sizeof(float), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(n->adam_m, 0, (size_t)count * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemset(n->adam_v, 0, (size_t)count * sizeof(float));
+    if (e == cudaSuccess) e = sync_weights(n, 0);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    n->adam_step = 0;
+    if (e != cudaSuccess) { m2d_set_last_error(e, "m2d_unet_set_params", __FILE__, __LINE__); return M2D_ERR_CUDA; }
+    return M2D_OK;
+}
+
+static int copy_out(m2d_unet *n, const float *src, float *host, long count, const char *what)
+{
+    if (!n || !host || count != n->nparam) return unet_fail(M2D_ERR_ARG, what);
+    cudaSetDevice(n->device);
+    cudaError_t e = cudaMemcpy(host, src, (size_t)count * sizeof(float), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) { m2d_set_last_error(e, what, __FILE__, __LINE__); return M2D_ERR_CUDA; }
+    return M2D_OK;
+}
+extern "C" int m2d_unet_get_params(m2d_unet *n, float *host, long count)
+{ return copy_out(n, n ? n->params : nullptr, host, count, "m2d_unet_get_params"); }
+extern "C" int m2d_unet_get_grads(m2d_unet *n, float *host, long count)
+{ return copy_out(n, n ? n->grads : nullptr, host, count, "m2d_unet_get_grads"); }
+
+// forward pass of nimg images; d_in: [img][11][H][W] FP32 planes; d_out: [img][H][W]
+static cudaError_t forward(m2d_unet *n, int nimg, const float *d_in, float *d_out, bool train, cudaStream_t st)
+{
+    const int H = n->H, W = n->W;
+    k_pack_input<<<grid_for((long long)nimg * H * W), 256, 0, st>>>(nimg, H, W, d_in, n->in0);
+    cudaError_t e = cudaGetLastError();
+    auto conv = [&](int k) {
+        ConvLayer &c = n->L[k];
+        const int lh = H >> c.level, lw = W >> c.level;
+        if (e == cudaSuccess)
+            e = launch_conv(nimg, lh, lw, c.x, c.ldx, c.wb, c.cin, c.cout, n->params + c.boff, train ? c.z : nullptr,
+                            c.y, c.ldy, nullptr, 0, 0, 1, st);
+    };
+    const int upch[3] = {32, 64, 128}, dch[3] = {48, 96, 192};
+    for (int l = 0; l < 4; l++) {
+        conv(2 * l);
+        conv(2 * l + 1);
+        if (l < 3 && e == cudaSuccess) {
+            const int lh = H >> l, lw = W >> l;
+            k_pool<<<grid_for((long long)nimg * (lh / 2) * (lw / 2) * kChan[l]), 256, 0, st>>>(
+                nimg, lh, lw, kChan[l], n->D[l] + upch[l], dch[l], n->pooled[l]);
+            e = cudaGetLastError();
+        }
+    }
+    for (int l = 2; l >= 0; l--) {
+        const bf16 *src = (l == 2) ? n->e3b : n->U[l + 1];
+        const int lh = H >> l, lw = W >> l;
+        if (e == cudaSuccess) {
+            k_up<<<grid_for((long long)nimg * lh * lw * upch[l]), 256, 0, st>>>(nimg, lh, lw, upch[l], src, n->D[l], dch[l]);
+            e = cudaGetLastError();
+        }
+        conv(8 + 2 * (2 - l));
+        conv(9 + 2 * (2 - l));
+    }
+    if (e == cudaSuccess) {
+        k_head<<<grid_for((long long)nimg * H * W), 256, 0, st>>>((long long)nimg * H * W, n->U[0],
+                                                                 n->params + (n->nparam - 17), d_out);
+        e = cudaGetLastError();
+    }
+    return e;
+}
+
+extern "C" int m2d_unet_forward(m2d_unet *n, int nimg, const float *d_in, float *d_out, void *stream)
+{
+    if (!n || !d_in || !d_out || nimg < 1 || nimg > n->bmax) return unet_fail(M2D_ERR_ARG, "m2d_unet_forward: bad arguments");
+    cudaError_t e = forward(n, nimg, d_in, d_out, false, (cudaStream_t)stream);
+    if (e != cudaSuccess) { m2d_set_last_error(e, "m2d_unet_forward", __FILE__, __LINE__); return M2D_ERR_CUDA; }
+    return M2D_OK;
+}
+
+// one training step's gradients: forward, MSE loss against d_target over
+// d_mask (may be null), backward into the gradient array (zeroed first)
+extern "C" int m2d_unet_loss_grad(m2d_unet *n, int nimg, const float *d_in, const float *d_target, const float *d_mask,
+                                  float loss_scale, float *loss_host, void *stream)
+{
+    if (!n || !d_in || !d_target || nimg < 1 || nimg > n->bmax)
+        return unet_fail(M2D_ERR_ARG, "m2d_unet_loss_grad: bad arguments");
+    cudaStream_t st = (cudaStream_t)stream;
+    const int H = n->H, W = n->W;
+    const long long P0 = (long long)nimg * H * W;
+    cudaError_t e = forward(n, nimg, d_in, n->out, true, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(n->grads, 0, (size_t)n->nparam * sizeof(float), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(n->loss, 0, sizeof(float), st);
+    if (e == cudaSuccess) {
+        k_loss<<<grid_for(P0), 256, 0, st>>>(P0, n->out, d_target, d_mask, loss_scale, n->dout, n->loss);
+        k_head_bwd<<<grid_for(P0), 256, 0, st>>>(P0, n->U[0], n->params + (n->nparam - 17), n->dout, n->dU0,
+                                                 n->grads + (n->nparam - 17));
+        e = cudaGetLastError();
+    }
+    const int upch[3] = {32, 64, 128}, dch[3] = {48, 96, 192};
+    // one conv layer backwards: dZ, dW, db, and dX when the layer has an input gradient
+    auto back = [&](int k) {
+        ConvLayer &c = n->L[k];
+        const int lh = H >> c.level, lw = W >> c.level;
+        const long long np = (long long)nimg * lh * lw;
+        if (e != cudaSuccess) return;
+        k_gelu_bwd<<<grid_for(np * c.cout), 256, 0, st>>>(np, c.cout, c.dy, c.lddy, c.z, n->dz, n->grads + c.boff);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = launch_wgrad(nimg, lh, lw, c.x, c.ldx, n->dz, n->grads + c.woff, c.cin, c.cout, st);
+        if (e == cudaSuccess && c.dx)
+            e = launch_conv(nimg, lh, lw, n->dz, c.cout, c.wt, c.cout, c.cin, nullptr, nullptr, nullptr, 0, c.dx,
+                            c.lddx, 0, 0, st);
+    };
+    for (int l = 0; l < 3; l++) {          // decoder, finest level first
+        back(13 - 2 * l);
+        back(12 - 2 * l);
+        // dD[l][:, 0:upch] -> gradient of the upsampled tensor
+        const int li = l + 1, lh = H >> li, lw = W >> li;
+        float *dsrc = (l == 2) ? n->L[7].dy : n->L[11 - 2 * l].dy;
+        if (e == cudaSuccess) {
+            k_up_bwd<<<grid_for((long long)nimg * lh * lw * upch[l]), 256, 0, st>>>(nimg, lh, lw, upch[l], n->dD[l],
+                                                                                    dch[l], dsrc);
+            e = cudaGetLastError();
+        }
+    }
+    for (int l = 3; l >= 0; l--) {         // encoder, coarsest level first
+        back(2 * l + 1);
+        back(2 * l);
+        if (l > 0 && e == cudaSuccess) {
+            // pooled[l-1] gradient -> skip slice of D[l-1]
+            const int lh = H >> (l - 1), lw = W >> (l - 1);
+            k_pool_bwd<<<grid_for((long long)nimg * lh * lw * kChan[l - 1]), 256, 0, st>>>(
+                nimg, lh, lw, kChan[l - 1], n->dpool[l - 1], n->dD[l - 1] + upch[l - 1], dch[l - 1]);
+            e = cudaGetLastError();
+        }
+    }
+    if (e == cudaSuccess && loss_host) {
+        e = cudaMemcpyAsync(loss_host, n->loss, sizeof(float), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    }
+    if (e != cudaSuccess) { m2d_set_last_error(e, "m2d_unet_loss_grad", __FILE__, __LINE__); return M2D_ERR_CUDA; }
+    return M2D_OK;
+}
+
+extern "C" int m2d_unet_adam(m2d_unet *n, float lr, float beta1, float beta2, float eps, void *stream)
+{
+    if (!n || !(lr > 0.f)) return unet_fail(M2D_ERR_ARG, "m2d_unet_adam: bad arguments");
+    cudaStream_t st = (cudaStream_t)stream;
+    n->adam_step++;
+    const float c1 = 1.f - powf(beta1, (float)n->adam_step), c2 = 1.f - powf(beta2, (float)n->adam_step);
+    k_adam<<<grid_for(n->nparam), 256, 0, st>>>(n->nparam, n->params, n->grads, n->adam_m, n->adam_v, lr, beta1, beta2,
+                                                eps, c1, c2);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = sync_weights(n, st);
+    if (e != cudaSuccess) { m2d_set_last_error(e, "m2d_unet_adam", __FILE__, __LINE__); return M2D_ERR_CUDA; }
+    return M2D_OK;
+}
+
+extern "C" int m2d_unet_shape(const m2d_unet *n, int *bmax, int *H, int *W)
+{
+    if (!n) return unet_fail(M2D_ERR_ARG, "m2d_unet_shape: null network");
+    if (bmax) *bmax = n->bmax;
+    if (H) *H = n->H;
+    if (W) *W = n->W;
+    return M2D_OK;
+}
+
+// ------------------------------------------------- p' system <-> network images
+// Pixel (y, x) of an H x W image is real cell (i, j) = (x + 2, y + 2) of an
+// nx x ny system (nx - 2 <= W, ny - 2 <= H); pixels outside are zero.
+namespace {
+
+constexpr int kStatThreads = 1024;
+
+// one block: deterministic sums over the real cells.  mode 0: sum r^2 into
+// s[0]; mode 1: also sum (r/aP)^2, log Jp, (log Jp)^2 into s[1..3] and the
+// derived sigma, mean and standard deviation of log Jp into s[4..6]
+__global__ void __launch_bounds__(kStatThreads) k_sys_stats(int nx, int ny, const double *a5, const double *r,
+                                                            const double *Jp, double *s, int mode)
+{
+    __shared__ double red[4][kStatThreads / 32];
+    const long long N = (long long)nx * ny;
+    const long long nreal = (long long)(nx - 2) * (ny - 2);
+    double v[4] = {0, 0, 0, 0};
+    for (long long k = threadIdx.x; k < nreal; k += kStatThreads) {
+        const int j = (int)(k / (nx - 2)) + 2, i = (int)(k % (nx - 2)) + 2;
+        const long long np = (long long)(j - 1) * nx + (i - 1);
+        const double rv = r[np];
+        v[0] += rv * rv;
+        if (mode) {
+            const double rh = rv / a5[2 * N + np];
+            const double lj = log(Jp[np]);
+            v[1] += rh * rh; v[2] += lj; v[3] += lj * lj;
+        }
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    for (int q = 0; q < 4; q++) {
+        double t = v[q];
+        for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+        if (l == 0) red[q][w] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t[4] = {0, 0, 0, 0};
+        for (int q = 0; q < 4; q++)
+            for (int k = 0; k < kStatThreads / 32; k++) t[q] += red[q][k];
+        s[0] = t[0];
+        if (mode) {
+            s[1] = t[1]; s[2] = t[2]; s[3] = t[3];
+            const double sig = sqrt(t[1] / (double)nreal);
+            const double mean = t[2] / (double)nreal;
+            const double var = t[3] / (double)nreal - mean * mean;
+            s[4] = sig > 0.0 ? sig : 1.0;
+            s[5] = mean;
+            s[6] = var > 1e-24 ? sqrt(var) : 1.0;
+        }
+    }
+}
+
+// r = b - A x on the real cells (5 diagonals S, W, P, E, N), zero elsewhere
+__global__ void k_residual5(int nx, int ny, const double *a5, const double *b, const double *x, double *r)
+{
+    const long long N = (long long)nx * ny;
+    for (long long np = (long long)blockIdx.x * blockDim.x + threadIdx.x; np < N; np += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(np / nx) + 1, i = (int)(np - (long long)(j - 1) * nx) + 1;
+        if (i == 1 || i == nx || j == 1 || j == ny) { r[np] = 0.0; continue; }
+        const double ax = a5[np] * x[np - nx] + a5[N + np] * x[np - 1] + a5[2 * N + np] * x[np] +
+                          a5[3 * N + np] * x[np + 1] + a5[4 * N + np] * x[np + nx];
+        r[np] = b[np] - ax;
+    }
+}
+
+// the 11 input planes: r / (aP sigma), the nine coefficients over aP
+// (SW, S, SE, W, P, E, NW, N, NE; corners zero for a 5-diagonal system) and
+// the standardised log Jp
+__global__ void k_features(int nx, int ny, int H, int W, const double *a5, const double *r, const double *Jp,
+                           const double *s, float *feat)
+{
+    const long long N = (long long)nx * ny, HW = (long long)H * W;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < HW; p += (long long)gridDim.x * blockDim.x) {
+        const int y = (int)(p / W), x = (int)(p - (long long)y * W);
+        float f[11];
+#pragma unroll
+        for (int c = 0; c < 11; c++) f[c] = 0.f;
+        if (x < nx - 2 && y < ny - 2) {
+            const long long np = (long long)(y + 1) * nx + (x + 1);
+            const double ap = a5[2 * N + np];
+            f[0] = (float)(r[np] / ap / s[4]);
+            f[2] = (float)(a5[np] / ap);
+            f[4] = (float)(a5[N + np] / ap);
+            f[5] = 1.f;
+            f[6] = (float)(a5[3 * N + np] / ap);
+            f[8] = (float)(a5[4 * N + np] / ap);
+            f[10] = (float)((log(Jp[np]) - s[5]) / s[6]);
+        }
+#pragma unroll
+        for (int c = 0; c < 11; c++) feat[c * HW + p] = f[c];
+    }
+}
+
+// xout = x + sigma y on the real cells, x elsewhere
+__global__ void k_apply(int nx, int ny, int H, int W, const float *y, const double *s, const double *x, double *xout)
+{
+    const long long N = (long long)nx * ny;
+    for (long long np = (long long)blockIdx.x * blockDim.x + threadIdx.x; np < N; np += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(np / nx) + 1, i = (int)(np - (long long)(j - 1) * nx) + 1;
+        double v = x[np];
+        if (i > 1 && i < nx && j > 1 && j < ny) v += s[4] * (double)y[(long long)(j - 2) * W + (i - 2)];
+        xout[np] = v;
+    }
+}
+
+// training target t = delta / sigma and mask (1 on real cells)
+__global__ void k_target(int nx, int ny, int H, int W, const double *delta, const double *s, float *t, float *mask)
+{
+    const long long HW = (long long)H * W;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < HW; p += (long long)gridDim.x * blockDim.x) {
+        const int y = (int)(p / W), x = (int)(p - (long long)y * W);
+        const bool in = x < nx - 2 && y < ny - 2;
+        t[p] = in ? (float)(delta[(long long)(y + 1) * nx + (x + 1)] / s[4]) : 0.f;
+        if (mask) mask[p] = in ? 1.f : 0.f;
+    }
+}
+
+bool image_fits(int nx, int ny, int H, int W) { return nx >= 4 && ny >= 4 && nx - 2 <= W && ny - 2 <= H; }
+
+}  // namespace
+
+extern "C" int m2d_residual5(int nx, int ny, const double *d_a, const double *d_b, const double *d_x, double *d_r,
+                             double *d_rr, void *stream)
+{
+    if (nx < 3 || ny < 3 || !d_a || !d_b || !d_x || !d_r) return unet_fail(M2D_ERR_ARG, "m2d_residual5: bad arguments");
+    cudaStream_t st = (cudaStream_t)stream;
+    k_residual5<<<grid_for((long long)nx * ny), 256, 0, st>>>(nx, ny, d_a, d_b, d_x, d_r);
+    if (d_rr) k_sys_stats<<<1, kStatThreads, 0, st>>>(nx, ny, d_a, d_r, nullptr, d_rr, 0);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) { m2d_set_last_error(e, "m2d_residual5", __FILE__, __LINE__); return M2D_ERR_CUDA; }
+    return M2D_OK;
+}
+
+extern "C" int m2d_pprime_features(int nx, int ny, int H, int W, const double *d_a, const double *d_r,
+                                   const double *d_Jp, float *d_feat, double *d_stats, void *stream)
+{
+    if (!image_fits(nx, ny, H, W) || !d_a || !d_r || !d_Jp || !d_feat || !d_stats)
+        return unet_fail(M2D_ERR_ARG, "m2d_pprime_features: bad arguments");
+    cudaStream_t st = (cudaStream_t)stream;
+    k_sys_stats<<<1, kStatThreads, 0, st>>>(nx, ny, d_a, d_r, d_Jp, d_stats, 1);
+    k_features<<<grid_for((long long)H * W), 256, 0, st>>>(nx, ny, H, W, d_a, d_r, d_Jp, d_stats, d_feat);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) { m2d_set_last_error(e, "m2d_pprime_features", __FILE__, __LINE__); return M2D_ERR_CUDA; }
+    return M2D_OK;
+}
+
+extern "C" int m2d_pprime_apply(int nx, int ny, int H, int W, const float *d_y, const double *d_stats,
+                                const double *d_x, double *d_xout, void *stream)
+{
+    if (!image_fits(nx, ny, H, W) || !d_y || !d_stats || !d_x || !d_xout)
+        return unet_fail(M2D_ERR_ARG, "m2d_pprime_apply: bad arguments");
+    k_apply<<<grid_for((long long)nx * ny), 256, 0, (cudaStream_t)stream>>>(nx, ny, H, W, d_y, d_stats, d_x, d_xout);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) { m2d_set_last_error(e, "m2d_pprime_apply", __FILE__, __LINE__); return M2D_ERR_CUDA; }
+    return M2D_OK;
+}
+
+extern "C" int m2d_pprime_target(int nx, int ny, int H, int W, const double *d_delta, const double *d_stats,
+                                 float *d_t, float *d_mask, void *stream)
+{
+    if (!image_fits(nx, ny, H, W) || !d_delta || !d_stats || !d_t)
+        return unet_fail(M2D_ERR_ARG, "m2d_pprime_target: bad arguments");
+    k_target<<<grid_for((long long)H * W), 256, 0, (cudaStream_t)stream>>>(nx, ny, H, W, d_delta, d_stats, d_t, d_mask);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) { m2d_set_last_error(e, "m2d_pprime_target", __FILE__, __LINE__); return M2D_ERR_CUDA; }
+    return M2D_OK;
+}
+
+extern "C" int m2d_msi_solve_device_ws(int nd, int nx, int ny, int nitm, double tol, const double *d_a,
+                                       const double *d_b, double *d_x, double *d_work, long work_doubles,
+                                       void *stream, int *d_nit, unsigned long long *d_times, int prec);
+extern "C" long m2d_msi_workspace_doubles(int nd, int nx, int ny);
+
+// Flexible pressure-correction solve: the network's correction first, kept
+// only if it lowers |b - A x|; then the MSI iteration, whose stopping test
+// stays relative to the residual before the correction.
+extern "C" int m2d_pprime_solve_learned(m2d_unet *n, int nx, int ny, int nitm, double tol, const double *d_a,
+                                        const double *d_b, double *d_x, const double *d_Jp, double *d_work, int prec,
+                                        void *stream, m2d_learned_report *rep)
+{
+    if (!n || !image_fits(nx, ny, n->H, n->W) || !d_a || !d_b || !d_x || !d_Jp || !d_work || nitm < 1)
+        return unet_fail(M2D_ERR_ARG, "m2d_pprime_solve_learned: bad arguments");
+    cudaStream_t st = (cudaStream_t)stream;
+    const int H = n->H, W = n->W;
+    const long long N = (long long)nx * ny;
+    double *s = n->stats;       // s[0..6] features, s[8] |r0|^2, s[9] |r1|^2
+    k_residual5<<<grid_for(N), 256, 0, st>>>(nx, ny, d_a, d_b, d_x, n->r);
+    k_sys_stats<<<1, kStatThreads, 0, st>>>(nx, ny, d_a, n->r, d_Jp, s, 1);
+    k_features<<<grid_for((long long)H * W), 256, 0, st>>>(nx, ny, H, W, d_a, n->r, d_Jp, s, n->feat);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = forward(n, 1, n->feat, n->yout, false, st);
+    if (e == cudaSuccess) {
+        k_apply<<<grid_for(N), 256, 0, st>>>(nx, ny, H, W, n->yout, s, d_x, n->x1);
+        k_residual5<<<grid_for(N), 256, 0, st>>>(nx, ny, d_a, d_b, n->x1, n->r);
+        k_sys_stats<<<1, kStatThreads, 0, st>>>(nx, ny, d_a, n->r, nullptr, s + 9, 0);
+        e = cudaGetLastError();
+    }
+    double hs[10];
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hs, s, sizeof hs, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) { m2d_set_last_error(e, "m2d_pprime_solve_learned", __FILE__, __LINE__); return M2D_ERR_CUDA; }
+    const double r0 = std::sqrt(hs[0]), r1 = std::sqrt(hs[9]);
+    const bool accept = std::isfinite(r1) && r1 < r0;
+    double tol_eff = tol;
+    if (accept) {
+        e = cudaMemcpyAsync(d_x, n->x1, (size_t)N * sizeof(double), cudaMemcpyDeviceToDevice, st);
+        tol_eff = r1 > 0.0 ? tol * r0 / r1 : 2.0;
+    }
+    int nit = 0;
+    if (e == cudaSuccess && tol_eff < 1.0) {
+        const int rc = m2d_msi_solve_device_ws(5, nx, ny, nitm, tol_eff, d_a, d_b, d_x, d_work,
+                                               m2d_msi_workspace_doubles(5, nx, ny), stream, n->nit, nullptr, prec);
+        if (rc) return rc;
+        e = cudaMemcpyAsync(&nit, n->nit, sizeof(int), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    }
+    if (e != cudaSuccess) { m2d_set_last_error(e, "m2d_pprime_solve_learned", __FILE__, __LINE__); return M2D_ERR_CUDA; }
+    if (rep) { rep->accepted = accept ? 1 : 0; rep->r0 = r0; rep->r1 = r1; rep->nit = nit; }
+    return M2D_OK;
+}
