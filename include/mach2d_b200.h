@@ -464,6 +464,13 @@ typedef struct m2d_learned_report {
 int m2d_pprime_solve_learned(m2d_unet *net, int nx, int ny, int nitm, double tol,
                              const double *d_a, const double *d_b, double *d_x, const double *d_Jp,
                              double *d_work, int prec, void *stream, m2d_learned_report *rep);
+/* Two-level cycles: the network's correction (kept only when it lowers |r|)
+ * alternating with m MSI iterations until |r| <= tol |r0| or max_cycles;
+ * rep->nit counts every MSI iteration, rep->accepted the kept corrections,
+ * rep->r1 is the final |r|. */
+int m2d_pprime_solve_cycles(m2d_unet *net, int nx, int ny, int m, int max_cycles, double tol,
+                            const double *d_a, const double *d_b, double *d_x, const double *d_Jp,
+                            double *d_work, int prec, void *stream, m2d_learned_report *rep);
 int m2d_batch_destroy(m2d_batch *b);
 
 #ifdef __cplusplus

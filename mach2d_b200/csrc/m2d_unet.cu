@@ -1016,3 +1016,74 @@ extern "C" int m2d_pprime_solve_learned(m2d_unet *n, int nx, int ny, int nitm, d
     if (rep) { rep->accepted = accept ? 1 : 0; rep->r0 = r0; rep->r1 = r1; rep->nit = nit; }
     return M2D_OK;
 }
+
+// Two-level cycles: the network's correction (kept only if it lowers |r|)
+// alternating with m MSI iterations, until |r| <= tol |r0| or max_cycles.
+// rep->nit counts all MSI iterations, rep->accepted the kept corrections,
+// rep->r0 and rep->r1 the initial and final |r|.
+extern "C" int m2d_pprime_solve_cycles(m2d_unet *n, int nx, int ny, int m, int max_cycles, double tol,
+                                       const double *d_a, const double *d_b, double *d_x, const double *d_Jp,
+                                       double *d_work, int prec, void *stream, m2d_learned_report *rep)
+{
+    if (!n || !image_fits(nx, ny, n->H, n->W) || !d_a || !d_b || !d_x || !d_Jp || !d_work || m < 1 || max_cycles < 1)
+        return unet_fail(M2D_ERR_ARG, "m2d_pprime_solve_cycles: bad arguments");
+    cudaStream_t st = (cudaStream_t)stream;
+    const int H = n->H, W = n->W;
+    const long long N = (long long)nx * ny;
+    double *s = n->stats;
+    const long wd = m2d_msi_workspace_doubles(5, nx, ny);
+    const double *rr = d_work + (wd - 4);      // the MSI call's |r0|^2, |r|^2
+    auto fail_cuda = [&](cudaError_t e) {
+        m2d_set_last_error(e, "m2d_pprime_solve_cycles", __FILE__, __LINE__);
+        return M2D_ERR_CUDA;
+    };
+    k_residual5<<<grid_for(N), 256, 0, st>>>(nx, ny, d_a, d_b, d_x, n->r);
+    k_sys_stats<<<1, kStatThreads, 0, st>>>(nx, ny, d_a, n->r, nullptr, s + 8, 0);
+    double h;
+    cudaError_t e = cudaMemcpyAsync(&h, s + 8, sizeof h, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return fail_cuda(e);
+    const double r0 = std::sqrt(h), goal = tol * r0;
+    double rcur = r0;
+    int accepted = 0, nit_total = 0;
+    for (int cyc = 0; cyc < max_cycles && rcur > goal; cyc++) {
+        // n->r holds b - A x here
+        k_sys_stats<<<1, kStatThreads, 0, st>>>(nx, ny, d_a, n->r, d_Jp, s, 1);
+        k_features<<<grid_for((long long)H * W), 256, 0, st>>>(nx, ny, H, W, d_a, n->r, d_Jp, s, n->feat);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = forward(n, 1, n->feat, n->yout, false, st);
+        if (e != cudaSuccess) return fail_cuda(e);
+        k_apply<<<grid_for(N), 256, 0, st>>>(nx, ny, H, W, n->yout, s, d_x, n->x1);
+        k_residual5<<<grid_for(N), 256, 0, st>>>(nx, ny, d_a, d_b, n->x1, n->r);
+        k_sys_stats<<<1, kStatThreads, 0, st>>>(nx, ny, d_a, n->r, nullptr, s + 9, 0);
+        e = cudaMemcpyAsync(&h, s + 9, sizeof h, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return fail_cuda(e);
+        const double r1 = std::sqrt(h);
+        if (std::isfinite(r1) && r1 < rcur) {
+            e = cudaMemcpyAsync(d_x, n->x1, (size_t)N * sizeof(double), cudaMemcpyDeviceToDevice, st);
+            if (e != cudaSuccess) return fail_cuda(e);
+            rcur = r1;
+            accepted++;
+            if (rcur <= goal) break;
+        }
+        const int rc = m2d_msi_solve_device_ws(5, nx, ny, m, goal / rcur, d_a, d_b, d_x, d_work, wd, stream, n->nit,
+                                               nullptr, prec);
+        if (rc) return rc;
+        int nit = 0;
+        double rrh[2];
+        e = cudaMemcpyAsync(&nit, n->nit, sizeof(int), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(rrh, rr, sizeof rrh, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return fail_cuda(e);
+        nit_total += nit;
+        rcur = std::sqrt(rrh[1]);
+        if (rcur > goal && cyc + 1 < max_cycles) {
+            k_residual5<<<grid_for(N), 256, 0, st>>>(nx, ny, d_a, d_b, d_x, n->r);
+            e = cudaGetLastError();
+            if (e != cudaSuccess) return fail_cuda(e);
+        }
+    }
+    if (rep) { rep->accepted = accepted; rep->r0 = r0; rep->r1 = rcur; rep->nit = nit_total; }
+    return M2D_OK;
+}

@@ -43,6 +43,8 @@ def _bind():
     L.m2d_pprime_target.argtypes = [_int] * 4 + [_vp] * 4 + [_vp]
     L.m2d_pprime_solve_learned.argtypes = [_vp, _int, _int, _int, _d] + [_vp] * 5 + [_int, _vp,
                                                                                         ctypes.POINTER(LearnedReport)]
+    L.m2d_pprime_solve_cycles.argtypes = [_vp, _int, _int, _int, _int, _d] + [_vp] * 5 + [_int, _vp,
+                                                                                     ctypes.POINTER(LearnedReport)]
     L.m2d_msi_workspace_doubles.restype = ctypes.c_long
     L.m2d_msi_workspace_doubles.argtypes = [_int] * 3
     L.m2d_msi_solve_device_ws.argtypes = [_int] * 4 + [_d] + [_vp] * 4 + [ctypes.c_long, _vp, _vp, _vp, _int]
@@ -134,6 +136,13 @@ class UNet:
         rep = LearnedReport()
         check(lib().m2d_pprime_solve_learned(self._h, nx, ny, nitm, tol, _ptr(a), _ptr(b), _ptr(x), _ptr(Jp),
                                              _ptr(work), prec, stream, ctypes.byref(rep)))
+        return rep
+
+    def solve_cycles(self, nx, ny, m, max_cycles, tol, a, b, x, Jp, work, prec=0, stream=None):
+        """Two-level cycles (m2d_pprime_solve_cycles) on device tensors."""
+        rep = LearnedReport()
+        check(lib().m2d_pprime_solve_cycles(self._h, nx, ny, m, max_cycles, tol, _ptr(a), _ptr(b), _ptr(x), _ptr(Jp),
+                                            _ptr(work), prec, stream, ctypes.byref(rep)))
         return rep
 
 
