@@ -344,7 +344,9 @@ typedef struct m2d_case {
     double Rg, gamma, mu, kappa;            /* CONSTANT thermophysical model (ktm = 0) */
     int itmmax, itpmax;
     double tolm, tolt;
-    int solver;                             /* 0 MSI, 1 TDMA, 2 MSI with FP32 factors and sweeps */
+    int solver;                             /* 0 MSI, 1 TDMA, 2 MSI with FP32 factors and sweeps,
+                                               3 as 2 with the learned p' correction first
+                                               (m2d_ctx_set_unet) */
     int nitm_u, nitm_p;
     double tol_u, tol_p;
     int dtmodel;                            /* 0 RAMP, 1 SCARBOROUGH */
@@ -385,6 +387,11 @@ int m2d_integrals(m2d_ctx *ctx, double *fmi, double *fme, double *Fd, double *Cd
 /* the cudaStream_t the context launches on, and the device address of a
  * named field (for callers that time or chain their own kernels) */
 int m2d_ctx_stream(const m2d_ctx *ctx, void **stream);
+/* the network of solver 3 (not owned; its images must hold the real cells);
+ * NULL detaches.  Scalars learned_calls / learned_accepted count the p'
+ * solves and the corrections kept. */
+struct m2d_unet;
+int m2d_ctx_set_unet(m2d_ctx *ctx, struct m2d_unet *net);
 int m2d_ctx_field_device(m2d_ctx *ctx, const char *name, double **dptr, long *n);
 
 /* ---- batches of instances (no counterpart in the reference) ------------
@@ -440,22 +447,25 @@ int m2d_unet_adam(m2d_unet *net, float lr, float beta1, float beta2, float eps, 
 /* p' system <-> images.  d_a: 5 planes (S, W, P, E, N), d_stats: 16 doubles.
  * Features: r/(aP sigma) with sigma the RMS of r/aP, the nine coefficient
  * planes over aP (SW, S, SE, W, P, E, NW, N, NE; corners zero), and the
- * standardised log Jp.  apply: x_out = x + sigma y.  target: t = delta /
- * sigma and mask = 1 on real cells.  residual5: r = b - A x on real cells,
- * *d_rr = |r|^2 (may be NULL). */
+ * standardised log Jp.  apply: x_out = x + sigma y on the real cells and,
+ * on the ghost ring, the value that satisfies the cell's own row given its
+ * corrected neighbours (x_out must not alias x).  target: t = delta /
+ * sigma and mask = 1 on real cells.  residual5: r = b - A x on every cell
+ * (the norm of the MSI stopping test), *d_rr = |r|^2 (may be NULL). */
 int m2d_residual5(int nx, int ny, const double *d_a, const double *d_b, const double *d_x,
                   double *d_r, double *d_rr, void *stream);
 int m2d_pprime_features(int nx, int ny, int H, int W, const double *d_a, const double *d_r,
                         const double *d_Jp, float *d_feat, double *d_stats, void *stream);
-int m2d_pprime_apply(int nx, int ny, int H, int W, const float *d_y, const double *d_stats,
-                     const double *d_x, double *d_xout, void *stream);
+int m2d_pprime_apply(int nx, int ny, int H, int W, const double *d_a, const double *d_b,
+                     const float *d_y, const double *d_stats, const double *d_x, double *d_xout,
+                     void *stream);
 int m2d_pprime_target(int nx, int ny, int H, int W, const double *d_delta, const double *d_stats,
                       float *d_t, float *d_mask, void *stream);
 /* Flexible pressure-correction solve of the 5-diagonal p' system: the
  * network's correction is kept only when it lowers |b - A x|; the MSI
  * iteration (prec 0 FP64, 1 FP32 sweeps) then runs with its stopping test
- * relative to the residual before the correction, and is skipped when the
- * correction alone meets it.  d_work: m2d_msi_workspace_doubles(5, nx, ny). */
+ * relative to the residual before the correction; like plain MSI it runs at
+ * least one iteration.  d_work: m2d_msi_workspace_doubles(5, nx, ny). */
 typedef struct m2d_learned_report {
     int accepted;          /* 1: the network's correction was kept */
     double r0, r1;         /* |r| before and after the correction */
@@ -465,7 +475,8 @@ int m2d_pprime_solve_learned(m2d_unet *net, int nx, int ny, int nitm, double tol
                              const double *d_a, const double *d_b, double *d_x, const double *d_Jp,
                              double *d_work, int prec, void *stream, m2d_learned_report *rep);
 /* Two-level cycles: the network's correction (kept only when it lowers |r|)
- * alternating with m MSI iterations until |r| <= tol |r0| or max_cycles;
+ * alternating with m MSI iterations (the last step of a cycle is always MSI)
+ * until |r| <= tol |r0| or max_cycles;
  * rep->nit counts every MSI iteration, rep->accepted the kept corrections,
  * rep->r1 is the final |r|. */
 int m2d_pprime_solve_cycles(m2d_unet *net, int nx, int ny, int m, int max_cycles, double tol,

@@ -36,6 +36,8 @@ struct m2d_ctx {
     double *dsc = nullptr;
     int *dint = nullptr;
     m2d_mixture *dmix = nullptr;   // device copy of c.mix (ktm = 1)
+    m2d_unet *net = nullptr;       // learned p' correction (solver 3), not owned
+    long long learned_calls = 0, learned_accepted = 0;
     double *hsc = nullptr;   // pinned mirror of dsc
     int *hint = nullptr;     // pinned mirror of dint
     double dt = 0, norm = 0, normpl = 0, rmass = 0, p_avg = 0;
@@ -132,7 +134,7 @@ extern "C" int m2d_create(const m2d_case *c, int device, m2d_ctx **out)
     // one arena: planes + 9N x 3 + 5N + strips + solver scratch + reductions
     const size_t nplanes = h.planes().size();
     const size_t strips = (size_t)9 * h.ny + 2 * (size_t)h.nx + 64;
-    const size_t solver = 2 * msi_work_doubles(9, h.nx, h.ny) + msi_work_doubles(5, h.nx, h.ny) + 2 * N + 3 * 32;
+    const size_t solver = 2 * msi_work_doubles(9, h.nx, h.ny) + msi_work_doubles(5, h.nx, h.ny) + 4 + 2 * N + 3 * 32;
     const size_t mixd = (sizeof(m2d_mixture) + sizeof(double) - 1) / sizeof(double);
     const size_t total = nplanes * N + 32 * N + strips + solver + (size_t)red_parts() + 64 + S_COUNT + mixd;
     e = cudaMalloc(&x->arena, total * sizeof(double));
@@ -153,7 +155,7 @@ extern "C" int m2d_create(const m2d_case *c, int device, m2d_ctx **out)
     // MSI scratch starts on 256-byte boundaries (one line per warp step)
     auto take_aligned = [&](size_t n) { cur = x->arena + (((size_t)(cur - x->arena) + 31) / 32) * 32; return take(n); };
     for (int k = 0; k < 2; k++) x->ws9[k] = take_aligned(msi_work_doubles(9, h.nx, h.ny));
-    x->ws5 = take_aligned(msi_work_doubles(5, h.nx, h.ny));
+    x->ws5 = take_aligned(msi_work_doubles(5, h.nx, h.ny) + 4);   // + the rr words of m2d_msi_workspace_doubles
     x->P = take(N); x->Q = take(N);
     x->part = take((size_t)red_parts() + 8);
     x->dsc = take(S_COUNT);
@@ -232,7 +234,7 @@ static int solve9(m2d_ctx *x, int nsys, double *const *a, double *const *b, doub
         MsiLaunch L;
         memset(&L, 0, sizeof L);
         L.nx = x->nx; L.ny = x->ny; L.nitm = c.nitm_u; L.tol = c.tol_u;
-        L.prec = (c.solver == 2) ? 1 : 0;
+        L.prec = (c.solver >= 2) ? 1 : 0;
         L.err = x->dint + I_ERR;
         for (int k = 0; k < nsys; k++) {
             L.s[k].a = a[k]; L.s[k].b = b[k]; L.s[k].x = v[k];
@@ -250,11 +252,22 @@ static int solve9(m2d_ctx *x, int nsys, double *const *a, double *const *b, doub
 static int solve5(m2d_ctx *x)
 {
     const m2d_case &c = x->c;
+    if (c.solver == 3) {
+        // flexible p' solve: the network's correction, then MSI with FP32 sweeps
+        if (!x->net) return ctx_fail(M2D_ERR_ARG, "m2d_iterate: solver 3 needs a network (m2d_ctx_set_unet)");
+        m2d_learned_report r;
+        const int rc = m2d_pprime_solve_learned(x->net, x->nx, x->ny, c.nitm_p, c.tol_p, x->f.ap, x->f.bp, x->f.pl,
+                                                x->f.Jp, x->ws5, 1, x->st, &r);
+        if (rc) return rc;
+        x->learned_calls++;
+        x->learned_accepted += r.accepted;
+        return M2D_OK;
+    }
     if (c.solver != 1) {
         MsiLaunch L;
         memset(&L, 0, sizeof L);
         L.nx = x->nx; L.ny = x->ny; L.nitm = c.nitm_p; L.tol = c.tol_p;
-        L.prec = (c.solver == 2) ? 1 : 0;
+        L.prec = (c.solver >= 2) ? 1 : 0;
         L.err = x->dint + I_ERR;
         L.s[0].a = x->f.ap; L.s[0].b = x->f.bp; L.s[0].x = x->f.pl;
         L.s[0].ws = x->ws5;
@@ -476,10 +489,23 @@ extern "C" int m2d_get_scalar(const m2d_ctx *x, const char *name, double *out)
         {"Fd1D", x->Fd1D}, {"Fpv1D", x->Fpv1D}, {"Sg", x->Sg}, {"it", (double)x->it},
         {"it_stop", (double)x->it_stop}, {"itp_used", (double)x->itp_used},
         {"launches", (double)x->launches}, {"nit_u", (double)x->hint[I_NIT_U]}, {"nit_v", (double)x->hint[I_NIT_V]},
-        {"nit_p", (double)x->hint[I_NIT_P]}, {"nit_T", (double)x->hint[I_NIT_T]}};
+        {"nit_p", (double)x->hint[I_NIT_P]}, {"nit_T", (double)x->hint[I_NIT_T]},
+        {"learned_calls", (double)x->learned_calls}, {"learned_accepted", (double)x->learned_accepted}};
     for (auto &t : tab)
         if (!strcmp(name, t.nm)) { *out = t.v; return M2D_OK; }
     return ctx_fail(M2D_ERR_ARG, "m2d_get_scalar: unknown scalar");
+}
+
+extern "C" int m2d_ctx_set_unet(m2d_ctx *x, m2d_unet *net)
+{
+    if (!x) return ctx_fail(M2D_ERR_ARG, "m2d_ctx_set_unet: null context");
+    if (net) {
+        int H = 0, W = 0;
+        m2d_unet_shape(net, nullptr, &H, &W);
+        if (x->nx - 2 > W || x->ny - 2 > H) return ctx_fail(M2D_ERR_ARG, "m2d_ctx_set_unet: network images smaller than the grid");
+    }
+    x->net = net;
+    return M2D_OK;
 }
 
 extern "C" int m2d_ctx_stream(const m2d_ctx *x, void **stream)

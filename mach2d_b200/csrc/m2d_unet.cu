@@ -803,9 +803,10 @@ namespace {
 
 constexpr int kStatThreads = 1024;
 
-// one block: deterministic sums over the real cells.  mode 0: sum r^2 into
-// s[0]; mode 1: also sum (r/aP)^2, log Jp, (log Jp)^2 into s[1..3] and the
-// derived sigma, mean and standard deviation of log Jp into s[4..6]
+// one block: deterministic sums.  s[0] = sum of r^2 over every cell (the
+// norm the MSI stopping test uses, msi2d5-v03.f90:68-120); mode 1 also sums
+// (r/aP)^2, log Jp, (log Jp)^2 over the real cells into s[1..3] and stores
+// sigma, the mean and the standard deviation of log Jp in s[4..6]
 __global__ void __launch_bounds__(kStatThreads) k_sys_stats(int nx, int ny, const double *a5, const double *r,
                                                             const double *Jp, double *s, int mode)
 {
@@ -813,17 +814,15 @@ __global__ void __launch_bounds__(kStatThreads) k_sys_stats(int nx, int ny, cons
     const long long N = (long long)nx * ny;
     const long long nreal = (long long)(nx - 2) * (ny - 2);
     double v[4] = {0, 0, 0, 0};
-    for (long long k = threadIdx.x; k < nreal; k += kStatThreads) {
-        const int j = (int)(k / (nx - 2)) + 2, i = (int)(k % (nx - 2)) + 2;
-        const long long np = (long long)(j - 1) * nx + (i - 1);
-        const double rv = r[np];
-        v[0] += rv * rv;
-        if (mode) {
-            const double rh = rv / a5[2 * N + np];
+    for (long long k = threadIdx.x; k < N; k += kStatThreads) v[0] += r[k] * r[k];
+    if (mode)
+        for (long long k = threadIdx.x; k < nreal; k += kStatThreads) {
+            const int j = (int)(k / (nx - 2)) + 2, i = (int)(k % (nx - 2)) + 2;
+            const long long np = (long long)(j - 1) * nx + (i - 1);
+            const double rh = r[np] / a5[2 * N + np];
             const double lj = log(Jp[np]);
             v[1] += rh * rh; v[2] += lj; v[3] += lj * lj;
         }
-    }
     const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
     for (int q = 0; q < 4; q++) {
         double t = v[q];
@@ -848,15 +847,18 @@ __global__ void __launch_bounds__(kStatThreads) k_sys_stats(int nx, int ny, cons
     }
 }
 
-// r = b - A x on the real cells (5 diagonals S, W, P, E, N), zero elsewhere
+// r = b - A x on every cell (5 diagonals S, W, P, E, N); a neighbour outside
+// the grid contributes nothing, as in the residual of msi2d5-v03.f90:68-120
 __global__ void k_residual5(int nx, int ny, const double *a5, const double *b, const double *x, double *r)
 {
     const long long N = (long long)nx * ny;
     for (long long np = (long long)blockIdx.x * blockDim.x + threadIdx.x; np < N; np += (long long)gridDim.x * blockDim.x) {
         const int j = (int)(np / nx) + 1, i = (int)(np - (long long)(j - 1) * nx) + 1;
-        if (i == 1 || i == nx || j == 1 || j == ny) { r[np] = 0.0; continue; }
-        const double ax = a5[np] * x[np - nx] + a5[N + np] * x[np - 1] + a5[2 * N + np] * x[np] +
-                          a5[3 * N + np] * x[np + 1] + a5[4 * N + np] * x[np + nx];
+        double ax = a5[2 * N + np] * x[np];
+        if (j > 1) ax += a5[np] * x[np - nx];
+        if (i > 1) ax += a5[N + np] * x[np - 1];
+        if (i < nx) ax += a5[3 * N + np] * x[np + 1];
+        if (j < ny) ax += a5[4 * N + np] * x[np + nx];
         r[np] = b[np] - ax;
     }
 }
@@ -889,15 +891,32 @@ __global__ void k_features(int nx, int ny, int H, int W, const double *a5, const
     }
 }
 
-// xout = x + sigma y on the real cells, x elsewhere
-__global__ void k_apply(int nx, int ny, int H, int W, const float *y, const double *s, const double *x, double *xout)
+// xout = x + sigma y on the real cells; on the ghost ring, the value that
+// satisfies the cell's own row of A x = b given its neighbours (the real ones
+// already corrected, the ghost ones as they were), so that the boundary rows
+// carry no residual after the correction
+__global__ void k_apply(int nx, int ny, int H, int W, const double *a5, const double *b, const float *y,
+                        const double *s, const double *x, double *xout)
 {
     const long long N = (long long)nx * ny;
+    const double sg = s[4];
+    auto corrected = [&](long long q) {
+        const int jq = (int)(q / nx) + 1, iq = (int)(q - (long long)(jq - 1) * nx) + 1;
+        double v = x[q];
+        if (iq > 1 && iq < nx && jq > 1 && jq < ny) v += sg * (double)y[(long long)(jq - 2) * W + (iq - 2)];
+        return v;
+    };
     for (long long np = (long long)blockIdx.x * blockDim.x + threadIdx.x; np < N; np += (long long)gridDim.x * blockDim.x) {
         const int j = (int)(np / nx) + 1, i = (int)(np - (long long)(j - 1) * nx) + 1;
-        double v = x[np];
-        if (i > 1 && i < nx && j > 1 && j < ny) v += s[4] * (double)y[(long long)(j - 2) * W + (i - 2)];
-        xout[np] = v;
+        if (i > 1 && i < nx && j > 1 && j < ny) { xout[np] = corrected(np); continue; }
+        const double ap = a5[2 * N + np];
+        if (ap == 0.0) { xout[np] = x[np]; continue; }
+        double v = b[np];
+        if (j > 1) v -= a5[np] * corrected(np - nx);
+        if (i > 1) v -= a5[N + np] * corrected(np - 1);
+        if (i < nx) v -= a5[3 * N + np] * corrected(np + 1);
+        if (j < ny) v -= a5[4 * N + np] * corrected(np + nx);
+        xout[np] = v / ap;
     }
 }
 
@@ -942,12 +961,13 @@ extern "C" int m2d_pprime_features(int nx, int ny, int H, int W, const double *d
     return M2D_OK;
 }
 
-extern "C" int m2d_pprime_apply(int nx, int ny, int H, int W, const float *d_y, const double *d_stats,
-                                const double *d_x, double *d_xout, void *stream)
+extern "C" int m2d_pprime_apply(int nx, int ny, int H, int W, const double *d_a, const double *d_b, const float *d_y,
+                                const double *d_stats, const double *d_x, double *d_xout, void *stream)
 {
-    if (!image_fits(nx, ny, H, W) || !d_y || !d_stats || !d_x || !d_xout)
+    if (!image_fits(nx, ny, H, W) || !d_a || !d_b || !d_y || !d_stats || !d_x || !d_xout || d_x == d_xout)
         return unet_fail(M2D_ERR_ARG, "m2d_pprime_apply: bad arguments");
-    k_apply<<<grid_for((long long)nx * ny), 256, 0, (cudaStream_t)stream>>>(nx, ny, H, W, d_y, d_stats, d_x, d_xout);
+    k_apply<<<grid_for((long long)nx * ny), 256, 0, (cudaStream_t)stream>>>(nx, ny, H, W, d_a, d_b, d_y, d_stats, d_x,
+                                                                           d_xout);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) { m2d_set_last_error(e, "m2d_pprime_apply", __FILE__, __LINE__); return M2D_ERR_CUDA; }
     return M2D_OK;
@@ -970,8 +990,9 @@ extern "C" int m2d_msi_solve_device_ws(int nd, int nx, int ny, int nitm, double 
 extern "C" long m2d_msi_workspace_doubles(int nd, int nx, int ny);
 
 // Flexible pressure-correction solve: the network's correction first, kept
-// only if it lowers |b - A x|; then the MSI iteration, whose stopping test
-// stays relative to the residual before the correction.
+// only if it lowers |b - A x|; then the MSI iteration (at least one, as in
+// plain MSI), whose stopping test stays relative to the residual before the
+// correction.
 extern "C" int m2d_pprime_solve_learned(m2d_unet *n, int nx, int ny, int nitm, double tol, const double *d_a,
                                         const double *d_b, double *d_x, const double *d_Jp, double *d_work, int prec,
                                         void *stream, m2d_learned_report *rep)
@@ -988,7 +1009,7 @@ extern "C" int m2d_pprime_solve_learned(m2d_unet *n, int nx, int ny, int nitm, d
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = forward(n, 1, n->feat, n->yout, false, st);
     if (e == cudaSuccess) {
-        k_apply<<<grid_for(N), 256, 0, st>>>(nx, ny, H, W, n->yout, s, d_x, n->x1);
+        k_apply<<<grid_for(N), 256, 0, st>>>(nx, ny, H, W, d_a, d_b, n->yout, s, d_x, n->x1);
         k_residual5<<<grid_for(N), 256, 0, st>>>(nx, ny, d_a, d_b, n->x1, n->r);
         k_sys_stats<<<1, kStatThreads, 0, st>>>(nx, ny, d_a, n->r, nullptr, s + 9, 0);
         e = cudaGetLastError();
@@ -1002,10 +1023,10 @@ extern "C" int m2d_pprime_solve_learned(m2d_unet *n, int nx, int ny, int nitm, d
     double tol_eff = tol;
     if (accept) {
         e = cudaMemcpyAsync(d_x, n->x1, (size_t)N * sizeof(double), cudaMemcpyDeviceToDevice, st);
-        tol_eff = r1 > 0.0 ? tol * r0 / r1 : 2.0;
+        tol_eff = r1 > 0.0 ? tol * r0 / r1 : 1.0;
     }
     int nit = 0;
-    if (e == cudaSuccess && tol_eff < 1.0) {
+    if (e == cudaSuccess) {      // at least one MSI iteration, as the judge of the correction
         const int rc = m2d_msi_solve_device_ws(5, nx, ny, nitm, tol_eff, d_a, d_b, d_x, d_work,
                                                m2d_msi_workspace_doubles(5, nx, ny), stream, n->nit, nullptr, prec);
         if (rc) return rc;
@@ -1053,7 +1074,7 @@ extern "C" int m2d_pprime_solve_cycles(m2d_unet *n, int nx, int ny, int m, int m
         e = cudaGetLastError();
         if (e == cudaSuccess) e = forward(n, 1, n->feat, n->yout, false, st);
         if (e != cudaSuccess) return fail_cuda(e);
-        k_apply<<<grid_for(N), 256, 0, st>>>(nx, ny, H, W, n->yout, s, d_x, n->x1);
+        k_apply<<<grid_for(N), 256, 0, st>>>(nx, ny, H, W, d_a, d_b, n->yout, s, d_x, n->x1);
         k_residual5<<<grid_for(N), 256, 0, st>>>(nx, ny, d_a, d_b, n->x1, n->r);
         k_sys_stats<<<1, kStatThreads, 0, st>>>(nx, ny, d_a, n->r, nullptr, s + 9, 0);
         e = cudaMemcpyAsync(&h, s + 9, sizeof h, cudaMemcpyDeviceToHost, st);
@@ -1065,7 +1086,6 @@ extern "C" int m2d_pprime_solve_cycles(m2d_unet *n, int nx, int ny, int m, int m
             if (e != cudaSuccess) return fail_cuda(e);
             rcur = r1;
             accepted++;
-            if (rcur <= goal) break;
         }
         const int rc = m2d_msi_solve_device_ws(5, nx, ny, m, goal / rcur, d_a, d_b, d_x, d_work, wd, stream, n->nit,
                                                nullptr, prec);

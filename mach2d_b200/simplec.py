@@ -119,6 +119,13 @@ class Simplec:
         check(L.m2d_run(self._ctx, int(itmax), ctypes.byref(rep)))
         return rep
 
+    def set_unet(self, net):
+        """Attaches the network solver 3 uses for its p' corrections (None detaches)."""
+        L = lib()
+        L.m2d_ctx_set_unet.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        check(L.m2d_ctx_set_unet(self._ctx, None if net is None else net._h))
+        self._net = net
+
     def field(self, name):
         n = self._size(name)
         out = np.empty(n, dtype=np.float64)

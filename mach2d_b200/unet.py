@@ -39,7 +39,7 @@ def _bind():
     L.m2d_unet_adam.argtypes = [_vp, _f, _f, _f, _f, _vp]
     L.m2d_residual5.argtypes = [_int, _int, _vp, _vp, _vp, _vp, _vp, _vp]
     L.m2d_pprime_features.argtypes = [_int] * 4 + [_vp] * 5 + [_vp]
-    L.m2d_pprime_apply.argtypes = [_int] * 4 + [_vp] * 4 + [_vp]
+    L.m2d_pprime_apply.argtypes = [_int] * 4 + [_vp] * 6 + [_vp]
     L.m2d_pprime_target.argtypes = [_int] * 4 + [_vp] * 4 + [_vp]
     L.m2d_pprime_solve_learned.argtypes = [_vp, _int, _int, _int, _d] + [_vp] * 5 + [_int, _vp,
                                                                                         ctypes.POINTER(LearnedReport)]
@@ -150,8 +150,8 @@ def features(nx, ny, H, W, a, r, Jp, feat, stats, stream=None):
     check(_bind().m2d_pprime_features(nx, ny, H, W, _ptr(a), _ptr(r), _ptr(Jp), _ptr(feat), _ptr(stats), stream))
 
 
-def apply(nx, ny, H, W, y, stats, x, xout, stream=None):
-    check(_bind().m2d_pprime_apply(nx, ny, H, W, _ptr(y), _ptr(stats), _ptr(x), _ptr(xout), stream))
+def apply(nx, ny, H, W, a, b, y, stats, x, xout, stream=None):
+    check(_bind().m2d_pprime_apply(nx, ny, H, W, _ptr(a), _ptr(b), _ptr(y), _ptr(stats), _ptr(x), _ptr(xout), stream))
 
 
 def target(nx, ny, H, W, delta, stats, t, mask, stream=None):

@@ -188,7 +188,6 @@ def init_params(seed):
 # ------------------------------------------------------------ p' adapters
 def features(nx, ny, H, W, a5, r, Jp):
     """11 planes [11, H, W] and (sigma, mean log Jp, std log Jp)."""
-    N = nx * ny
     A = a5.reshape(5, ny, nx)[:, 1:-1, 1:-1]
     rr = r.reshape(ny, nx)[1:-1, 1:-1]
     lj = np.log(Jp.reshape(ny, nx)[1:-1, 1:-1])
@@ -208,15 +207,46 @@ def features(nx, ny, H, W, a5, r, Jp):
     f[6, :h, :w] = A[3] / ap
     f[8, :h, :w] = A[4] / ap
     f[10, :h, :w] = (lj - mean) / std
-    del N
     return f, (sig, mean, std)
 
 
 def residual5(nx, ny, a5, b, x):
+    """b - A x on every cell; neighbours outside the grid contribute nothing."""
     A = a5.reshape(5, ny, nx)
     X = x.reshape(ny, nx)
-    r = np.zeros((ny, nx))
-    r[1:-1, 1:-1] = b.reshape(ny, nx)[1:-1, 1:-1] - (
-        A[0, 1:-1, 1:-1] * X[:-2, 1:-1] + A[1, 1:-1, 1:-1] * X[1:-1, :-2] + A[2, 1:-1, 1:-1] * X[1:-1, 1:-1] +
-        A[3, 1:-1, 1:-1] * X[1:-1, 2:] + A[4, 1:-1, 1:-1] * X[2:, 1:-1])
-    return r.reshape(-1)
+    ax = A[2] * X
+    ax[1:, :] += A[0, 1:, :] * X[:-1, :]
+    ax[:, 1:] += A[1, :, 1:] * X[:, :-1]
+    ax[:, :-1] += A[3, :, :-1] * X[:, 1:]
+    ax[:-1, :] += A[4, :-1, :] * X[1:, :]
+    return (b.reshape(ny, nx) - ax).reshape(-1)
+
+
+def apply(nx, ny, H, W, a5, b, y, sigma, x):
+    """x + sigma y on the real cells; each ghost cell solves its own row with
+    the corrected real neighbours and the old ghost values."""
+    X = x.reshape(ny, nx)
+    C = X.copy()
+    C[1:-1, 1:-1] += sigma * y[:ny - 2, :nx - 2]
+    A = a5.reshape(5, ny, nx)
+    B = b.reshape(ny, nx)
+    out = C.copy()
+    for j in range(ny):
+        for i in range(nx):
+            if 0 < i < nx - 1 and 0 < j < ny - 1:
+                continue
+            ap = A[2, j, i]
+            if ap == 0.0:
+                out[j, i] = X[j, i]
+                continue
+            v = B[j, i]
+            if j > 0:
+                v -= A[0, j, i] * C[j - 1, i]
+            if i > 0:
+                v -= A[1, j, i] * C[j, i - 1]
+            if i < nx - 1:
+                v -= A[3, j, i] * C[j, i + 1]
+            if j < ny - 1:
+                v -= A[4, j, i] * C[j + 1, i]
+            out[j, i] = v / ap
+    return out.reshape(-1)

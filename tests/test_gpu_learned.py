@@ -1,0 +1,127 @@
+"""The learned p' correction inside the SIMPLEC iteration (solver 3) and what a
+trained network gains over plain MSI.
+
+The network is trained here, on the GPU, by the library's own kernels, on
+p' systems harvested from the solver (Euler cosine nozzles of the batched
+sweep's distribution at 64 x 32), each paired with its converged MSI
+solution.  On held-out systems the trained correction alone must remove at
+least half of the residual (a network that has learned nothing removes
+none, and its corrections are rejected); MSI then needs no more iterations
+than without it.  Inside the SIMPLEC iteration (solver 3) the outer
+iteration follows solver 2's to within the p' tolerance.  Solver 3 with a
+network whose corrections are all rejected reproduces solver 2 bitwise,
+since plain MSI is then the whole solve.
+"""
+import numpy as np
+import pytest
+
+from mach2d_b200 import unet
+from mach2d_b200.simplec import Simplec, euler_cosine_case
+
+pytestmark = pytest.mark.gpu
+NXR, NYR = 64, 32
+
+
+def _case(seed, **over):
+    r = np.random.default_rng(seed)
+    return euler_cosine_case(NXR, NYR, Rin=r.uniform(1.5, 2.5), Rout=r.uniform(1.3, 2.2), Lc=r.uniform(1, 3),
+                             Ld=r.uniform(2, 6), p0=r.uniform(5e5, 3e6), T0=r.uniform(600, 1500), **over)
+
+
+@pytest.fixture(scope="module")
+def trained():
+    H, W = unet.image_shape(NXR + 2, NYR + 2)
+    pairs = unet.PairSet(240, H, W)
+    for s in range(8):
+        sim = Simplec(_case(s))
+        for _ in range(3):
+            sim.iterate()
+        unet.harvest(sim, pairs, iters_between=4, count=30)
+        sim.close()
+    held = []
+    hp = unet.PairSet(12, H, W)
+    sim = Simplec(_case(50))
+    for _ in range(5):
+        sim.iterate()
+    unet.harvest(sim, hp, iters_between=6, count=12, held_out=held)
+    Jp = sim.field("Jp")
+    sim.close()
+    net = unet.UNet(16, H, W, seed=1)
+    hist = unet.train(net, pairs, 1000, batch=16, lr=2e-3, lr_final=1e-4)
+    return net, held, Jp, hist
+
+
+def test_training_reduces_the_loss(trained):
+    _, _, _, hist = trained
+    assert np.mean(hist[-50:]) < 0.05 * hist[0]
+
+
+def test_trained_correction_removes_most_of_the_residual(trained):
+    import torch
+    net, held, Jp, _ = trained
+    dev = torch.device("cuda:0")
+    nx, ny = NXR + 2, NYR + 2
+    L = unet._bind()
+    work = torch.empty(L.m2d_msi_workspace_doubles(5, nx, ny), dtype=torch.float64, device=dev)
+    nit = torch.zeros(2, dtype=torch.int32, device=dev)
+    dJ = torch.from_numpy(Jp).to(dev)
+    ratios, n_plain, n_learned = [], [], []
+    for a, b in held:
+        x = torch.zeros(nx * ny, dtype=torch.float64, device=dev)
+        unet.msi5(nx, ny, 1000, 1e-8, a, b, x, work, nit)
+        n_plain.append(int(nit[0].item()))
+        x = torch.zeros(nx * ny, dtype=torch.float64, device=dev)
+        rep = net.solve(nx, ny, 1000, 1e-8, a, b, x, dJ, work)
+        ratios.append(rep.r1 / rep.r0)
+        n_learned.append(rep.nit)
+        # the flexible solve meets the same tolerance as plain MSI
+        r = torch.zeros_like(x)
+        rr = torch.zeros(1, dtype=torch.float64, device=dev)
+        unet.residual5(nx, ny, a, b, x, r, rr)
+        assert np.sqrt(rr.item()) <= 1e-8 * rep.r0 * (1 + 1e-9)
+    assert np.median(ratios) < 0.5
+    assert sum(n_learned) <= sum(n_plain)
+
+
+def test_solver3_with_rejected_corrections_equals_solver2():
+    c2, c3 = _case(60, solver=2), _case(60, solver=3)
+    g2, g3 = Simplec(c2), Simplec(c3)
+    H, W = unet.image_shape(g3.nx, g3.ny)
+    net = unet.UNet(1, H, W, seed=2)
+    p = net.params()
+    p[-17:-1] = 0.0
+    p[-1] = 1e6                        # a huge constant correction: raises |r|, always rejected
+    net.set_params(p)
+    g3.set_unet(net)
+    for _ in range(15):
+        r2, r3 = g2.iterate(), g3.iterate()
+        assert (r2.norm, r2.normpl, r2.dt, r2.itp_used) == (r3.norm, r3.normpl, r3.dt, r3.itp_used)
+    for f in ("u", "v", "p", "T", "pl"):
+        assert np.array_equal(g2.field(f), g3.field(f)), f
+    assert g3.scalar("learned_calls") > 0 and g3.scalar("learned_accepted") == 0
+    g2.close(), g3.close(), net.close()
+
+
+def test_solver3_with_trained_network_runs_and_keeps_corrections(trained):
+    net, _, _, _ = trained
+    g2, g3 = Simplec(_case(61, solver=2)), Simplec(_case(61, solver=3))
+    small = unet.UNet(1, net.H, net.W, params=net.params())
+    g3.set_unet(small)
+    for _ in range(40):
+        r2, r3 = g2.iterate(), g3.iterate()
+        # the outer iteration follows solver 2's to within the p' tolerance
+        assert r3.itp_used == r2.itp_used and abs(r3.normpl / r2.normpl - 1) < 1e-2
+    for f in ("u", "v", "p", "T"):
+        a, b = g2.field(f), g3.field(f)
+        assert np.max(np.abs(a - b)) <= 1e-3 * np.max(np.abs(a)), f
+    assert g3.scalar("learned_accepted") > 0
+    g2.close(), g3.close(), small.close()
+
+
+def test_solver3_without_network_fails_loudly():
+    from mach2d_b200 import M2DError
+    g = Simplec(_case(62, solver=3))
+    with pytest.raises(M2DError) as e:
+        g.iterate()
+    assert e.value.code == 2
+    g.close()
