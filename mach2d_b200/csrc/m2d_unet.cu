@@ -88,6 +88,7 @@ struct ConvArgs {
     int accumulate;                // yf += result
     int act;                       // 1: y = gelu(result)
     int nimg, H, W, cin, cout;
+    int *err;                      // device error word (ERR_WAIT_TIMEOUT), may be null
 };
 
 template <int NT>
@@ -171,6 +172,202 @@ __global__ void __launch_bounds__(128) k_conv3x3(ConvArgs a)
             }
 }
 
+// ---- the same convolution on the 5th-generation tensor cores (tcgen05)
+// One CTA computes two 128-pixel row segments (image rows gy0, gy0 + 1, the
+// same columns) for all output channels: for row r, D_r[128 x N] (FP32, in
+// tensor memory columns [rN, rN + N)) = sum over 16-channel chunks and the 9
+// taps of A_{r,tap}[128 x 16] * B_tap[N x 16]^T, each one tcgen05.mma of
+// M = 128, N = cout, K = 16 issued by one thread; the two rows share the
+// staged weights.  Operands sit in shared memory in the K-major layout
+// without swizzle: 8-row core matrices of 16-byte rows, the two 8-channel
+// halves of K `lbo` bytes apart, consecutive groups of 8 rows 128 bytes
+// apart.  A chunk's halo is stored [K half][4 rows][130 pixels][8 channels],
+// so the A operand of (row r, tap (dy, dx)) is that layout started
+// (130 (r + dy) + dx) pixels in; the weights are stored
+// [tap][K half][n][8 channels].  Two stages filled with cp.async: the
+// threads fill one while the tensor cores read the other, and a
+// tcgen05.commit on the stage's mbarrier frees it.  The epilogue reads the
+// accumulators with tcgen05.ld (warp w owns tensor-memory lanes
+// 32w..32w+31, i.e. pixels 32w..32w+31 of each segment).  Used when W is a
+// multiple of 128 and H is even.
+constexpr int kTcPix = 128, kTcHaloW = kTcPix + 2, kTcRows = 2, kTcHaloRows = kTcRows + 2;
+constexpr int kTcHaloBytes = 2 * kTcHaloRows * kTcHaloW * 16;
+constexpr int kTcMaxN = 256;
+constexpr int kTcStageMax = kTcHaloBytes + 9 * 2 * kTcMaxN * 16;
+constexpr unsigned kTcWaitCap = 1u << 24;
+
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
+{
+    // start, leading and stride byte offsets in 16-byte units; version 1; no swizzle
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+__device__ __forceinline__ uint32_t umma_idesc_bf16_f32(int M, int N)
+{
+    // D F32 (bits 4-5 = 1), A and B BF16 (bits 7-9, 10-12 = 1), both K-major,
+    // N >> 3 at bit 17, M >> 4 at bit 24
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+__device__ __forceinline__ void tc_mbar_init(unsigned long long *b)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(b)) : "memory");
+}
+// bounded wait for the completion of phase `parity`; false when the cap ran out
+__device__ __forceinline__ bool tc_mbar_wait(unsigned long long *b, uint32_t parity)
+{
+    const uint32_t addr = smem_u32(b);
+    for (unsigned it = 0; it < kTcWaitCap; it++) {
+        uint32_t done;
+        asm volatile("{\n\t.reg .pred p;\n\t"
+                     "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}"
+                     : "=r"(done) : "r"(addr), "r"(parity) : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+// 16-byte asynchronous copy global -> shared; zero-filled when !valid
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, bool valid)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(valid ? 16 : 0) : "memory");
+}
+
+__global__ void __launch_bounds__(128, 1) k_conv3x3_tc(ConvArgs a)
+{
+    extern __shared__ __align__(1024) unsigned char tc_smem[];
+    __shared__ __align__(8) unsigned long long bar[2];
+    __shared__ uint32_t tmem_slot;
+    __shared__ int s_timeout;
+    const int N = a.cout;
+    const int stage_bytes = kTcHaloBytes + 9 * 2 * N * 16;
+    const int segs = a.W / kTcPix;
+    const int gy0 = (blockIdx.x / segs) * kTcRows, gx0 = (blockIdx.x % segs) * kTcPix;
+    const int img = blockIdx.z;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int cols = kTcRows * N;
+    const uint32_t ncols = cols <= 32 ? 32u : (cols <= 64 ? 64u : (cols <= 128 ? 128u : (cols <= 256 ? 256u : 512u)));
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(&tmem_slot)), "r"(ncols) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (threadIdx.x == 0) {
+        tc_mbar_init(&bar[0]);
+        tc_mbar_init(&bar[1]);
+        s_timeout = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_slot;
+    const uint32_t idesc = umma_idesc_bf16_f32(kTcPix, N);
+    const uint32_t base = smem_u32(tc_smem);
+    const int nchunks = a.cin / 16;
+    auto fill = [&](int c, int stg) {
+        const uint32_t sb = base + (uint32_t)(stg * stage_bytes);
+        for (int q = threadIdx.x; q < 2 * kTcHaloRows * kTcHaloW; q += 128) {
+            const int h = q / (kTcHaloRows * kTcHaloW), r = q - h * (kTcHaloRows * kTcHaloW);
+            const int hy = r / kTcHaloW, hx = r - hy * kTcHaloW;
+            const int yy = gy0 + hy - 1, xx = gx0 + hx - 1;
+            const bool in = yy >= 0 && yy < a.H && xx >= 0 && xx < a.W;
+            const bf16 *src = in ? a.x + ((long long)(img * a.H + yy) * a.W + xx) * a.ldx + c * 16 + h * 8 : a.x;
+            cp_async16(sb + (uint32_t)q * 16u, src, in);
+        }
+        const uint32_t wb = sb + kTcHaloBytes;
+        for (int q = threadIdx.x; q < 18 * N; q += 128) {
+            const int tap = q / (2 * N), r = q - tap * 2 * N, h = r / N, n = r - h * N;
+            cp_async16(wb + (uint32_t)q * 16u, a.w + ((long long)n * 9 + tap) * a.cin + c * 16 + h * 8, true);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    uint32_t phase[2] = {0u, 0u};
+    bool ok = true;
+    fill(0, 0);
+    for (int c = 0; c < nchunks; c++) {
+        const int st = c & 1;
+        if (c + 1 < nchunks) {
+            if (c >= 1) {     // the MMAs of chunk c - 1 read the stage chunk c + 1 goes to
+                ok = tc_mbar_wait(&bar[st ^ 1], phase[st ^ 1]) && ok;
+                phase[st ^ 1] ^= 1u;
+            }
+            fill(c + 1, st ^ 1);
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+        } else {
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (threadIdx.x == 0 && ok) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t sa = base + (uint32_t)(st * stage_bytes), sw = sa + kTcHaloBytes;
+#pragma unroll 1
+            for (int tap = 0; tap < 9; tap++) {
+                const int dy = tap / 3, dx = tap - dy * 3;
+                const uint64_t bd = umma_desc(sw + (uint32_t)tap * 2u * (uint32_t)N * 16u, (uint32_t)N * 16u, 128u);
+                const uint32_t acc = (c > 0 || tap > 0) ? 1u : 0u;
+#pragma unroll
+                for (int r = 0; r < kTcRows; r++) {
+                    const uint64_t ad = umma_desc(sa + (uint32_t)((r + dy) * kTcHaloW + dx) * 16u,
+                                                  (uint32_t)(kTcHaloRows * kTcHaloW * 16), 128u);
+                    asm volatile("{\n\t.reg .pred p;\n\t"
+                                 "setp.ne.b32 p, %4, 0;\n\t"
+                                 "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                                 ::"r"(tmem + (uint32_t)(r * N)), "l"(ad), "l"(bd), "r"(idesc), "r"(acc) : "memory");
+                }
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                         ::"r"(smem_u32(&bar[st])) : "memory");
+        }
+    }
+    // the last commit covers every MMA of the CTA
+    const int sl = (nchunks - 1) & 1;
+    ok = tc_mbar_wait(&bar[sl], phase[sl]) && ok;
+    if (!ok) {
+        s_timeout = 1;
+        if (a.err) atomicOr(a.err, m2d::ERR_WAIT_TIMEOUT);
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (!s_timeout) {
+        const int pl = warp * 32 + lane;
+        const uint32_t tlane = tmem + ((uint32_t)(warp * 32) << 16);
+        for (int r = 0; r < kTcRows; r++) {
+            const long long p = (long long)(img * a.H + gy0 + r) * a.W + gx0 + pl;
+            for (int cc = 0; cc < N; cc += 16) {
+                uint32_t v[16];
+                asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+                             "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                             : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                               "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                               "=r"(v[14]), "=r"(v[15])
+                             : "r"(tlane + (uint32_t)(r * N + cc)));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+                for (int k = 0; k < 16; k += 2) {
+                    const int co = cc + k;
+                    float v0 = __uint_as_float(v[k]), v1 = __uint_as_float(v[k + 1]);
+                    if (a.bias) { v0 += a.bias[co]; v1 += a.bias[co + 1]; }
+                    if (a.z) *reinterpret_cast<float2 *>(a.z + p * a.cout + co) = make_float2(v0, v1);
+                    if (a.yf) {
+                        float2 *d = reinterpret_cast<float2 *>(a.yf + p * a.ldyf + co);
+                        if (a.accumulate) { const float2 o = *d; v0 += o.x; v1 += o.y; }
+                        *d = make_float2(v0, v1);
+                    }
+                    if (a.y) {
+                        if (a.act) { v0 = gelu(v0); v1 = gelu(v1); }
+                        *reinterpret_cast<__nv_bfloat162 *>(a.y + p * a.ldy + co) = __floats2bfloat162_rn(v0, v1);
+                    }
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
+}
+
 // dW[co][tap][ci] += sum over pixels of dZ[p][co] X[p + tap offset][ci]:
 // a GEMM with M = output channels (64 per CTA, 16 per warp), N = 9 taps x 16
 // input channels, K = pixels (16 per step, one tile row).  Both operands come
@@ -188,7 +385,11 @@ __global__ void __launch_bounds__(128) k_conv3x3_wgrad(WgradArgs a)
     __shared__ __align__(128) unsigned char s_halo[kHaloPix * 32];
     const int c0 = blockIdx.x * 16, co0 = blockIdx.y * 64;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int wco = warp * 16;
+    // warps along the output channels of the tile (1, 2 or 4); the rest of
+    // the warps split the tile's pixel rows (each adds its own partial sums)
+    const int rem = a.cout - co0;
+    const int nco = rem > 32 ? 4 : (rem > 16 ? 2 : 1);
+    const int wco = (warp % nco) * 16, row0 = warp / nco, rstep = 4 / nco;
     const bool active = co0 + wco < a.cout;
     float acc[18][4];
 #pragma unroll
@@ -219,7 +420,7 @@ __global__ void __launch_bounds__(128) k_conv3x3_wgrad(WgradArgs a)
         __syncthreads();
         if (active) {
 #pragma unroll 1
-            for (int yy = 0; yy < kTileH; yy++) {
+            for (int yy = row0; yy < kTileH; yy += rstep) {
                 uint32_t af[4];
                 {
                     const int mi = lane >> 3, r = lane & 7;
@@ -256,22 +457,31 @@ __global__ void __launch_bounds__(128) k_conv3x3_wgrad(WgradArgs a)
     }
 }
 
-// dZ = bf16(dA * gelu'(Z)); db[c] += sum of dZ over pixels (before rounding)
-__global__ void k_gelu_bwd(long long npix, int cout, const float *dA, int lda, const float *z, bf16 *dz, float *db)
+// dZ = bf16(dA * gelu'(Z)); db[c] += sum of dZ over pixels (before rounding).
+// 256 threads, cout divides 256: every element a thread visits has channel
+// threadIdx.x % cout, so the bias sums stay in registers until one block
+// reduction per channel
+constexpr int kEltBlock = 256;
+__global__ void __launch_bounds__(kEltBlock) k_gelu_bwd(long long npix, int cout, const float *dA, int lda,
+                                                        const float *z, bf16 *dz, float *db)
 {
-    __shared__ float s_db[128];
-    for (int c = threadIdx.x; c < cout; c += blockDim.x) s_db[c] = 0.f;
-    __syncthreads();
+    __shared__ float s_part[kEltBlock];
     const long long n = npix * cout;
-    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const int c = threadIdx.x % cout;
+    float acc = 0.f;
+    for (long long e = (long long)blockIdx.x * kEltBlock + threadIdx.x; e < n; e += (long long)gridDim.x * kEltBlock) {
         const long long p = e / cout;
-        const int c = (int)(e - p * cout);
         const float g = dA[p * lda + c] * gelu_grad(z[e]);
         dz[e] = __float2bfloat16_rn(g);
-        atomicAdd(&s_db[c], g);
+        acc += g;
     }
+    s_part[threadIdx.x] = acc;
     __syncthreads();
-    for (int c = threadIdx.x; c < cout; c += blockDim.x) atomicAdd(&db[c], s_db[c]);
+    if (threadIdx.x < cout) {
+        float t = 0.f;
+        for (int k = threadIdx.x; k < kEltBlock; k += cout) t += s_part[k];
+        atomicAdd(&db[threadIdx.x], t);
+    }
 }
 
 // 2x2 mean (outputs rounded to bf16) and its adjoint (added into dX)
@@ -305,14 +515,15 @@ __global__ void k_pool_bwd(int nimg, int H, int W, int C, const float *dy, float
 // nearest 2x upsampling into a channel slice, and its adjoint
 __global__ void k_up(int nimg, int Ho, int Wo, int C, const bf16 *x, bf16 *y, int ldy)
 {
-    const long long n = (long long)nimg * Ho * Wo * C;
+    const int C8 = C / 8;      // 16-byte groups of channels
+    const long long n = (long long)nimg * Ho * Wo * C8;
     for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
-        const long long p = e / C;
-        const int c = (int)(e - p * C);
+        const long long p = e / C8;
+        const int c = (int)(e - p * C8) * 8;
         const int img = (int)(p / ((long long)Ho * Wo));
         const int r = (int)(p - (long long)img * Ho * Wo), yy = r / Wo, xx = r - yy * Wo;
         const long long q = ((long long)img * (Ho / 2) + yy / 2) * (Wo / 2) + xx / 2;
-        y[p * ldy + c] = x[q * C + c];
+        *reinterpret_cast<uint4 *>(y + p * ldy + c) = *reinterpret_cast<const uint4 *>(x + q * C + c);
     }
 }
 __global__ void k_up_bwd(int nimg, int Hi, int Wi, int C, const float *dy, int lddy, float *dx)
@@ -371,12 +582,14 @@ __global__ void k_loss(long long npix, const float *out, const float *t, const f
     if ((threadIdx.x & 31) == 0) atomicAdd(loss, s * scale);
 }
 // head adjoint: dU[p][c] = dout[p] wh[c]; dwh[c] += sum dout U; dbh += sum dout
-__global__ void k_head_bwd(long long npix, const bf16 *u, const float *wh, const float *dout, float *du, float *dwh)
+__global__ void __launch_bounds__(kEltBlock) k_head_bwd(long long npix, const bf16 *u, const float *wh,
+                                                        const float *dout, float *du, float *dwh)
 {
+    __shared__ float s_g[kEltBlock / 32][17];
     float g[17];
 #pragma unroll
     for (int c = 0; c < 17; c++) g[c] = 0.f;
-    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += (long long)gridDim.x * blockDim.x) {
+    for (long long p = (long long)blockIdx.x * kEltBlock + threadIdx.x; p < npix; p += (long long)gridDim.x * kEltBlock) {
         const float d = dout[p];
 #pragma unroll
         for (int c = 0; c < 16; c++) {
@@ -385,11 +598,18 @@ __global__ void k_head_bwd(long long npix, const bf16 *u, const float *wh, const
         }
         g[16] += d;
     }
+    const int w = threadIdx.x >> 5;
 #pragma unroll
     for (int c = 0; c < 17; c++) {
         float v = g[c];
         for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if ((threadIdx.x & 31) == 0) atomicAdd(&dwh[c], v);
+        if ((threadIdx.x & 31) == 0) s_g[w][c] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 17) {
+        float t = 0.f;
+        for (int k = 0; k < kEltBlock / 32; k++) t += s_g[k][threadIdx.x];
+        atomicAdd(&dwh[threadIdx.x], t);
     }
 }
 
@@ -456,6 +676,7 @@ struct m2d_unet {
     float *feat = nullptr, *yout = nullptr;
     double *r = nullptr, *x1 = nullptr, *stats = nullptr;
     int *nit = nullptr;
+    int *err = nullptr;        // device error word of the tensor-core kernels
 };
 
 namespace {
@@ -475,13 +696,33 @@ T *dalloc(m2d_unet *n, long long count, cudaError_t &e)
     return (T *)p;
 }
 
+// tcgen05 kernel policy (m2d_unet_set_tensor_path): 0 never, 1 where it
+// measured at least as fast as the mma.sync kernel (96 or more input
+// channels: enough 16-channel chunks for its two-stage pipeline to overlap
+// the staging with the MMAs), 2 wherever the shape allows
+int g_tensor_tc = 1;
+
 cudaError_t launch_conv(int nimg, int H, int W, const bf16 *x, int ldx, const bf16 *w, int cin, int cout,
                         const float *bias, float *z, bf16 *y, int ldy, float *yf, int ldyf, int accumulate, int act,
-                        cudaStream_t st)
+                        int *err, cudaStream_t st)
 {
     ConvArgs a;
     a.x = x; a.ldx = ldx; a.w = w; a.bias = bias; a.z = z; a.y = y; a.ldy = ldy; a.yf = yf; a.ldyf = ldyf;
     a.accumulate = accumulate; a.act = act; a.nimg = nimg; a.H = H; a.W = W; a.cin = cin; a.cout = cout;
+    a.err = err;
+    const bool tc_shape = W % kTcPix == 0 && H % kTcRows == 0 && cout % 16 == 0 && cout <= kTcMaxN && cin % 16 == 0;
+    if (tc_shape && (g_tensor_tc == 2 || (g_tensor_tc == 1 && cin >= 96))) {
+        static bool attr = false;
+        if (!attr) {
+            cudaError_t e = cudaFuncSetAttribute(k_conv3x3_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 2 * kTcStageMax);
+            if (e != cudaSuccess) return e;
+            attr = true;
+        }
+        const int smem = 2 * (kTcHaloBytes + 9 * 2 * cout * 16);
+        k_conv3x3_tc<<<dim3((unsigned)((H / kTcRows) * (W / kTcPix)), 1, nimg), 128, smem, st>>>(a);
+        return cudaGetLastError();
+    }
     const unsigned tiles = (unsigned)(((H + kTileH - 1) / kTileH) * ((W + kTileW - 1) / kTileW));
     if (cout % 64 == 0) k_conv3x3<64><<<dim3(tiles, cout / 64, nimg), 128, 0, st>>>(a);
     else if (cout % 32 == 0) k_conv3x3<32><<<dim3(tiles, cout / 32, nimg), 128, 0, st>>>(a);
@@ -578,6 +819,7 @@ extern "C" int m2d_unet_create(int bmax, int H, int W, int device, m2d_unet **ou
     n->x1 = dalloc<double>(n, cells, e);
     n->stats = dalloc<double>(n, 16, e);
     n->nit = dalloc<int>(n, 4, e);
+    n->err = dalloc<int>(n, 1, e);
     if (e != cudaSuccess) {
         m2d_set_last_error(e, "m2d_unet_create: allocation", __FILE__, __LINE__);
         m2d_unet_destroy(n);
@@ -670,7 +912,7 @@ static cudaError_t forward(m2d_unet *n, int nimg, const float *d_in, float *d_ou
         const int lh = H >> c.level, lw = W >> c.level;
         if (e == cudaSuccess)
             e = launch_conv(nimg, lh, lw, c.x, c.ldx, c.wb, c.cin, c.cout, n->params + c.boff, train ? c.z : nullptr,
-                            c.y, c.ldy, nullptr, 0, 0, 1, st);
+                            c.y, c.ldy, nullptr, 0, 0, 1, n->err, st);
     };
     const int upch[3] = {32, 64, 128}, dch[3] = {48, 96, 192};
     for (int l = 0; l < 4; l++) {
@@ -687,7 +929,8 @@ static cudaError_t forward(m2d_unet *n, int nimg, const float *d_in, float *d_ou
         const bf16 *src = (l == 2) ? n->e3b : n->U[l + 1];
         const int lh = H >> l, lw = W >> l;
         if (e == cudaSuccess) {
-            k_up<<<grid_for((long long)nimg * lh * lw * upch[l]), 256, 0, st>>>(nimg, lh, lw, upch[l], src, n->D[l], dch[l]);
+            k_up<<<grid_for((long long)nimg * lh * lw * upch[l] / 8), 256, 0, st>>>(nimg, lh, lw, upch[l], src, n->D[l],
+                                                                                    dch[l]);
             e = cudaGetLastError();
         }
         conv(8 + 2 * (2 - l));
@@ -724,7 +967,7 @@ extern "C" int m2d_unet_loss_grad(m2d_unet *n, int nimg, const float *d_in, cons
     if (e == cudaSuccess) e = cudaMemsetAsync(n->loss, 0, sizeof(float), st);
     if (e == cudaSuccess) {
         k_loss<<<grid_for(P0), 256, 0, st>>>(P0, n->out, d_target, d_mask, loss_scale, n->dout, n->loss);
-        k_head_bwd<<<grid_for(P0), 256, 0, st>>>(P0, n->U[0], n->params + (n->nparam - 17), n->dout, n->dU0,
+        k_head_bwd<<<grid_for(P0), kEltBlock, 0, st>>>(P0, n->U[0], n->params + (n->nparam - 17), n->dout, n->dU0,
                                                  n->grads + (n->nparam - 17));
         e = cudaGetLastError();
     }
@@ -735,12 +978,12 @@ extern "C" int m2d_unet_loss_grad(m2d_unet *n, int nimg, const float *d_in, cons
         const int lh = H >> c.level, lw = W >> c.level;
         const long long np = (long long)nimg * lh * lw;
         if (e != cudaSuccess) return;
-        k_gelu_bwd<<<grid_for(np * c.cout), 256, 0, st>>>(np, c.cout, c.dy, c.lddy, c.z, n->dz, n->grads + c.boff);
+        k_gelu_bwd<<<grid_for(np * c.cout), kEltBlock, 0, st>>>(np, c.cout, c.dy, c.lddy, c.z, n->dz, n->grads + c.boff);
         e = cudaGetLastError();
         if (e == cudaSuccess) e = launch_wgrad(nimg, lh, lw, c.x, c.ldx, n->dz, n->grads + c.woff, c.cin, c.cout, st);
         if (e == cudaSuccess && c.dx)
             e = launch_conv(nimg, lh, lw, n->dz, c.cout, c.wt, c.cout, c.cin, nullptr, nullptr, nullptr, 0, c.dx,
-                            c.lddx, 0, 0, st);
+                            c.lddx, 0, 0, n->err, st);
     };
     for (int l = 0; l < 3; l++) {          // decoder, finest level first
         back(13 - 2 * l);
@@ -1106,4 +1349,21 @@ extern "C" int m2d_pprime_solve_cycles(m2d_unet *n, int nx, int ny, int m, int m
     }
     if (rep) { rep->accepted = accepted; rep->r0 = r0; rep->r1 = rcur; rep->nit = nit_total; }
     return M2D_OK;
+}
+
+extern "C" int m2d_unet_set_tensor_path(int mode)
+{
+    if (mode < 0 || mode > 2) return unet_fail(M2D_ERR_ARG, "m2d_unet_set_tensor_path: mode 0, 1 or 2");
+    g_tensor_tc = mode;
+    return M2D_OK;
+}
+
+extern "C" int m2d_unet_status(m2d_unet *n, int *flags)
+{
+    if (!n || !flags) return unet_fail(M2D_ERR_ARG, "m2d_unet_status: null argument");
+    cudaSetDevice(n->device);
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(flags, n->err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) { m2d_set_last_error(e, "m2d_unet_status", __FILE__, __LINE__); return M2D_ERR_CUDA; }
+    return *flags ? M2D_ERR_TIMEOUT : M2D_OK;
 }

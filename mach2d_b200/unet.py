@@ -45,11 +45,20 @@ def _bind():
                                                                                         ctypes.POINTER(LearnedReport)]
     L.m2d_pprime_solve_cycles.argtypes = [_vp, _int, _int, _int, _int, _d] + [_vp] * 5 + [_int, _vp,
                                                                                      ctypes.POINTER(LearnedReport)]
+    L.m2d_unet_set_tensor_path.argtypes = [_int]
+    L.m2d_unet_status.argtypes = [_vp, ctypes.POINTER(_int)]
     L.m2d_msi_workspace_doubles.restype = ctypes.c_long
     L.m2d_msi_workspace_doubles.argtypes = [_int] * 3
     L.m2d_msi_solve_device_ws.argtypes = [_int] * 4 + [_d] + [_vp] * 4 + [ctypes.c_long, _vp, _vp, _vp, _int]
     L._unet_bound = True
     return L
+
+
+def set_tensor_path(mode):
+    """Which convolutions run on the tcgen05 kernel: 0 none (mma.sync), 1 those
+    with 96 or more input channels (the default), 2 every one whose image
+    shape allows it (even height, width a multiple of 128)."""
+    check(_bind().m2d_unet_set_tensor_path(int(mode)))
 
 
 def param_count():
@@ -98,6 +107,12 @@ class UNet:
             self.close()
         except Exception:
             pass
+
+    def status(self):
+        """Synchronises and returns the device error word (0: no wait ran out)."""
+        flags = _int()
+        lib().m2d_unet_status(self._h, ctypes.byref(flags))
+        return flags.value
 
     def set_params(self, p):
         p = np.ascontiguousarray(p, dtype=np.float32)

@@ -56,6 +56,39 @@ def test_forward_matches_oracle(n, H, W):
     net.close()
 
 
+def test_tcgen05_and_mma_sync_paths_agree():
+    """With every convolution that fits on the tcgen05 kernel (images 256 and
+    128 wide here) against none: the mma.sync kernel accumulates the same
+    16-channel, per-tap products in the same order, so the forward outputs
+    agree bitwise, and the gradients up to the atomics' order."""
+    torch, dev = _torch()
+    n, H, W = 2, 16, 256
+    p = _params(11)
+    rng = np.random.default_rng(12)
+    feat = torch.from_numpy(rng.standard_normal((n, 11, H, W)).astype(np.float32)).to(dev)
+    t = torch.from_numpy(rng.standard_normal((n, H, W)).astype(np.float32)).to(dev)
+    m = torch.ones(n, H, W, dtype=torch.float32, device=dev)
+    net = unet.UNet(n, H, W, params=p)
+    outs, grads, losses = [], [], []
+    try:
+        for mode in (2, 0):
+            unet.set_tensor_path(mode)
+            o = torch.zeros(n, H, W, dtype=torch.float32, device=dev)
+            net.forward(feat, o)
+            outs.append(o.cpu().numpy())
+            losses.append(net.loss_grad(feat, t, m))
+            grads.append(net.grads())
+            assert net.status() == 0
+    finally:
+        unet.set_tensor_path(1)
+    assert np.array_equal(outs[0], outs[1])
+    assert abs(losses[0] / losses[1] - 1) < 1e-6      # the loss is summed with atomics
+    assert _rel(grads[0], grads[1]) < 1e-5          # weight gradients use FP32 atomics
+    ref, _ = U.forward(p.astype(np.float64), feat.cpu().numpy().astype(np.float64))
+    assert _rel(outs[0], ref) < 2e-2
+    net.close()
+
+
 def test_gradients_match_oracle():
     torch, dev = _torch()
     n, H, W = 2, 16, 32
