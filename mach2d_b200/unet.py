@@ -254,3 +254,58 @@ def train(net, pairs, steps, batch=None, lr=1e-3, seed=0, lr_final=None, log=Non
         if log and (s % log == 0 or s == steps - 1):
             print(f"step {s} loss {hist[-1]:.4e}")
     return hist
+
+
+def _flops_per_image(H, W):
+    lv = (0, 0, 1, 1, 2, 2, 3, 3, 2, 2, 1, 1, 0, 0)
+    return sum(2 * (H >> l) * (W >> l) * ci * co * 9 for (ci, co), l in zip(LAYERS, lv))
+
+
+def main(argv=None):
+    """Times the network's kernels on random inputs:
+    python -m mach2d_b200.unet {forward,train} --batch B --height H --width W --path MODE --reps K"""
+    import argparse
+
+    import torch
+    ap = argparse.ArgumentParser(prog="python -m mach2d_b200.unet")
+    ap.add_argument("what", choices=["forward", "train"])
+    ap.add_argument("--batch", type=int, default=8)
+    ap.add_argument("--height", type=int, default=256)
+    ap.add_argument("--width", type=int, default=512)
+    ap.add_argument("--path", type=int, default=1, help="tensor-path mode (set_tensor_path)")
+    ap.add_argument("--reps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    a = ap.parse_args(argv)
+    dev = torch.device("cuda:0")
+    set_tensor_path(a.path)
+    net = UNet(a.batch, a.height, a.width, seed=1)
+    g = torch.Generator(device=dev).manual_seed(1)
+    feat = torch.randn(a.batch, 11, a.height, a.width, device=dev, generator=g)
+    out = torch.zeros(a.batch, a.height, a.width, device=dev)
+    t = torch.randn(a.batch, a.height, a.width, device=dev, generator=g)
+    m = torch.ones(a.batch, a.height, a.width, device=dev)
+
+    def step():
+        if a.what == "forward":
+            net.forward(feat, out)
+        else:
+            net.loss_grad(feat, t, m, stream=None)
+            net.adam(1e-4)
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.reps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / max(1, a.reps)
+    fl = a.batch * _flops_per_image(a.height, a.width) * (1 if a.what == "forward" else 3)
+    print(f"{a.what} {a.batch}x{a.height}x{a.width} path {a.path}: {ms:.3f} ms, {fl / ms / 1e9:.1f} TFLOP/s, "
+          f"status {net.status()}")
+    net.close()
+
+
+if __name__ == "__main__":
+    main()
