@@ -392,6 +392,13 @@ int m2d_ctx_stream(const m2d_ctx *ctx, void **stream);
  * solves and the corrections kept. */
 struct m2d_unet;
 int m2d_ctx_set_unet(m2d_ctx *ctx, struct m2d_unet *net);
+/* 1: run each outer iteration as one captured CUDA graph (built on the next
+ * m2d_iterate): the p' loop is a conditional WHILE node whose exit
+ * (normpl < tolm or itpmax cycles) and the next time step are computed on
+ * the device, so an iteration costs one graph launch and one read-back
+ * instead of about 60 launches and a host synchronisation per p' cycle.
+ * Results are bitwise those of the default mode (0).  Not with solver 3. */
+int m2d_ctx_set_graph(m2d_ctx *ctx, int on);
 int m2d_ctx_field_device(m2d_ctx *ctx, const char *name, double **dptr, long *n);
 
 /* ---- batches of instances (no counterpart in the reference) ------------

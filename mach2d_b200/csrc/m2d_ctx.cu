@@ -18,9 +18,17 @@ using namespace m2d;
 namespace {
 enum Slot {
     S_PSUM = 0, S_MAXPL, S_NU_A, S_NU_B, S_NV_A, S_NV_B, S_NP, S_NT_A, S_NT_B, S_RMASS,
-    S_CC_U, S_CC_V, S_CC_T, S_CC_P, S_FMI, S_FME, S_FD, S_RR = 20, S_COUNT = 40
+    S_CC_U, S_CC_V, S_CC_T, S_CC_P, S_FMI, S_FME, S_FD, S_RR = 20,
+    // device-resident control of a captured iteration
+    S_DT = 30, S_PAVG, S_NORMPL, S_NORM, S_IT, S_COUNT = 40
 };
-enum ISlot { I_NIT_U = 0, I_NIT_V, I_NIT_P, I_NIT_T, I_ERR, I_COUNT = 8 };
+enum ISlot { I_NIT_U = 0, I_NIT_V, I_NIT_P, I_NIT_T, I_ERR, I_ITP, I_ITP_TOTAL, I_COUNT = 8 };
+
+// what the end of an iteration needs to pick the next time step
+struct StepCtl {
+    int dtmodel, nan_policy, it1, it2, energy_eq, itpmax;
+    double dt1, dt2, h0, mincc, maxcc, tolm;
+};
 }
 
 struct m2d_ctx {
@@ -38,6 +46,14 @@ struct m2d_ctx {
     m2d_mixture *dmix = nullptr;   // device copy of c.mix (ktm = 1)
     m2d_unet *net = nullptr;       // learned p' correction (solver 3), not owned
     long long learned_calls = 0, learned_accepted = 0;
+    // captured iteration (m2d_ctx_set_graph): the whole `it` body as one CUDA
+    // graph, the p' loop a conditional WHILE node, dt and the loop exit on the
+    // device
+    bool graph_on = false;
+    cudaStream_t st2 = nullptr;    // captures the p' loop body
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    long long launches_fixed = 0, launches_body = 0;
     double *hsc = nullptr;   // pinned mirror of dsc
     int *hint = nullptr;     // pinned mirror of dint
     double dt = 0, norm = 0, normpl = 0, rmass = 0, p_avg = 0;
@@ -201,6 +217,9 @@ extern "C" int m2d_destroy(m2d_ctx *x)
 {
     if (!x) return M2D_OK;
     if (x->st) cudaStreamSynchronize(x->st);
+    if (x->exec) cudaGraphExecDestroy(x->exec);
+    if (x->graph) cudaGraphDestroy(x->graph);
+    if (x->st2) cudaStreamDestroy(x->st2);
     if (x->arena) cudaFree(x->arena);
     if (x->hsc) cudaFreeHost(x->hsc);
     if (x->hint) cudaFreeHost(x->hint);
@@ -225,8 +244,8 @@ static RedArgs red(const m2d_ctx *x, int kind)
     return r;
 }
 
-// linear solves of the iteration: solver9d%solve / solver5d%solve
-static int solve9(m2d_ctx *x, int nsys, double *const *a, double *const *b, double *const *v,
+// linear solves of the iteration: solver9d%solve / solver5d%solve, on stream s
+static int solve9(m2d_ctx *x, cudaStream_t s, int nsys, double *const *a, double *const *b, double *const *v,
                   const int *islot, const int *rslot)
 {
     const m2d_case &c = x->c;
@@ -241,15 +260,15 @@ static int solve9(m2d_ctx *x, int nsys, double *const *a, double *const *b, doub
             L.s[k].ws = x->ws9[k];
             L.s[k].nit = x->dint + islot[k]; L.s[k].rr = x->dsc + rslot[k];
         }
-        KL(launch_msi(9, L, nsys, x->st), 2);   // A transpose + solve
+        KL(launch_msi(9, L, nsys, s), 2);   // A transpose + solve
     } else {
         for (int k = 0; k < nsys; k++)
-            KL(launch_tdma(9, x->nx, x->ny, c.nitm_u, a[k], b[k], v[k], x->P, x->Q, x->st), 4 * c.nitm_u);
+            KL(launch_tdma(9, x->nx, x->ny, c.nitm_u, a[k], b[k], v[k], x->P, x->Q, s), 4 * c.nitm_u);
     }
     return M2D_OK;
 }
 
-static int solve5(m2d_ctx *x)
+static int solve5(m2d_ctx *x, cudaStream_t s)
 {
     const m2d_case &c = x->c;
     if (c.solver == 3) {
@@ -257,7 +276,7 @@ static int solve5(m2d_ctx *x)
         if (!x->net) return ctx_fail(M2D_ERR_ARG, "m2d_iterate: solver 3 needs a network (m2d_ctx_set_unet)");
         m2d_learned_report r;
         const int rc = m2d_pprime_solve_learned(x->net, x->nx, x->ny, c.nitm_p, c.tol_p, x->f.ap, x->f.bp, x->f.pl,
-                                                x->f.Jp, x->ws5, 1, x->st, &r);
+                                                x->f.Jp, x->ws5, 1, s, &r);
         if (rc) return rc;
         x->learned_calls++;
         x->learned_accepted += r.accepted;
@@ -272,40 +291,166 @@ static int solve5(m2d_ctx *x)
         L.s[0].a = x->f.ap; L.s[0].b = x->f.bp; L.s[0].x = x->f.pl;
         L.s[0].ws = x->ws5;
         L.s[0].nit = x->dint + I_NIT_P; L.s[0].rr = x->dsc + S_RR + 4;
-        KL(launch_msi(5, L, 1, x->st), 2);   // A transpose + solve
+        KL(launch_msi(5, L, 1, s), 2);   // A transpose + solve
     } else {
-        KL(launch_tdma(5, x->nx, x->ny, c.nitm_p, x->f.ap, x->f.bp, x->f.pl, x->P, x->Q, x->st), 4 * c.nitm_p);
+        KL(launch_tdma(5, x->nx, x->ny, c.nitm_p, x->f.ap, x->f.bp, x->f.pl, x->P, x->Q, s), 4 * c.nitm_p);
     }
     return M2D_OK;
 }
 
-static double max4(double a, double b, double c, double d, int nan_policy)
+// ---- end-of-iteration scalars, the same arithmetic on the host and on the
+// device: the outer norm (src/mach2d_main.f90:338-395) and the next time step
+// (tstepper_dt, mod_tstepper_scarborough.f90:80-123 / the ramp)
+__host__ __device__ static inline bool is_nan(double v) { return v != v; }
+__host__ __device__ static inline double ctl_max4(double a, double b, double c, double d, int nan_policy)
 {
-    double v[4] = {a, b, c, d};
+    const double v[4] = {a, b, c, d};
     if (nan_policy == 1) {
-        for (double t : v) if (std::isnan(t)) return NAN;
+        for (int k = 0; k < 4; k++) if (is_nan(v[k])) return v[k];
         double m = a;
         for (int k = 1; k < 4; k++) if (v[k] > m) m = v[k];
         return m;
     }
-    double m = NAN;
-    for (double t : v) {
-        if (std::isnan(t)) continue;
-        if (std::isnan(m) || t > m) m = t;
+    double m = 0.0;
+    bool have = false;
+    for (int k = 0; k < 4; k++) {
+        if (is_nan(v[k])) continue;
+        if (!have || v[k] > m) { m = v[k]; have = true; }
     }
-    return m;
+    return have ? m : a + b + c + d;   // all NaN: a NaN
+}
+__host__ __device__ static inline double ctl_ramp_dt(int it, const StepCtl &k)
+{
+    double dt = 0.0;
+    if (it + 1 <= k.it1) dt = k.dt1;
+    if (it + 1 > k.it1 && it + 1 < k.it2) dt = k.dt1 + (k.dt2 - k.dt1) * (double)(it + 1 - k.it1) / (double)(k.it2 - k.it1);
+    if (it + 1 >= k.it2) dt = k.dt2;
+    return dt;
+}
+__host__ __device__ static inline void ctl_finish(const StepCtl &k, const double *hs, int it, double dt, double *norm,
+                                                  double *dt_next)
+{
+    const double eps = 10.0 * 2.220446049250313e-16;
+    double n = 0.0;
+    n = n + (hs[S_NU_B] > eps ? hs[S_NU_A] / hs[S_NU_B] : hs[S_NU_A]);
+    n = n + (hs[S_NV_B] > eps ? hs[S_NV_A] / hs[S_NV_B] : hs[S_NV_A]);
+    n = n + hs[S_NP];
+    if (k.energy_eq) n = n + (hs[S_NT_B] > eps ? hs[S_NT_A] / hs[S_NT_B] : hs[S_NT_A]);
+    *norm = n;
+    if (k.dtmodel == 1) {
+        const double cc = ctl_max4(hs[S_CC_U], hs[S_CC_V], hs[S_CC_T], hs[S_CC_P], k.nan_policy);
+        double hh;
+        if (cc < k.mincc) hh = k.h0 * sqrt(1.0 - cc / k.mincc);
+        else if (k.maxcc < cc) hh = -(k.h0 * sqrt(cc / k.maxcc - 1.0));
+        else hh = 0.0;
+        *dt_next = dt * (1.0 + hh);
+    } else {
+        *dt_next = ctl_ramp_dt(it, k);
+    }
+}
+static StepCtl step_ctl(const m2d_case &c)
+{
+    StepCtl k;
+    k.dtmodel = c.dtmodel; k.nan_policy = c.nan_policy; k.it1 = c.it1; k.it2 = c.it2;
+    k.energy_eq = !(c.modvis == 0 && c.ktm == 0); k.itpmax = c.itpmax;
+    k.dt1 = c.dt1; k.dt2 = c.dt2; k.h0 = c.h0; k.mincc = c.mincc; k.maxcc = c.maxcc; k.tolm = c.tolm;
+    return k;
 }
 
-extern "C" int m2d_iterate(m2d_ctx *x, m2d_report *rep)
+// device control kernels of a captured iteration (one thread each)
+__global__ void k_ctx_pavg(double *dsc, int nx, int ny)
 {
-    if (!x) return ctx_fail(M2D_ERR_ARG, "m2d_iterate: null context");
-    TRY(cudaSetDevice(x->device));
+    dsc[S_PAVG] = dsc[S_PSUM] / ((double)(nx - 2) * (double)(ny - 2));
+}
+__global__ void k_ctx_itp_reset(int *dint) { dint[I_ITP] = 0; }
+// after a p' cycle: normpl = max|p'| / p_avg (src/mach2d_main.f90:307) and the
+// loop's exit (normpl < tolm or itpmax cycles) as the WHILE node's condition
+__global__ void k_ctx_itp_decide(double *dsc, int *dint, double tolm, int itpmax, cudaGraphConditionalHandle h)
+{
+    const int itp = dint[I_ITP] + 1;
+    dint[I_ITP] = itp;
+    dint[I_ITP_TOTAL] += 1;
+    const double normpl = dsc[S_MAXPL] / dsc[S_PAVG];
+    dsc[S_NORMPL] = normpl;
+    cudaGraphSetConditional(h, (normpl < tolm || itp >= itpmax) ? 0u : 1u);
+}
+__global__ void k_ctx_finish(double *dsc, StepCtl k)
+{
+    const int it = (int)dsc[S_IT] + 1;
+    double norm, dtn;
+    ctl_finish(k, dsc, it, dsc[S_DT], &norm, &dtn);
+    dsc[S_NORM] = norm;
+    dsc[S_DT] = dtn;
+    dsc[S_IT] = (double)it;
+}
+
+// one p' cycle on stream s: coefficients, boundary rows, source, solve,
+// corrections, face densities and max|p'| (src/mach2d_main.f90:259-309)
+static int issue_p_cycle(m2d_ctx *x, const Params &q, cudaStream_t s)
+{
+    Fields &f = x->f;
+    KL(launch_p_assembly(f, q, ASM_COEF, s), 1);
+    KL(launch_set_bcpl(f, s), 1);
+    KL(launch_p_assembly(f, q, ASM_SRC, s), 1);
+    int rc = solve5(x, s);
+    if (rc) return rc;
+    KL(launch_velocity_correction_at_faces(f, s), 1);
+    KL(launch_velocities_at_boundary_faces(f, x->c.modvis, s), 1);
+    KL(launch_p_ro_correction(f, 1, 1, s), 1);
+    KL(launch_density_at_faces(f, x->c.beta, s), 1);
+    RedArgs r = red(x, RED_MAXABS_ALL); r.x = f.pl;
+    KL(launch_reduce(r, x->part, x->dsc + S_MAXPL, s), 2);
+    return M2D_OK;
+}
+
+// during a capture of x->st: a conditional WHILE node whose body (captured on
+// x->st2) is one p' cycle followed by k_ctx_itp_decide
+static int capture_p_loop(m2d_ctx *x, const Params &q)
+{
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t nd = 0;
+    TRY(cudaStreamGetCaptureInfo(x->st, &cs, nullptr, &g, &deps, &nd));
+    cudaGraphConditionalHandle h;
+    TRY(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    TRY(cudaGraphAddNode(&node, g, deps, nd, &cp));
+    TRY(cudaStreamUpdateCaptureDependencies(x->st, &node, 1, cudaStreamSetCaptureDependencies));
+    TRY(cudaStreamBeginCaptureToGraph(x->st2, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeRelaxed));
+    const long long l0 = x->launches;
+    int rc = issue_p_cycle(x, q, x->st2);
+    if (rc == M2D_OK) {
+        k_ctx_itp_decide<<<1, 1, 0, x->st2>>>(x->dsc, x->dint, x->c.tolm, x->c.itpmax, h);
+        x->launches++;
+    }
+    cudaGraph_t body = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(x->st2, &body);
+    x->launches_body = x->launches - l0;
+    if (rc) return rc;
+    TRY(e);
+    TRY(cudaGetLastError());
+    return M2D_OK;
+}
+
+// the launches of one outer iteration, src/mach2d_main.f90:94-445.  Host mode:
+// the p' loop exit is read back after each cycle.  Capture mode: the p' loop
+// is captured as a WHILE node, p_avg and the end-of-iteration scalars are
+// computed on the device, and nothing is read back.
+static int issue_iteration(m2d_ctx *x, bool capture, int *itp_used_out)
+{
     const m2d_case &c = x->c;
     Fields &f = x->f;
     Params q = x->q;
     cudaStream_t st = x->st;
-    const int it = ++x->it;
-    q.dt = x->dt;
+    if (capture) q.dtp = x->dsc + S_DT;
+    else q.dt = x->dt;
     TRY(cudaMemsetAsync(x->dint, 0, I_COUNT * sizeof(int), st));
     KL(launch_backup(f, st), 1);
     KL(launch_inlet_update(f, q, st), 1);
@@ -315,7 +460,12 @@ extern "C" int m2d_iterate(m2d_ctx *x, m2d_report *rep)
         KL(launch_reduce(r, x->part, x->dsc + S_PSUM, st), 2);
     }
     KL(launch_g(f, q.Rg, st), 1);
-    TRY(cudaMemcpyAsync(x->hsc, x->dsc, S_COUNT * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (capture) {
+        k_ctx_pavg<<<1, 1, 0, st>>>(x->dsc, x->nx, x->ny);
+        KL(cudaGetLastError(), 1);
+    } else {
+        TRY(cudaMemcpyAsync(x->hsc, x->dsc, S_COUNT * sizeof(double), cudaMemcpyDeviceToHost, st));
+    }
     bool have_pavg = false;
     int itp_used = 0;
     for (int itm = 1; itm <= c.itmmax; itm++) {
@@ -328,7 +478,7 @@ extern "C" int m2d_iterate(m2d_ctx *x, m2d_report *rep)
         {
             double *a[2] = {f.au, f.av}, *b[2] = {f.bu, f.bv}, *v[2] = {f.u, f.v};
             int is[2] = {I_NIT_U, I_NIT_V}, rs[2] = {S_RR, S_RR + 2};
-            int rc = solve9(x, 2, a, b, v, is, rs);
+            int rc = solve9(x, st, 2, a, b, v, is, rs);
             if (rc) return rc;
         }
         {
@@ -341,30 +491,28 @@ extern "C" int m2d_iterate(m2d_ctx *x, m2d_report *rep)
             r.kind = RED_SUM_ABS_B;
             KL(launch_reduce(r, x->part, x->dsc + S_NV_B, st), 2);
         }
-        KL(launch_velocities_at_internal_faces(f, q.dt, st), 1);
+        KL(launch_velocities_at_internal_faces(f, q.dt, st, q.dtp), 1);
         KL(launch_velocities_at_boundary_faces(f, c.modvis, st), 1);
         TRY(cudaMemsetAsync(f.pl, 0, x->N * sizeof(double), st));
-        for (int itp = 1; itp <= c.itpmax; itp++) {
-            itp_used = itp;
-            KL(launch_p_assembly(f, q, ASM_COEF, st), 1);
-            KL(launch_set_bcpl(f, st), 1);
-            KL(launch_p_assembly(f, q, ASM_SRC, st), 1);
-            int rc = solve5(x);
+        if (capture) {
+            k_ctx_itp_reset<<<1, 1, 0, st>>>(x->dint);
+            KL(cudaGetLastError(), 1);
+            int rc = capture_p_loop(x, q);
             if (rc) return rc;
-            KL(launch_velocity_correction_at_faces(f, st), 1);
-            KL(launch_velocities_at_boundary_faces(f, c.modvis, st), 1);
-            KL(launch_p_ro_correction(f, 1, 1, st), 1);
-            KL(launch_density_at_faces(f, c.beta, st), 1);
-            RedArgs r = red(x, RED_MAXABS_ALL); r.x = f.pl;
-            KL(launch_reduce(r, x->part, x->dsc + S_MAXPL, st), 2);
-            TRY(cudaMemcpyAsync(x->hsc + S_MAXPL, x->dsc + S_MAXPL, sizeof(double), cudaMemcpyDeviceToHost, st));
-            TRY(cudaStreamSynchronize(st));
-            if (!have_pavg) {
-                x->p_avg = x->hsc[S_PSUM] / ((double)(x->nx - 2) * (double)(x->ny - 2));
-                have_pavg = true;
+        } else {
+            for (int itp = 1; itp <= c.itpmax; itp++) {
+                itp_used = itp;
+                int rc = issue_p_cycle(x, q, st);
+                if (rc) return rc;
+                TRY(cudaMemcpyAsync(x->hsc + S_MAXPL, x->dsc + S_MAXPL, sizeof(double), cudaMemcpyDeviceToHost, st));
+                TRY(cudaStreamSynchronize(st));
+                if (!have_pavg) {
+                    x->p_avg = x->hsc[S_PSUM] / ((double)(x->nx - 2) * (double)(x->ny - 2));
+                    have_pavg = true;
+                }
+                x->normpl = x->hsc[S_MAXPL] / x->p_avg;
+                if (x->normpl < c.tolm) break;
             }
-            x->normpl = x->hsc[S_MAXPL] / x->p_avg;
-            if (x->normpl < c.tolm) break;
         }
         {
             RedArgs r = red(x, RED_NORM_L1_5D); r.a = f.ap; r.b = f.bp; r.x = f.pl;
@@ -376,7 +524,7 @@ extern "C" int m2d_iterate(m2d_ctx *x, m2d_report *rep)
     {
         RedArgs r = red(x, RED_MASS);
         r.rp = f.rp; r.re = f.re; r.rn = f.rn; r.Jp = f.Jp; r.ro = f.ro; r.roa = f.roa;
-        r.ron = f.ron; r.roe = f.roe; r.Uce = f.Uce; r.Vcn = f.Vcn; r.dt = q.dt;
+        r.ron = f.ron; r.roe = f.roe; r.Uce = f.Uce; r.Vcn = f.Vcn; r.dt = q.dt; r.dtp = q.dtp;
         KL(launch_reduce(r, x->part, x->dsc + S_RMASS, st), 2);
     }
     // T from total-enthalpy conservation for Euler with constant properties
@@ -389,7 +537,7 @@ extern "C" int m2d_iterate(m2d_ctx *x, m2d_report *rep)
         KL(launch_set_bcT(f, c.Twall, st), 1);
         double *a[1] = {f.at}, *b[1] = {f.bt}, *v[1] = {f.T};
         int is[1] = {I_NIT_T}, rs[1] = {S_RR + 6};
-        int rc = solve9(x, 1, a, b, v, is, rs);
+        int rc = solve9(x, st, 1, a, b, v, is, rs);
         if (rc) return rc;
         RedArgs r = red(x, RED_NORM_L1_9D); r.a = f.at; r.b = f.bt; r.x = f.T;
         KL(launch_reduce(r, x->part, x->dsc + S_NT_A, st), 2);
@@ -409,29 +557,99 @@ extern "C" int m2d_iterate(m2d_ctx *x, m2d_report *rep)
         KL(launch_reduce(r, x->part, x->dsc + S_CC_P, st), 2);
     }
     KL(launch_mass_flow_thrust(f, x->dsc + S_FMI, st), 1);
-    TRY(cudaMemcpyAsync(x->hsc, x->dsc, S_COUNT * sizeof(double), cudaMemcpyDeviceToHost, st));
-    TRY(cudaMemcpyAsync(x->hint, x->dint, I_COUNT * sizeof(int), cudaMemcpyDeviceToHost, st));
-    TRY(cudaStreamSynchronize(st));
+    if (capture) {
+        k_ctx_finish<<<1, 1, 0, st>>>(x->dsc, step_ctl(c));
+        KL(cudaGetLastError(), 1);
+    }
+    *itp_used_out = itp_used;
+    return M2D_OK;
+}
+
+// captures issue_iteration once into x->exec
+static int build_graph(m2d_ctx *x)
+{
+    if (!x->st2) TRY(cudaStreamCreateWithFlags(&x->st2, cudaStreamNonBlocking));
+    TRY(cudaStreamBeginCapture(x->st, cudaStreamCaptureModeRelaxed));
+    const long long l0 = x->launches;
+    int itp = 0;
+    const int rc = issue_iteration(x, true, &itp);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(x->st, &g);
+    const long long captured = x->launches - l0;
+    x->launches = l0;                       // capturing launches nothing
+    if (rc || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        (void)cudaGetLastError();
+        if (rc) return rc;
+        m2d_set_last_error(e, "m2d_iterate: capture", __FILE__, __LINE__);
+        return M2D_ERR_CUDA;
+    }
+    x->launches_fixed = captured - (long long)x->c.itmmax * x->launches_body;
+    cudaError_t ei = cudaGraphInstantiate(&x->exec, g, 0);
+    if (ei != cudaSuccess) {
+        cudaGraphDestroy(g);
+        m2d_set_last_error(ei, "m2d_iterate: cudaGraphInstantiate", __FILE__, __LINE__);
+        return M2D_ERR_CUDA;
+    }
+    x->graph = g;
+    return M2D_OK;
+}
+
+extern "C" int m2d_ctx_set_graph(m2d_ctx *x, int on)
+{
+    if (!x) return ctx_fail(M2D_ERR_ARG, "m2d_ctx_set_graph: null context");
+    if (on && x->c.solver == 3)
+        return ctx_fail(M2D_ERR_ARG, "m2d_ctx_set_graph: solver 3 decides on the host and is not captured");
+    TRY(cudaSetDevice(x->device));
+    if (on && !x->graph_on) {
+        // the device copies of dt and of the iteration counter start from the host's
+        x->hsc[S_DT] = x->dt;
+        x->hsc[S_IT] = (double)x->it;
+        TRY(cudaMemcpyAsync(x->dsc + S_DT, x->hsc + S_DT, sizeof(double), cudaMemcpyHostToDevice, x->st));
+        TRY(cudaMemcpyAsync(x->dsc + S_IT, x->hsc + S_IT, sizeof(double), cudaMemcpyHostToDevice, x->st));
+        TRY(cudaStreamSynchronize(x->st));
+    }
+    x->graph_on = on != 0;
+    return M2D_OK;
+}
+
+extern "C" int m2d_iterate(m2d_ctx *x, m2d_report *rep)
+{
+    if (!x) return ctx_fail(M2D_ERR_ARG, "m2d_iterate: null context");
+    TRY(cudaSetDevice(x->device));
+    const m2d_case &c = x->c;
+    cudaStream_t st = x->st;
+    const int it = ++x->it;
+    int itp_used = 0;
     const double *hs = x->hsc;
-    const double eps = 10.0 * 2.220446049250313e-16;
-    double norm = 0.0;
-    norm = norm + (hs[S_NU_B] > eps ? hs[S_NU_A] / hs[S_NU_B] : hs[S_NU_A]);
-    norm = norm + (hs[S_NV_B] > eps ? hs[S_NV_A] / hs[S_NV_B] : hs[S_NV_A]);
-    norm = norm + hs[S_NP];
-    if (!h_conservation) norm = norm + (hs[S_NT_B] > eps ? hs[S_NT_A] / hs[S_NT_B] : hs[S_NT_A]);
-    x->norm = norm;
+    if (x->graph_on) {
+        if (!x->exec) {
+            int rc = build_graph(x);
+            if (rc) { x->it--; return rc; }
+        }
+        TRY(cudaGraphLaunch(x->exec, st));
+        TRY(cudaMemcpyAsync(x->hsc, x->dsc, S_COUNT * sizeof(double), cudaMemcpyDeviceToHost, st));
+        TRY(cudaMemcpyAsync(x->hint, x->dint, I_COUNT * sizeof(int), cudaMemcpyDeviceToHost, st));
+        TRY(cudaStreamSynchronize(st));
+        itp_used = x->hint[I_ITP];
+        x->launches += x->launches_fixed + x->launches_body * x->hint[I_ITP_TOTAL];
+        x->p_avg = hs[S_PAVG];
+        x->normpl = hs[S_NORMPL];
+        x->norm = hs[S_NORM];
+        x->dt = hs[S_DT];
+    } else {
+        int rc = issue_iteration(x, false, &itp_used);
+        if (rc) return rc;
+        TRY(cudaMemcpyAsync(x->hsc, x->dsc, S_COUNT * sizeof(double), cudaMemcpyDeviceToHost, st));
+        TRY(cudaMemcpyAsync(x->hint, x->dint, I_COUNT * sizeof(int), cudaMemcpyDeviceToHost, st));
+        TRY(cudaStreamSynchronize(st));
+        double norm, dtn;
+        ctl_finish(step_ctl(c), hs, it, x->dt, &norm, &dtn);
+        x->norm = norm;
+        x->dt = dtn;
+    }
     x->rmass = hs[S_RMASS];
     x->itp_used = itp_used;
-    if (c.dtmodel == 1) {
-        double cc = max4(hs[S_CC_U], hs[S_CC_V], hs[S_CC_T], hs[S_CC_P], c.nan_policy);
-        double hh;
-        if (cc < c.mincc) hh = c.h0 * std::sqrt(1.0 - cc / c.mincc);
-        else if (c.maxcc < cc) hh = -(c.h0 * std::sqrt(cc / c.maxcc - 1.0));
-        else hh = 0.0;
-        x->dt = x->dt * (1.0 + hh);
-    } else {
-        x->dt = ramp_dt(it, c);
-    }
     if (rep) {
         rep->it = it; rep->dt = x->dt; rep->norm = x->norm; rep->normpl = x->normpl;
         rep->rmass = x->rmass; rep->fmi = hs[S_FMI]; rep->fme = hs[S_FME]; rep->Fd = hs[S_FD];

@@ -31,6 +31,7 @@ struct Fields {
 struct Params {
     int modvis, coord;
     double beta, dt, Rg, gamma, p0, T0, Cpref, Href, Twall;
+    const double *dtp;     // when set, dt is read from this device word (captured iterations)
 };
 
 // what = bit 1: coefficients, bit 2: source (lets one kernel serve both the
@@ -44,7 +45,8 @@ cudaError_t launch_u_assembly(const Fields &f, const Params &q, int what, cudaSt
 cudaError_t launch_v_assembly(const Fields &f, const Params &q, int what, cudaStream_t st);
 cudaError_t launch_T_assembly(const Fields &f, const Params &q, cudaStream_t st);
 cudaError_t launch_p_assembly(const Fields &f, const Params &q, int what, cudaStream_t st);
-cudaError_t launch_velocities_at_internal_faces(const Fields &f, double dt, cudaStream_t st);
+cudaError_t launch_velocities_at_internal_faces(const Fields &f, double dt, cudaStream_t st,
+                                                const double *dtp = nullptr);
 cudaError_t launch_internal_simplec(const Fields &f, cudaStream_t st);
 cudaError_t launch_p_ro_correction(const Fields &f, int do_p, int do_ro, cudaStream_t st);
 cudaError_t launch_uv_nodes_correction(const Fields &f, cudaStream_t st);
@@ -84,6 +86,7 @@ struct RedArgs {
     // mass-conservation inputs
     const double *rp, *re, *rn, *Jp, *ro, *roa, *ron, *roe, *Uce, *Vcn, *u, *v;
     double dt;
+    const double *dtp;     // when set, dt is read from this device word
 };
 cudaError_t launch_reduce(const RedArgs &r, double *part, double *out, cudaStream_t st);
 

@@ -67,7 +67,7 @@ __device__ __forceinline__ double cell_value(const RedArgs &r, int i, int j)
         double fmw = r.roe[npw] * r.re[npw] * r.Uce[npw];
         double fmn = r.ron[np] * r.rn[np] * r.Vcn[np];
         double fms = r.ron[nps] * r.rn[nps] * r.Vcn[nps];
-        return fabs((r.ro[np] - r.roa[np]) * r.rp[np] / (r.Jp[np] * r.dt) + fme - fmw + fmn - fms);
+        return fabs((r.ro[np] - r.roa[np]) * r.rp[np] / (r.Jp[np] * (r.dtp ? *r.dtp : r.dt)) + fme - fmw + fmn - fms);
     }
     case RED_MEAN_CC_9D: {
         const double *a = r.a;

@@ -68,7 +68,7 @@ __global__ void k_u_assembly(Fields f, Params q, int what)
     const double mpa = f.roa[np] * f.rp[np] / f.Jp[np];
     const double as = sgn05(Vcn[nps]), an = sgn05(Vcn[np]);
     const double aw = sgn05(Uce[npw]), ae = sgn05(Uce[np]);
-    const double dt = q.dt;
+    const double dt = q.dtp ? *q.dtp : q.dt;
     if (what & ASM_COEF) {
         double *a = f.au;
         if (q.modvis == 0) {
@@ -166,7 +166,7 @@ __global__ void k_v_assembly(Fields f, Params q, int what)
     const double mpa = f.roa[np] * f.rp[np] / f.Jp[np];
     const double as = sgn05(Vcn[nps]), an = sgn05(Vcn[np]);
     const double aw = sgn05(Uce[npw]), ae = sgn05(Uce[np]);
-    const double dt = q.dt;
+    const double dt = q.dtp ? *q.dtp : q.dt;
     if (what & ASM_COEF) {
         double *a = f.av;
         if (q.modvis == 0) {
@@ -247,7 +247,7 @@ __global__ void k_T_assembly(Fields f, Params q)
     const long long npsw = nps - 1, npse = nps + 1, npnw = npn - 1, npne = npn + 1;
     const double *roe = f.roe, *ron = f.ron, *re = f.re, *rn = f.rn, *Uce = f.Uce, *Vcn = f.Vcn;
     const double *cp = f.cp, *u = f.u, *v = f.v, *T = f.T, *rp = f.rp, *Jp = f.Jp;
-    const double beta = q.beta, dt = q.dt, eps = 2.220446049250313e-16;
+    const double beta = q.beta, dt = q.dtp ? *q.dtp : q.dt, eps = 2.220446049250313e-16;
     const double fme = roe[np] * re[np] * Uce[np];
     const double fmw = roe[npw] * re[npw] * Uce[npw];
     const double fmn = ron[np] * rn[np] * Vcn[np];
@@ -383,7 +383,7 @@ __global__ void k_p_assembly(Fields f, Params q, int what)
     const long long np = IDX(i, j), nps = np - nx, npn = np + nx, npw = np - 1, npe = np + 1;
     const double *re = f.re, *rn = f.rn, *Uce = f.Uce, *Vcn = f.Vcn, *g = f.g;
     const double *de = f.de, *dn = f.dn, *roe = f.roe, *ron = f.ron;
-    const double dt = q.dt;
+    const double dt = q.dtp ? *q.dtp : q.dt;
     const double as = sgn05(Vcn[nps]), an = sgn05(Vcn[np]);
     const double aw = sgn05(Uce[npw]), ae = sgn05(Uce[np]);
     if (what & ASM_COEF) {
@@ -418,8 +418,9 @@ __global__ void k_p_assembly(Fields f, Params q, int what)
 }
 
 // get_velocities_at_internal_faces  src/equations/mach2d_coef.f90:1350-1501
-__global__ void k_faces_internal(Fields f, double dt)
+__global__ void k_faces_internal(Fields f, double dt, const double *dtp)
 {
+    if (dtp) dt = *dtp;
     const int nx = f.nx, ny = f.ny;
     const long long N = (long long)nx * ny;
     CELL_IJ
@@ -1031,8 +1032,8 @@ cudaError_t launch_T_assembly(const Fields &f, const Params &q, cudaStream_t st)
 { k_T_assembly<<<grid2d(f.nx, f.ny), kBlock2d, 0, st>>>(f, q); return cudaGetLastError(); }
 cudaError_t launch_p_assembly(const Fields &f, const Params &q, int what, cudaStream_t st)
 { k_p_assembly<<<grid2d(f.nx, f.ny), kBlock2d, 0, st>>>(f, q, what); return cudaGetLastError(); }
-cudaError_t launch_velocities_at_internal_faces(const Fields &f, double dt, cudaStream_t st)
-{ k_faces_internal<<<grid2d(f.nx, f.ny), kBlock2d, 0, st>>>(f, dt); return cudaGetLastError(); }
+cudaError_t launch_velocities_at_internal_faces(const Fields &f, double dt, cudaStream_t st, const double *dtp)
+{ k_faces_internal<<<grid2d(f.nx, f.ny), kBlock2d, 0, st>>>(f, dt, dtp); return cudaGetLastError(); }
 cudaError_t launch_internal_simplec(const Fields &f, cudaStream_t st)
 { k_simplec_internal<<<grid2d(f.nx, f.ny), kBlock2d, 0, st>>>(f); return cudaGetLastError(); }
 cudaError_t launch_p_ro_correction(const Fields &f, int do_p, int do_ro, cudaStream_t st)

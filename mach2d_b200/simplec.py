@@ -119,6 +119,12 @@ class Simplec:
         check(L.m2d_run(self._ctx, int(itmax), ctypes.byref(rep)))
         return rep
 
+    def set_graph(self, on=True):
+        """Run each outer iteration as one captured CUDA graph (m2d_ctx_set_graph)."""
+        L = lib()
+        L.m2d_ctx_set_graph.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        check(L.m2d_ctx_set_graph(self._ctx, 1 if on else 0))
+
     def set_unet(self, net):
         """Attaches the network solver 3 uses for its p' corrections (None detaches)."""
         L = lib()
