@@ -7,11 +7,22 @@ volumes (514 x 258 with the ghost ring), Euler, constant properties
 (nitm_u = 5, nitm_p = 20, tol 1e-2), itpmax = 20, SCARBOROUGH time stepper,
 FP64.  Metric: cell-updates/s = real cells x outer iterations / time.
 
+Each outer iteration runs as one captured CUDA graph (m2d_ctx_set_graph: the
+p' loop is a conditional node, its exit and the next time step are decided
+on the device), which gives bitwise the results of the host-driven mode.
+
 Each rank runs its own nozzle instance (replicas: a single grid does not
 shard, see the MSI factorisation); value = total cell-updates of all ranks /
 max-over-ranks time.  The per-iteration working set (~140 MB of fields,
 coefficients and solver factors) exceeds the 126 MB L2, so no explicit L2
 flush is inserted between iterations.
+
+Besides the headline line, one-GPU runs add: `fp32_sweeps` (the same
+workload with MSI factors and sweeps in FP32 inside the FP64 iteration),
+`time_to_residual` (the 80x40 Euler nozzle to its stopping iteration, FP64
+and FP32 sweeps on the GPU, and the serial oracle extrapolated from a
+sample), and `learned` (the learned p' correction trained on this workload's
+harvested p' systems, against plain MSI on held-out ones).
 
 --impl reference times the CPU restatement of the reference (the reference
 itself is Fortran and no Fortran compiler exists on this image) on the
@@ -46,6 +57,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch", type=int, default=8,
                     help="instances of the same workload for the batch throughput figure (0: skip)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the time-to-residual, FP32-sweep and learned-correction figures")
     return ap.parse_args()
 
 
@@ -206,6 +219,7 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     sim = Simplec(make_case(args.nxr, args.nyr), device=local)
+    sim.set_graph(True)          # one captured CUDA graph per outer iteration (bitwise the same results)
     L = lib()
     stream_ptr = ctypes.c_void_p()
     L.m2d_ctx_stream.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
@@ -251,14 +265,12 @@ def run_ours(args):
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
+    host = {f: pinned[f][1] for f in state}
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        for f in state:
-            sim.set_field(f, pinned[f][1])
+        sim.set_fields(host)         # one copy per field from pinned memory, one synchronisation
         sim.iterate()
-        for f in state:
-            src = sim.field(f)
-            pinned[f][1][:] = src
+        sim.get_fields(host)
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     if world > 1:
@@ -329,6 +341,10 @@ def run_ours(args):
                  "note": "independent instances of the same workload, one context and stream each"}
         b.close()
 
+    extras = {}
+    if world == 1 and not args.no_extras:
+        extras = run_extras(args, local)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, nsamp, secs = cpu_sample(args, args.cpu_seconds)
@@ -355,11 +371,165 @@ def run_ours(args):
             "batch": batch,
             "clocks": clk.summary(),
         }
+        line.update(extras)
         print(json.dumps(line), flush=True)
     sim.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def run_extras(args, local):
+    """Secondary figures, each on one GPU: the same workload with FP32 sweeps;
+    the time to the stopping residual of the 80x40 Euler nozzle (FP64, FP32
+    sweeps, and the serial oracle extrapolated from a sample); and what the
+    learned p' correction gains on this workload's p' systems."""
+    import numpy as np
+    import torch
+
+    from mach2d_b200 import unet
+    from mach2d_b200.simplec import Simplec, euler_cosine_case
+    out = {}
+    dev = torch.device("cuda", local)
+
+    # FP32 factors and sweeps inside the FP64 iteration (solver 2)
+    g = Simplec(euler_cosine_case(args.nxr, args.nyr, solver=2), device=local)
+    g.set_graph(True)
+    for _ in range(args.warmup):
+        g.iterate()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        g.iterate()
+    torch.cuda.synchronize()
+    s32 = time.perf_counter() - t0
+    out["fp32_sweeps"] = {"value": args.nxr * args.nyr * args.steps / s32, "unit": "cell-updates/s",
+                          "ms_per_step": 1e3 * s32 / args.steps,
+                          "timing": "host clock around the iterations (each ends in a read-back)",
+                          "note": "solver 2: MSI factors and sweeps in FP32 inside the FP64 iteration"}
+    g.close()
+
+    # time to the stopping residual (normpl < 1e-10 first at it, stop at 2 it) of the 80x40 nozzle
+    ttr = {"case": "C01 Euler 80x40, tolt 1e-10, SCARBOROUGH", "metric": "seconds to the stopping iteration"}
+    for solver, key in ((0, "gpu_fp64"), (2, "gpu_fp32_sweeps")):
+        g = Simplec(euler_cosine_case(80, 40, solver=solver), device=local)
+        g.set_graph(True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rep = g.run(200000)
+        torch.cuda.synchronize()
+        ttr[key] = {"seconds": time.perf_counter() - t0, "iterations": rep.it, "normpl": rep.normpl,
+                    "Cd": g.integrals()[3]}
+        g.close()
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from _oracle import OracleCase
+    o = OracleCase(euler_cosine_case(80, 40))
+    t0 = time.perf_counter()
+    n = 0
+    while time.perf_counter() - t0 < 3.0:
+        o.iterate()
+        n += 1
+    per = (time.perf_counter() - t0) / n
+    it_gpu = ttr["gpu_fp64"]["iterations"]
+    ttr["cpu_oracle_serial"] = {"seconds": per * it_gpu, "iterations": it_gpu, "cores": 1,
+                                "sample": f"extrapolated from {n} iterations of the serial C restatement"}
+    out["time_to_residual"] = ttr
+
+    # learned p' correction on this workload's p' systems
+    g = Simplec(make_case(args.nxr, args.nyr), device=local)
+    nx, ny = g.nx, g.ny
+    H, W = unet.image_shape(nx, ny)
+    pairs = unet.PairSet(48, H, W, device=local)
+    held = []
+    for _ in range(3):
+        g.iterate()
+    unet.harvest(g, pairs, iters_between=2, count=40)
+    hp = unet.PairSet(8, H, W, device=local)
+    unet.harvest(g, hp, iters_between=3, count=8, held_out=held)
+    Jp = torch.from_numpy(g.field("Jp")).to(dev)
+    g.close()
+    net = unet.UNet(8, H, W, device=local, seed=1)
+    t0 = time.perf_counter()
+    hist = unet.train(net, pairs, 300, batch=8, lr=2e-3, lr_final=1e-4)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    one = unet.UNet(1, H, W, device=local, params=net.params())
+    net.close()
+    Lb = unet._bind()
+    work = torch.empty(Lb.m2d_msi_workspace_doubles(5, nx, ny), dtype=torch.float64, device=dev)
+    nit = torch.zeros(2, dtype=torch.int32, device=dev)
+    res = {"msi_fp64": [], "msi_fp32": [], "learned_fp32": []}
+    nits = {"msi_fp64": [], "msi_fp32": [], "learned_fp32": []}
+    ratio = []
+    for a, b in held:
+        for key, prec in (("msi_fp64", 0), ("msi_fp32", 1)):
+            x = torch.zeros(nx * ny, dtype=torch.float64, device=dev)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            unet.msi5(nx, ny, 20, 1e-2, a, b, x, work, nit, prec=prec)
+            torch.cuda.synchronize()
+            res[key].append(time.perf_counter() - t0)
+            nits[key].append(int(nit[0].item()))
+        x = torch.zeros(nx * ny, dtype=torch.float64, device=dev)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = one.solve(nx, ny, 20, 1e-2, a, b, x, Jp, work, prec=1)
+        torch.cuda.synchronize()
+        res["learned_fp32"].append(time.perf_counter() - t0)
+        nits["learned_fp32"].append(r.nit)
+        ratio.append(r.r1 / r.r0)
+    one.close()
+    out["sweep256"] = run_sweep(local, n=256, iters=20)
+    out["learned"] = {
+        "train": {"pairs": pairs.n, "steps": 300, "batch": 8, "seconds": train_s, "loss_first": hist[0],
+                  "loss_last50": float(np.mean(hist[-50:]))},
+        "held_out_systems": len(held),
+        "residual_after_correction_median": float(np.median(ratio)),
+        "p_solve_ms_median": {k: 1e3 * float(np.median(v)) for k, v in res.items()},
+        "msi_iterations_mean": {k: float(np.mean(v)) for k, v in nits.items()},
+        "tolerance": "p' solve to |r| < 1e-2 |r0| (nitm_p = 20), host clock per solve"}
+    return out
+
+
+def sweep_cases(n, seed=2024):
+    """The batched sweep: n Euler nozzles drawn from the seed, nx in 64..512,
+    ny in 32..128, Rin in [1.5, 2.5], Rout in [1.3, 2.2], Lc in [1, 3],
+    Ld in [2, 6], p0 in [5e5, 3e6] Pa, T0 in [600, 1500] K; FP32 sweeps."""
+    import numpy as np
+
+    from mach2d_b200.simplec import euler_cosine_case
+    rng = np.random.default_rng(seed)
+    cases = []
+    for _ in range(n):
+        cases.append(euler_cosine_case(int(rng.integers(64, 513)), int(rng.integers(32, 129)),
+                                       Rin=rng.uniform(1.5, 2.5), Rout=rng.uniform(1.3, 2.2), Lc=rng.uniform(1, 3),
+                                       Ld=rng.uniform(2, 6), p0=rng.uniform(5e5, 3e6), T0=rng.uniform(600, 1500),
+                                       solver=2))
+    return cases
+
+
+def run_sweep(local, n, iters):
+    import torch
+
+    from mach2d_b200.simplec import Batch
+    cases = sweep_cases(n)
+    t0 = time.perf_counter()
+    b = Batch(cases, device=local)
+    for s in b.instances:
+        s.set_graph(True)
+    setup = time.perf_counter() - t0
+    b.iterate(2)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    b.iterate(iters)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    cells = sum(c.nxr * c.nyr for c in cases)
+    b.close()
+    return {"instances": n, "iterations": iters, "value": cells * iters / dt, "unit": "cell-updates/s",
+            "real_cells": cells, "setup_seconds": setup,
+            "note": "independent Euler nozzles of the seeded sweep distribution, FP32 sweeps, one captured graph "
+                    "per instance iteration, host worker threads"}
 
 
 def main():

@@ -376,6 +376,12 @@ int m2d_run(m2d_ctx *ctx, int itmax, m2d_report *last);
 /* copy a named field (reference variable name: "u", "p", "au", "Tbn", ...) */
 int m2d_get_field(m2d_ctx *ctx, const char *name, double *host, long n);
 int m2d_set_field(m2d_ctx *ctx, const char *name, const double *host, long n);
+/* several fields per call (one copy each, one synchronisation; pinned host
+ * buffers make the copies asynchronous DMA) */
+int m2d_set_fields(m2d_ctx *ctx, int count, const char *const *names, const double *const *host,
+                   const long *n);
+int m2d_get_fields(m2d_ctx *ctx, int count, const char *const *names, double *const *host,
+                   const long *n);
 /* named scalars: dt, norm, normpl, rmass, p_avg, Href, Cpref, fm1D, Fd1D,
  * Fpv1D, Sg, it, it_stop */
 int m2d_get_scalar(const m2d_ctx *ctx, const char *name, double *out);

@@ -698,6 +698,33 @@ extern "C" int m2d_set_field(m2d_ctx *x, const char *name, const double *host, l
     return M2D_OK;
 }
 
+// several fields per call: one asynchronous copy each, one synchronisation
+static int copy_fields(m2d_ctx *x, int count, const char *const *names, double *const *host, const long *n,
+                       bool to_device)
+{
+    if (!x || count < 0 || (count > 0 && (!names || !host || !n)))
+        return ctx_fail(M2D_ERR_ARG, "m2d_set_fields/m2d_get_fields: null argument");
+    TRY(cudaSetDevice(x->device));
+    for (int k = 0; k < count; k++) {
+        long len = 0;
+        double *d = names[k] ? plane_ptr(x, names[k], &len) : nullptr;
+        if (!d || !host[k]) return ctx_fail(M2D_ERR_ARG, "m2d_set_fields/m2d_get_fields: unknown field");
+        if (to_device ? n[k] != len : n[k] < len)
+            return ctx_fail(M2D_ERR_ARG, "m2d_set_fields/m2d_get_fields: size mismatch");
+        if (to_device)
+            TRY(cudaMemcpyAsync(d, host[k], (size_t)len * sizeof(double), cudaMemcpyHostToDevice, x->st));
+        else
+            TRY(cudaMemcpyAsync(host[k], d, (size_t)len * sizeof(double), cudaMemcpyDeviceToHost, x->st));
+    }
+    TRY(cudaStreamSynchronize(x->st));
+    return M2D_OK;
+}
+extern "C" int m2d_set_fields(m2d_ctx *x, int count, const char *const *names, const double *const *host,
+                              const long *n)
+{ return copy_fields(x, count, names, const_cast<double *const *>(host), n, true); }
+extern "C" int m2d_get_fields(m2d_ctx *x, int count, const char *const *names, double *const *host, const long *n)
+{ return copy_fields(x, count, names, host, n, false); }
+
 extern "C" int m2d_get_scalar(const m2d_ctx *x, const char *name, double *out)
 {
     if (!x || !name || !out) return ctx_fail(M2D_ERR_ARG, "m2d_get_scalar: null argument");

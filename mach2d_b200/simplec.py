@@ -141,6 +141,30 @@ class Simplec:
         check(L.m2d_get_field(self._ctx, name.encode(), out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), n))
         return out
 
+    def _fields_call(self, fn, arrays):
+        names = list(arrays)
+        n = len(names)
+        cn = (ctypes.c_char_p * n)(*[k.encode() for k in names])
+        ptrs = (ctypes.POINTER(ctypes.c_double) * n)()
+        sizes = (ctypes.c_long * n)()
+        for k, name in enumerate(names):
+            a = arrays[name]
+            if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous):
+                raise TypeError("expected C-contiguous float64 arrays")
+            ptrs[k] = a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+            sizes[k] = a.size
+        fn.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_char_p),
+                       ctypes.POINTER(ctypes.POINTER(ctypes.c_double)), ctypes.POINTER(ctypes.c_long)]
+        check(fn(self._ctx, n, cn, ptrs, sizes))
+
+    def set_fields(self, arrays):
+        """Uploads several named fields {name: float64 array} with one synchronisation."""
+        self._fields_call(lib().m2d_set_fields, arrays)
+
+    def get_fields(self, arrays):
+        """Downloads several named fields into the given float64 arrays."""
+        self._fields_call(lib().m2d_get_fields, arrays)
+
     def set_field(self, name, values):
         values = np.ascontiguousarray(values, dtype=np.float64)
         L = lib()
