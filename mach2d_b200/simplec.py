@@ -119,6 +119,47 @@ class Simplec:
         check(L.m2d_run(self._ctx, int(itmax), ctypes.byref(rep)))
         return rep
 
+    def run_listing(self, itmax, fh, wlf=1):
+        """Like run(), writing the reference's residual listing to `fh`: a row
+        every `wlf` iterations and the last one again after the loop
+        (src/mach2d_main.f90:420-466)."""
+        from .listing import ResidualListing
+        lst = ResidualListing(fh, wlf)
+        rep = None
+        for _ in range(itmax):
+            rep = self.iterate()
+            lst.write(rep)
+            if self.scalar("it_stop") == rep.it:
+                break
+        if rep is not None:
+            lst.write(rep, finished=True)
+        return rep
+
+    def main_results(self, rep, rcg=None):
+        """write_main_results (mod_intflow_postp.f90:1062-1256) from the device
+        fields: (blocks, text).  rcg: the throat's radius of curvature (N01:
+        Rc2; C01: that of the diverging cosine, Ld^2 / (0.4 pi^2))."""
+        import math
+        from .listing import main_results
+        c = self.case
+        if rcg is None:
+            rcg = c.Rc2 if c.geom == 1 else c.Ld ** 2 / (0.4 * math.pi ** 2)
+        f = {k: self.field(k) for k in ("x", "y", "re", "ye", "p", "roe", "u", "Uce")}
+        nx, ny, y = self.nx, self.ny, f["y"]
+        ig = 1
+        for i in range(2, nx):
+            if y[(ny - 2) * nx + i - 2] < y[(ny - 2) * nx + i - 1]:
+                ig = i - 1
+                break
+        if c.ktm == 0:
+            gamma = c.gamma
+        else:                                    # gm(T0), as intflow_init takes it
+            from .thermo import mixture_eval
+            gamma = mixture_eval(c.mix, c.T0)[3]
+        return main_results(nx, ny, f["x"], y, f["re"], f["ye"], f["p"], f["roe"], f["u"], f["Uce"],
+                            self.scalar("Sg"), rcg, ig, gamma, c.p0, self.scalar("Fpv1D"), self.scalar("Fd1D"),
+                            self.scalar("fm1D"), rep.fme)
+
     def set_graph(self, on=True):
         """Run each outer iteration as one captured CUDA graph (m2d_ctx_set_graph)."""
         L = lib()
