@@ -57,6 +57,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch", type=int, default=8,
                     help="instances of the same workload for the batch throughput figure (0: skip)")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="drive each iteration from the host instead of one captured graph (same results; for "
+                         "profilers that do not look inside conditional graph nodes)")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the time-to-residual, FP32-sweep and learned-correction figures")
     return ap.parse_args()
@@ -219,7 +222,7 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     sim = Simplec(make_case(args.nxr, args.nyr), device=local)
-    sim.set_graph(True)          # one captured CUDA graph per outer iteration (bitwise the same results)
+    sim.set_graph(not args.no_graph)   # one captured CUDA graph per outer iteration (bitwise the same results)
     L = lib()
     stream_ptr = ctypes.c_void_p()
     L.m2d_ctx_stream.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
@@ -360,7 +363,8 @@ def run_ours(args):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded nozzle geometry, isentropic initial guess)",
-            "config": workload_config(args, {"p_cycles_per_iteration": sum(itp) / len(itp)}),
+            "config": workload_config(args, {"p_cycles_per_iteration": sum(itp) / len(itp),
+                                             "iteration_launch": "host loop" if args.no_graph else "captured CUDA graph"}),
             "e2e": {"value": e2e, "unit": "cell-updates/s", "h2d_bytes_per_step": nbytes,
                     "d2h_bytes_per_step": nbytes},
             "gpu_launches": launches,
