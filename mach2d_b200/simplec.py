@@ -31,13 +31,33 @@ class Case(ctypes.Structure):
         ("mix", Mixture),
     ]
 
+    @classmethod
+    def from_dict(cls, d):
+        """Inverse of as_dict (JSON round trips of float64 values are exact)."""
+        c = cls()
+        for k, _ in cls._fields_:
+            if k != "mix" and k in d:
+                setattr(c, k, d[k])
+        if d.get("ktm") == 1 and "mix" in d:
+            m = d["mix"]
+            c.mix.ngs, c.mix.Rg = m["ngs"], m["Rg"]
+            for q in range(m["ngs"]):
+                c.mix.Xi[q], c.mix.Yi[q], c.mix.Mi[q] = m["Xi"][q], m["Yi"][q], m["Mi"][q]
+                c.mix.Ri[q] = m["Ri"][q]
+                for k in range(10):
+                    c.mix.cpi[q][k] = m["cpi"][q][k]
+                for k in range(8):
+                    c.mix.mui[q][k] = m["mui"][q][k]
+                    c.mix.kpi[q][k] = m["kpi"][q][k]
+        return c
+
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_ if k != "mix"}
         if self.ktm == 1:
             m = self.mix
             n = m.ngs
             d["mix"] = {"ngs": n, "Rg": m.Rg, "Xi": list(m.Xi)[:n], "Yi": list(m.Yi)[:n],
-                        "Mi": list(m.Mi)[:n], "cpi": [list(r) for r in m.cpi][:n],
+                        "Mi": list(m.Mi)[:n], "Ri": list(m.Ri)[:n], "cpi": [list(r) for r in m.cpi][:n],
                         "mui": [list(r) for r in m.mui][:n], "kpi": [list(r) for r in m.kpi][:n]}
         return d
 
