@@ -458,7 +458,8 @@ int m2d_unet_loss_grad(m2d_unet *net, int nimg, const float *d_in, const float *
 int m2d_unet_adam(m2d_unet *net, float lr, float beta1, float beta2, float eps, void *stream);
 /* which convolutions run on the tcgen05 kernel (images of even height and a
  * width that is a multiple of 128): 0 none (all on the mma.sync kernel), 1
- * those with 96 or more input channels (default), 2 all that fit */
+ * those with 64 or more output or 48 or more input channels (default), 2 all
+ * that fit */
 int m2d_unet_set_tensor_path(int mode);
 /* synchronises; *flags = device error word (2: a tensor-core wait ran out,
  * returned as M2D_ERR_TIMEOUT) */

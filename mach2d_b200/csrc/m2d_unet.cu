@@ -14,6 +14,8 @@
 // on the tensor cores (mma.sync m16n8k16 BF16 -> FP32) from shared-memory
 // tiles read with ldmatrix; the halo tile is XOR-swizzled so that the eight
 // rows of every ldmatrix fall in distinct banks.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 #include <cmath>
 #include <cstring>
@@ -89,6 +91,7 @@ struct ConvArgs {
     int act;                       // 1: y = gelu(result)
     int nimg, H, W, cin, cout;
     int *err;                      // device error word (ERR_WAIT_TIMEOUT), may be null
+    const bf16 *wtc;               // the weights in the tcgen05 staging order, or null
 };
 
 template <int NT>
@@ -193,7 +196,6 @@ __global__ void __launch_bounds__(128) k_conv3x3(ConvArgs a)
 constexpr int kTcPix = 128, kTcHaloW = kTcPix + 2, kTcRows = 2, kTcHaloRows = kTcRows + 2;
 constexpr int kTcHaloBytes = 2 * kTcHaloRows * kTcHaloW * 16;
 constexpr int kTcMaxN = 256;
-constexpr int kTcStageMax = kTcHaloBytes + 9 * 2 * kTcMaxN * 16;
 constexpr unsigned kTcWaitCap = 1u << 24;
 
 __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
@@ -207,10 +209,6 @@ __device__ __forceinline__ uint32_t umma_idesc_bf16_f32(int M, int N)
     // D F32 (bits 4-5 = 1), A and B BF16 (bits 7-9, 10-12 = 1), both K-major,
     // N >> 3 at bit 17, M >> 4 at bit 24
     return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
-}
-__device__ __forceinline__ void tc_mbar_init(unsigned long long *b)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(b)) : "memory");
 }
 // bounded wait for the completion of phase `parity`; false when the cap ran out
 __device__ __forceinline__ bool tc_mbar_wait(unsigned long long *b, uint32_t parity)
@@ -226,122 +224,193 @@ __device__ __forceinline__ bool tc_mbar_wait(unsigned long long *b, uint32_t par
     }
     return false;
 }
-// 16-byte asynchronous copy global -> shared; zero-filled when !valid
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, bool valid)
+
+// ---- persistent, warp-specialised tcgen05 convolution fed by TMA
+// Each CTA loops over tiles (two 128-pixel row segments, as above).  One
+// lane of warp 8 stages (tile, chunk) items into a ring of S shared-memory
+// stages: two 4-D tensor-map loads (cp.async.bulk.tensor) bring the halo's two
+// 8-channel halves, each box [4 rows][130 pixels][8 channels] landing exactly
+// in the K-major operand layout (out-of-image pixels zero-filled), and one
+// bulk copy brings the chunk's weights from their staging-order copy; all
+// complete on the stage's `full` mbarrier.  One lane of warp 9 issues the
+// tile's MMAs into one of NB tensor-memory accumulator buffers and commits
+// each stage to its `empty` barrier and each finished tile to `tfull`.
+// Warps 0-7 run the epilogue: warp w reads tensor-memory lanes 32(w%4) ..
+// +31 of row w/4 and releases the buffer on `tempty`.  So the loads of the
+// next items, the MMAs of the current tile and the epilogue of the previous
+// one overlap.  Every wait is bounded; when one runs out the CTA sets the
+// error word and all roles stop.
+constexpr int kTcpThreads = 320;
+constexpr int kTcpSmemBudget = 200 * 1024;                   // staging ring
+constexpr int kTcpSmemMax = kTcpSmemBudget;    // two stages of the widest N fit: 2 x (kTcHaloBytes + 288 kTcMaxN)
+static_assert(2 * (kTcHaloBytes + 9 * 2 * kTcMaxN * 16) <= kTcpSmemBudget, "two stages must fit");
+constexpr int kTcHalfBytes = kTcHaloRows * kTcHaloW * 16;   // one 8-channel half of a halo chunk
+
+__device__ __forceinline__ void tc_mbar_init_n(unsigned long long *b, unsigned n)
 {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(valid ? 16 : 0) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(n) : "memory");
+}
+__device__ __forceinline__ void tc_mbar_arrive(unsigned long long *b)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
+}
+__device__ __forceinline__ void tc_mbar_expect(unsigned long long *b, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap *map, int c0, int c1, int c2, int c3,
+                                            unsigned long long *bar)
+{
+    asm volatile("cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];"
+                 ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3),
+                 "r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_t bytes, unsigned long long *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(dst), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
 }
 
-__global__ void __launch_bounds__(128, 1) k_conv3x3_tc(ConvArgs a)
+struct TcpShape {
+    int nstage, nbuf;      // staging ring depth, accumulator buffers
+    int tiles;             // tiles over all images
+};
+
+__global__ void __launch_bounds__(kTcpThreads, 1) k_conv3x3_tcp(ConvArgs a, TcpShape sh,
+                                                               const __grid_constant__ CUtensorMap xmap)
 {
     extern __shared__ __align__(1024) unsigned char tc_smem[];
-    __shared__ __align__(8) unsigned long long bar[2];
+    __shared__ __align__(8) unsigned long long full[4], empty[4], tfull[2], tempty[2], mdone;
     __shared__ uint32_t tmem_slot;
-    __shared__ int s_timeout;
-    const int N = a.cout;
+    __shared__ volatile int s_abort;
+    const int N = a.cout, S = sh.nstage, NB = sh.nbuf;
     const int stage_bytes = kTcHaloBytes + 9 * 2 * N * 16;
-    const int segs = a.W / kTcPix;
-    const int gy0 = (blockIdx.x / segs) * kTcRows, gx0 = (blockIdx.x % segs) * kTcPix;
-    const int img = blockIdx.z;
+    const int segs = a.W / kTcPix, rows2 = a.H / kTcRows;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int cols = kTcRows * N;
+    const int nchunks = a.cin / 16;
+    const int cols = NB * kTcRows * N;
     const uint32_t ncols = cols <= 32 ? 32u : (cols <= 64 ? 64u : (cols <= 128 ? 128u : (cols <= 256 ? 256u : 512u)));
-    if (warp == 0) {
+    if (warp == 9) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
                      ::"r"(smem_u32(&tmem_slot)), "r"(ncols) : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (threadIdx.x == 0) {
-        tc_mbar_init(&bar[0]);
-        tc_mbar_init(&bar[1]);
-        s_timeout = 0;
+        for (int q = 0; q < S; q++) { tc_mbar_init_n(&full[q], 1); tc_mbar_init_n(&empty[q], 1); }
+        for (int q = 0; q < NB; q++) { tc_mbar_init_n(&tfull[q], 1); tc_mbar_init_n(&tempty[q], 8); }
+        tc_mbar_init_n(&mdone, 1);
+        s_abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_slot;
-    const uint32_t idesc = umma_idesc_bf16_f32(kTcPix, N);
     const uint32_t base = smem_u32(tc_smem);
-    const int nchunks = a.cin / 16;
-    auto fill = [&](int c, int stg) {
-        const uint32_t sb = base + (uint32_t)(stg * stage_bytes);
-        for (int q = threadIdx.x; q < 2 * kTcHaloRows * kTcHaloW; q += 128) {
-            const int h = q / (kTcHaloRows * kTcHaloW), r = q - h * (kTcHaloRows * kTcHaloW);
-            const int hy = r / kTcHaloW, hx = r - hy * kTcHaloW;
-            const int yy = gy0 + hy - 1, xx = gx0 + hx - 1;
-            const bool in = yy >= 0 && yy < a.H && xx >= 0 && xx < a.W;
-            const bf16 *src = in ? a.x + ((long long)(img * a.H + yy) * a.W + xx) * a.ldx + c * 16 + h * 8 : a.x;
-            cp_async16(sb + (uint32_t)q * 16u, src, in);
-        }
-        const uint32_t wb = sb + kTcHaloBytes;
-        for (int q = threadIdx.x; q < 18 * N; q += 128) {
-            const int tap = q / (2 * N), r = q - tap * 2 * N, h = r / N, n = r - h * N;
-            cp_async16(wb + (uint32_t)q * 16u, a.w + ((long long)n * 9 + tap) * a.cin + c * 16 + h * 8, true);
-        }
-        asm volatile("cp.async.commit_group;" ::: "memory");
+    auto wait = [&](unsigned long long *b, uint32_t parity) {
+        if (s_abort) return false;
+        if (tc_mbar_wait(b, parity)) return true;
+        s_abort = 1;
+        if (a.err) atomicOr(a.err, m2d::ERR_WAIT_TIMEOUT);
+        return false;
     };
-    uint32_t phase[2] = {0u, 0u};
-    bool ok = true;
-    fill(0, 0);
-    for (int c = 0; c < nchunks; c++) {
-        const int st = c & 1;
-        if (c + 1 < nchunks) {
-            if (c >= 1) {     // the MMAs of chunk c - 1 read the stage chunk c + 1 goes to
-                ok = tc_mbar_wait(&bar[st ^ 1], phase[st ^ 1]) && ok;
-                phase[st ^ 1] ^= 1u;
-            }
-            fill(c + 1, st ^ 1);
-            asm volatile("cp.async.wait_group 1;" ::: "memory");
-        } else {
-            asm volatile("cp.async.wait_group 0;" ::: "memory");
-        }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        if (threadIdx.x == 0 && ok) {
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t sa = base + (uint32_t)(st * stage_bytes), sw = sa + kTcHaloBytes;
-#pragma unroll 1
-            for (int tap = 0; tap < 9; tap++) {
-                const int dy = tap / 3, dx = tap - dy * 3;
-                const uint64_t bd = umma_desc(sw + (uint32_t)tap * 2u * (uint32_t)N * 16u, (uint32_t)N * 16u, 128u);
-                const uint32_t acc = (c > 0 || tap > 0) ? 1u : 0u;
-#pragma unroll
-                for (int r = 0; r < kTcRows; r++) {
-                    const uint64_t ad = umma_desc(sa + (uint32_t)((r + dy) * kTcHaloW + dx) * 16u,
-                                                  (uint32_t)(kTcHaloRows * kTcHaloW * 16), 128u);
-                    asm volatile("{\n\t.reg .pred p;\n\t"
-                                 "setp.ne.b32 p, %4, 0;\n\t"
-                                 "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
-                                 ::"r"(tmem + (uint32_t)(r * N)), "l"(ad), "l"(bd), "r"(idesc), "r"(acc) : "memory");
+    auto tile_origin = [&](int t, int &img, int &gy0, int &gx0) {
+        img = t / (rows2 * segs);
+        const int r = t - img * rows2 * segs;
+        gy0 = (r / segs) * kTcRows;
+        gx0 = (r % segs) * kTcPix;
+    };
+
+    if (warp == 8) {
+        // ---- staging (one lane): items (tile, chunk) in order, S in flight
+        if (lane == 0) {
+            const uint32_t item_bytes = (uint32_t)(2 * kTcHalfBytes + 9 * 2 * N * 16);
+            long long it = 0;
+            for (int t = blockIdx.x; t < sh.tiles && !s_abort; t += gridDim.x) {
+                int img, gy0, gx0;
+                tile_origin(t, img, gy0, gx0);
+                for (int c = 0; c < nchunks; c++, it++) {
+                    const int stg = (int)(it % S);
+                    const long long use = it / S;
+                    if (use >= 1 && !wait(&empty[stg], (uint32_t)((use - 1) & 1))) break;
+                    const uint32_t sb = base + (uint32_t)(stg * stage_bytes);
+                    tc_mbar_expect(&full[stg], item_bytes);
+                    tma_load_4d(sb, &xmap, c * 16, gx0 - 1, gy0 - 1, img, &full[stg]);
+                    tma_load_4d(sb + kTcHalfBytes, &xmap, c * 16 + 8, gx0 - 1, gy0 - 1, img, &full[stg]);
+                    bulk_load(sb + kTcHaloBytes, a.wtc + (long long)c * 9 * 2 * N * 8, (uint32_t)(9 * 2 * N * 16),
+                              &full[stg]);
                 }
             }
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-                         ::"r"(smem_u32(&bar[st])) : "memory");
         }
-    }
-    // the last commit covers every MMA of the CTA
-    const int sl = (nchunks - 1) & 1;
-    ok = tc_mbar_wait(&bar[sl], phase[sl]) && ok;
-    if (!ok) {
-        s_timeout = 1;
-        if (a.err) atomicOr(a.err, m2d::ERR_WAIT_TIMEOUT);
-    }
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    __syncthreads();
-    if (!s_timeout) {
-        const int pl = warp * 32 + lane;
-        const uint32_t tlane = tmem + ((uint32_t)(warp * 32) << 16);
-        for (int r = 0; r < kTcRows; r++) {
+        __syncwarp();
+    } else if (warp == 9) {
+        // ---- MMA issue (one lane)
+        if (lane == 0) {
+            const uint32_t idesc = umma_idesc_bf16_f32(kTcPix, N);
+            long long it = 0, tl = 0;
+            for (int t = blockIdx.x; t < sh.tiles && !s_abort; t += gridDim.x, tl++) {
+                const int bsel = (int)(tl % NB);
+                const long long v = tl / NB;
+                if (v >= 1 && !wait(&tempty[bsel], (uint32_t)((v - 1) & 1))) break;
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t acc_base = tmem + (uint32_t)(bsel * kTcRows * N);
+                bool ok = true;
+                for (int c = 0; c < nchunks; c++, it++) {
+                    const int stg = (int)(it % S);
+                    if (!wait(&full[stg], (uint32_t)((it / S) & 1))) { ok = false; break; }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t sa = base + (uint32_t)(stg * stage_bytes), sw = sa + kTcHaloBytes;
+#pragma unroll 1
+                    for (int tap = 0; tap < 9; tap++) {
+                        const int dy = tap / 3, dx = tap - dy * 3;
+                        const uint64_t bd = umma_desc(sw + (uint32_t)tap * 2u * (uint32_t)N * 16u, (uint32_t)N * 16u, 128u);
+                        const uint32_t acc = (c > 0 || tap > 0) ? 1u : 0u;
+#pragma unroll
+                        for (int r = 0; r < kTcRows; r++) {
+                            const uint64_t ad = umma_desc(sa + (uint32_t)((r + dy) * kTcHaloW + dx) * 16u,
+                                                          (uint32_t)kTcHalfBytes, 128u);
+                            asm volatile("{\n\t.reg .pred p;\n\t"
+                                         "setp.ne.b32 p, %4, 0;\n\t"
+                                         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                                         ::"r"(acc_base + (uint32_t)(r * N)), "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+                                         : "memory");
+                        }
+                    }
+                    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                                 ::"r"(smem_u32(&empty[stg])) : "memory");
+                }
+                if (!ok) break;
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                             ::"r"(smem_u32(&tfull[bsel])) : "memory");
+            }
+            // every MMA this thread issued has completed before tensor memory is released
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                         ::"r"(smem_u32(&mdone)) : "memory");
+            if (!tc_mbar_wait(&mdone, 0u) && a.err) atomicOr(a.err, m2d::ERR_WAIT_TIMEOUT);
+        }
+        __syncwarp();
+    } else {
+        // ---- epilogue: warp w reads tensor-memory lanes 32 (w % 4) .. + 31 of row w / 4
+        long long tl = 0;
+        const int q = warp & 3, r = warp >> 2;
+        const int pl = q * 32 + lane;
+        for (int t = blockIdx.x; t < sh.tiles; t += gridDim.x, tl++) {
+            const int bsel = (int)(tl % NB);
+            // warp-uniform: the tensor-memory loads below are warp-collective
+            if (!__all_sync(0xffffffffu, wait(&tfull[bsel], (uint32_t)((tl / NB) & 1)))) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            int img, gy0, gx0;
+            tile_origin(t, img, gy0, gx0);
+            const uint32_t tlane = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(bsel * kTcRows * N + r * N);
             const long long p = (long long)(img * a.H + gy0 + r) * a.W + gx0 + pl;
             for (int cc = 0; cc < N; cc += 16) {
                 uint32_t v[16];
                 asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 "
                              "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-                             : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
-                               "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
-                               "=r"(v[14]), "=r"(v[15])
-                             : "r"(tlane + (uint32_t)(r * N + cc)));
+                             : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+                               "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
+                               "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+                             : "r"(tlane + (uint32_t)cc));
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
                 for (int k = 0; k < 16; k += 2) {
@@ -360,11 +429,14 @@ __global__ void __launch_bounds__(128, 1) k_conv3x3_tc(ConvArgs a)
                     }
                 }
             }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) tc_mbar_arrive(&tempty[bsel]);
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    if (warp == 0)
+    if (warp == 9)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
 }
 
@@ -624,9 +696,11 @@ __global__ void k_adam(long long n, float *p, const float *g, float *m, float *v
         p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
     }
 }
-// bf16 copies of one layer's weights: W [cout][9][cin] and the adjoint
-// kernel WT [cin][9][cout] with the taps reversed
-__global__ void k_sync_weights(int cin, int cout, const float *w, bf16 *wb, bf16 *wt)
+// bf16 copies of one layer's weights: W [cout][9][cin], the adjoint kernel
+// WT [cin][9][cout] with the taps reversed, and both in the tcgen05 kernel's
+// staging order: per 16-channel chunk of the K dimension, [tap][K half][n][8]
+// (one contiguous block of 288 n bytes per chunk, copied with one bulk copy)
+__global__ void k_sync_weights(int cin, int cout, const float *w, bf16 *wb, bf16 *wt, bf16 *wbtc, bf16 *wttc)
 {
     const int n = cout * 9 * cin;
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
@@ -634,6 +708,10 @@ __global__ void k_sync_weights(int cin, int cout, const float *w, bf16 *wb, bf16
         const bf16 v = __float2bfloat16_rn(w[e]);
         wb[e] = v;
         wt[((long long)ci * 9 + (8 - tap)) * cout + co] = v;
+        // forward: K = ci, N = co
+        wbtc[(((long long)(ci >> 4) * 9 + tap) * 2 + ((ci >> 3) & 1)) * cout * 8 + co * 8 + (ci & 7)] = v;
+        // adjoint: K = co, N = ci, tap reversed
+        wttc[(((long long)(co >> 4) * 9 + (8 - tap)) * 2 + ((co >> 3) & 1)) * cin * 8 + ci * 8 + (co & 7)] = v;
     }
 }
 
@@ -650,7 +728,7 @@ inline unsigned grid_for(long long n, int block = 256)
 struct ConvLayer {
     int cin, cout, level;
     long long woff, boff;      // offsets into the FP32 parameter array
-    bf16 *wb = nullptr, *wt = nullptr;
+    bf16 *wb = nullptr, *wt = nullptr, *wbtc = nullptr, *wttc = nullptr;
     // forward views
     const bf16 *x = nullptr; int ldx = 0;
     bf16 *y = nullptr; int ldy = 0;
@@ -697,30 +775,80 @@ T *dalloc(m2d_unet *n, long long count, cudaError_t &e)
 }
 
 // tcgen05 kernel policy (m2d_unet_set_tensor_path): 0 never, 1 where it
-// measured at least as fast as the mma.sync kernel (96 or more input
-// channels: enough 16-channel chunks for its two-stage pipeline to overlap
-// the staging with the MMAs), 2 wherever the shape allows
+// measured faster than the mma.sync kernel (64 or more output channels, or
+// 48 or more input channels; the 16- and 32-channel layers are bound by their
+// epilogue, which the mma.sync kernel's many small CTAs hide better), 2
+// wherever the shape allows
 int g_tensor_tc = 1;
 
-cudaError_t launch_conv(int nimg, int H, int W, const bf16 *x, int ldx, const bf16 *w, int cin, int cout,
-                        const float *bias, float *z, bf16 *y, int ldy, float *yf, int ldyf, int accumulate, int act,
-                        int *err, cudaStream_t st)
+// the 4-D tensor map of an activation view [img][H][W][channels 0..cin) with
+// `ldx` channels per pixel, box [1][4][130][8] (one K half of a halo chunk)
+bool encode_halo_map(CUtensorMap *map, const bf16 *x, int ldx, int cin, int nimg, int H, int W)
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    static bool looked = false;
+    if (!looked) {
+        looked = true;
+        cudaDriverEntryPointQueryResult q;
+        void *fn = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+        (void)cudaGetLastError();
+    }
+    if (!encode || ((uintptr_t)x % 16) != 0 || (ldx * 2) % 16 != 0 || cin % 16 != 0) return false;
+    const cuuint64_t dims[4] = {(cuuint64_t)cin, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)nimg};
+    const cuuint64_t strides[3] = {(cuuint64_t)ldx * 2, (cuuint64_t)W * ldx * 2, (cuuint64_t)H * W * ldx * 2};
+    const cuuint32_t box[4] = {8, (cuuint32_t)kTcHaloW, (cuuint32_t)kTcHaloRows, 1};
+    const cuuint32_t es[4] = {1, 1, 1, 1};
+    return encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16 *>(x), dims, strides, box, es,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+cudaError_t launch_conv(int nimg, int H, int W, const bf16 *x, int ldx, const bf16 *w, const bf16 *wtc, int cin,
+                        int cout, const float *bias, float *z, bf16 *y, int ldy, float *yf, int ldyf, int accumulate,
+                        int act, int *err, cudaStream_t st)
 {
     ConvArgs a;
     a.x = x; a.ldx = ldx; a.w = w; a.bias = bias; a.z = z; a.y = y; a.ldy = ldy; a.yf = yf; a.ldyf = ldyf;
     a.accumulate = accumulate; a.act = act; a.nimg = nimg; a.H = H; a.W = W; a.cin = cin; a.cout = cout;
     a.err = err;
+    a.wtc = wtc;
     const bool tc_shape = W % kTcPix == 0 && H % kTcRows == 0 && cout % 16 == 0 && cout <= kTcMaxN && cin % 16 == 0;
-    if (tc_shape && (g_tensor_tc == 2 || (g_tensor_tc == 1 && cin >= 96))) {
-        static bool attr = false;
-        if (!attr) {
-            cudaError_t e = cudaFuncSetAttribute(k_conv3x3_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 2 * kTcStageMax);
+    CUtensorMap xmap;
+    if (tc_shape && wtc && (g_tensor_tc == 2 || (g_tensor_tc == 1 && (cout >= 64 || cin >= 48))) &&
+        encode_halo_map(&xmap, x, ldx, cin, nimg, H, W)) {
+        static int attr_device = -1;
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return e;
+        if (attr_device != dev) {
+            e = cudaFuncSetAttribute(k_conv3x3_tcp, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcpSmemMax);
             if (e != cudaSuccess) return e;
-            attr = true;
+            attr_device = dev;
         }
-        const int smem = 2 * (kTcHaloBytes + 9 * 2 * cout * 16);
-        k_conv3x3_tc<<<dim3((unsigned)((H / kTcRows) * (W / kTcPix)), 1, nimg), 128, smem, st>>>(a);
+        const int stage = kTcHaloBytes + 9 * 2 * cout * 16;
+        TcpShape sh;
+        sh.nstage = kTcpSmemBudget / stage;
+        if (sh.nstage > 4) sh.nstage = 4;
+        if (sh.nstage < 2) sh.nstage = 2;
+        sh.nbuf = (4 * cout <= 512) ? 2 : 1;
+        sh.tiles = nimg * (H / kTcRows) * (W / kTcPix);
+        const int smem = sh.nstage * stage;
+        const int cols = sh.nbuf * kTcRows * cout;
+        const int ncols = cols <= 32 ? 32 : (cols <= 64 ? 64 : (cols <= 128 ? 128 : (cols <= 256 ? 256 : 512)));
+        // CTAs per SM: shared memory (227 KB per SM, 1 KB reserved per CTA),
+        // tensor-memory columns (512 per SM), at most 2
+        int per_sm = (227 * 1024) / (smem + 2048);
+        if (per_sm > 512 / ncols) per_sm = 512 / ncols;
+        if (per_sm > 2) per_sm = 2;
+        if (per_sm < 1) per_sm = 1;
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        int grid = sms * per_sm;
+        if (grid > sh.tiles) grid = sh.tiles;
+        k_conv3x3_tcp<<<grid, kTcpThreads, smem, st>>>(a, sh, xmap);
         return cudaGetLastError();
     }
     const unsigned tiles = (unsigned)(((H + kTileH - 1) / kTileH) * ((W + kTileW - 1) / kTileW));
@@ -786,6 +914,8 @@ extern "C" int m2d_unet_create(int bmax, int H, int W, int device, m2d_unet **ou
         ConvLayer &c = n->L[k];
         c.wb = dalloc<bf16>(n, (long long)c.cout * 9 * c.cin, e);
         c.wt = dalloc<bf16>(n, (long long)c.cout * 9 * c.cin, e);
+        c.wbtc = dalloc<bf16>(n, (long long)c.cout * 9 * c.cin, e);
+        c.wttc = dalloc<bf16>(n, (long long)c.cout * 9 * c.cin, e);
         c.z = dalloc<float>(n, P[c.level] * c.cout, e);
     }
     // activations: D[l] = [up from level l+1 | skip of level l]
@@ -869,7 +999,8 @@ static cudaError_t sync_weights(m2d_unet *n, cudaStream_t st)
 {
     for (int k = 0; k < kConvs; k++) {
         ConvLayer &c = n->L[k];
-        k_sync_weights<<<grid_for((long long)c.cout * 9 * c.cin), 256, 0, st>>>(c.cin, c.cout, n->params + c.woff, c.wb, c.wt);
+        k_sync_weights<<<grid_for((long long)c.cout * 9 * c.cin), 256, 0, st>>>(c.cin, c.cout, n->params + c.woff, c.wb, c.wt,
+                                                                             c.wbtc, c.wttc);
     }
     return cudaGetLastError();
 }
@@ -911,7 +1042,7 @@ static cudaError_t forward(m2d_unet *n, int nimg, const float *d_in, float *d_ou
         ConvLayer &c = n->L[k];
         const int lh = H >> c.level, lw = W >> c.level;
         if (e == cudaSuccess)
-            e = launch_conv(nimg, lh, lw, c.x, c.ldx, c.wb, c.cin, c.cout, n->params + c.boff, train ? c.z : nullptr,
+            e = launch_conv(nimg, lh, lw, c.x, c.ldx, c.wb, c.wbtc, c.cin, c.cout, n->params + c.boff, train ? c.z : nullptr,
                             c.y, c.ldy, nullptr, 0, 0, 1, n->err, st);
     };
     const int upch[3] = {32, 64, 128}, dch[3] = {48, 96, 192};
@@ -982,7 +1113,7 @@ extern "C" int m2d_unet_loss_grad(m2d_unet *n, int nimg, const float *d_in, cons
         e = cudaGetLastError();
         if (e == cudaSuccess) e = launch_wgrad(nimg, lh, lw, c.x, c.ldx, n->dz, n->grads + c.woff, c.cin, c.cout, st);
         if (e == cudaSuccess && c.dx)
-            e = launch_conv(nimg, lh, lw, n->dz, c.cout, c.wt, c.cout, c.cin, nullptr, nullptr, nullptr, 0, c.dx,
+            e = launch_conv(nimg, lh, lw, n->dz, c.cout, c.wt, c.wttc, c.cout, c.cin, nullptr, nullptr, nullptr, 0, c.dx,
                             c.lddx, 0, 0, n->err, st);
     };
     for (int l = 0; l < 3; l++) {          // decoder, finest level first
