@@ -485,6 +485,7 @@ def run_extras(args, local):
         nits["learned_fp32"].append(r.nit)
         ratio.append(r.r1 / r.r0)
     one.close()
+    out["isolated_system"] = run_isolated(local)
     out["learned"] = {
         "train": {"pairs": pairs.n, "steps": 300, "batch": 8, "seconds": train_s, "loss_first": hist[0],
                   "loss_last50": float(np.mean(hist[-50:]))},
@@ -493,6 +494,75 @@ def run_extras(args, local):
         "p_solve_ms_median": {k: 1e3 * float(np.median(v)) for k, v in res.items()},
         "msi_iterations_mean": {k: float(np.mean(v)) for k, v in nits.items()},
         "tolerance": "p' solve to |r| < 1e-2 |r0| (nitm_p = 20), host clock per solve"}
+    return out
+
+
+def isolated_system9(nx, ny, seed=1, dominance=1.05):
+    """The isolated 9-diagonal system: off-diagonals i.i.d. U[-1, 0], aP =
+    1.05 sum|a_nb|, rhs N(0, 1), a zero-Dirichlet ghost ring (ghost rows aP =
+    1, b = 0; couplings into the ring dropped).  Plane-major, reference order."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    off = [(-1, -1), (0, -1), (1, -1), (-1, 0), (0, 0), (1, 0), (-1, 1), (0, 1), (1, 1)]
+    inner = np.zeros((ny, nx), bool)
+    inner[1:-1, 1:-1] = True
+    a = np.zeros((9, ny, nx))
+    for k, (di, dj) in enumerate(off):
+        if k == 4:
+            continue
+        nb = np.zeros((ny, nx), bool)        # neighbour (i + di, j + dj) is a real cell
+        nb[max(0, -dj):ny - max(0, dj), max(0, -di):nx - max(0, di)] = \
+            inner[max(0, dj):ny - max(0, -dj), max(0, di):nx - max(0, -di)]
+        a[k] = np.where(inner & nb, -rng.uniform(0.0, 1.0, (ny, nx)), 0.0)
+    a[4] = np.where(inner, dominance * np.abs(a).sum(axis=0), 1.0)
+    b = np.where(inner, rng.standard_normal((ny, nx)), 0.0)
+    return a.reshape(-1).copy(), b.reshape(-1).copy()
+
+
+def run_isolated(local, nx=1026, ny=514, tol=1e-12):
+    """MSI on the isolated 1024x512 system to a relative residual of 1e-12:
+    FP64 and FP32 factors and sweeps inside the FP64 iteration on the GPU
+    (device time of the solve launch), and the serial oracle."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    from mach2d_b200._lib import check, lib
+    a, b = isolated_system9(nx, ny)
+    dev = torch.device("cuda", local)
+    L = lib()
+    L.m2d_msi_workspace_doubles.restype = ctypes.c_long
+    L.m2d_msi_workspace_doubles.argtypes = [ctypes.c_int] * 3
+    wsz = L.m2d_msi_workspace_doubles(9, nx, ny)
+    da, db = torch.from_numpy(a).to(dev), torch.from_numpy(b).to(dev)
+    work = torch.empty(wsz, dtype=torch.float64, device=dev)
+    nit = torch.zeros(2, dtype=torch.int32, device=dev)
+    out = {"system": f"9-diagonal {nx - 2}x{ny - 2} (+ghost ring), aP = 1.05 sum|a_nb|, seed 1",
+           "tolerance": tol}
+    for key, fn in (("gpu_fp64", "m2d_msi_solve_device"), ("gpu_fp32_refined", "m2d_msi_solve_device_mixed")):
+        f = getattr(L, fn)
+        f.argtypes = [ctypes.c_int] * 4 + [ctypes.c_double] + [ctypes.c_void_p] * 6
+        times = []
+        for rep in range(3):
+            x = torch.zeros(nx * ny, dtype=torch.float64, device=dev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            check(f(9, nx, ny, 5000, tol, da.data_ptr(), db.data_ptr(), x.data_ptr(), work.data_ptr(), None,
+                    nit.data_ptr()))
+            e1.record()
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+        rr = work[wsz - 4:wsz - 2].cpu().numpy()
+        out[key] = {"ms": min(times), "iterations": int(nit[0].item()),
+                    "relative_residual": float(np.sqrt(rr[1] / rr[0]))}
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from _oracle import call
+    x = np.zeros(nx * ny)
+    t0 = time.perf_counter()
+    its = call("msi9_solve", nx, ny, 5000, tol, a, b, x)
+    out["cpu_oracle_serial"] = {"ms": 1e3 * (time.perf_counter() - t0), "iterations": int(its), "cores": 1}
     return out
 
 
