@@ -9,8 +9,13 @@ reference's interfaces:
   coefficients   the routines of module coefficients and of the internal-flow
                  plug-in (src/equations/mach2d_coef.f90,
                  src/user/internal_flow/mod_intflow.f90)
-  simplec        the device-resident outer iteration (src/mach2d_main.f90)
+  simplec        the device-resident outer iteration (src/mach2d_main.f90),
+                 batches of instances
   ifile          reader for the reference's `value & name & description` decks
+  thermo         the gas-mixture model (src/thermophysical/) and its data files
+  listing        the reference's residual listing and main-results report
+  sweep          sweeps of independent nozzles sharded over GPUs
+  unet           the learned p' correction (no counterpart in the reference)
 """
 from ._lib import LIB_PATH, M2DError, lib  # noqa: F401
 
