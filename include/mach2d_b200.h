@@ -456,10 +456,9 @@ int m2d_unet_loss_grad(m2d_unet *net, int nimg, const float *d_in, const float *
                        const float *d_mask, float scale, float *loss, void *stream);
 /* one Adam step on the master parameters, then their BF16 copies */
 int m2d_unet_adam(m2d_unet *net, float lr, float beta1, float beta2, float eps, void *stream);
-/* which convolutions run on the tcgen05 kernel (images of even height and a
- * width that is a multiple of 128): 0 none (all on the mma.sync kernel), 1
- * those with 64 or more output or 48 or more input channels (default), 2 all
- * that fit */
+/* which convolutions run on the tcgen05 kernel: 0 none (all on the mma.sync
+ * kernel); 1 (default) or 2 every one whose image has an even height and a
+ * width that is a multiple of 128 (the others use the mma.sync kernel) */
 int m2d_unet_set_tensor_path(int mode);
 /* synchronises; *flags = device error word (2: a tensor-core wait ran out,
  * returned as M2D_ERR_TIMEOUT) */

@@ -412,21 +412,37 @@ __global__ void __launch_bounds__(kTcpThreads, 1) k_conv3x3_tcp(ConvArgs a, TcpS
                                "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
                              : "r"(tlane + (uint32_t)cc));
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                // the pixel's 16 channels with 16-byte stores (all offsets are
+                // multiples of 8 elements)
+                float f[16];
 #pragma unroll
-                for (int k = 0; k < 16; k += 2) {
-                    const int co = cc + k;
-                    float v0 = __uint_as_float(v[k]), v1 = __uint_as_float(v[k + 1]);
-                    if (a.bias) { v0 += a.bias[co]; v1 += a.bias[co + 1]; }
-                    if (a.z) *reinterpret_cast<float2 *>(a.z + p * a.cout + co) = make_float2(v0, v1);
-                    if (a.yf) {
-                        float2 *d = reinterpret_cast<float2 *>(a.yf + p * a.ldyf + co);
-                        if (a.accumulate) { const float2 o = *d; v0 += o.x; v1 += o.y; }
-                        *d = make_float2(v0, v1);
+                for (int k = 0; k < 16; k++) f[k] = __uint_as_float(v[k]) + (a.bias ? a.bias[cc + k] : 0.f);
+                if (a.z) {
+                    float4 *d = reinterpret_cast<float4 *>(a.z + p * a.cout + cc);
+#pragma unroll
+                    for (int k = 0; k < 4; k++) d[k] = make_float4(f[4 * k], f[4 * k + 1], f[4 * k + 2], f[4 * k + 3]);
+                }
+                if (a.yf) {
+                    float4 *d = reinterpret_cast<float4 *>(a.yf + p * a.ldyf + cc);
+#pragma unroll
+                    for (int k = 0; k < 4; k++) {
+                        float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
+                        if (a.accumulate) o = d[k];
+                        d[k] = make_float4(f[4 * k] + o.x, f[4 * k + 1] + o.y, f[4 * k + 2] + o.z, f[4 * k + 3] + o.w);
                     }
-                    if (a.y) {
+                }
+                if (a.y) {
+                    uint32_t h[8];
+#pragma unroll
+                    for (int k = 0; k < 8; k++) {
+                        float v0 = f[2 * k], v1 = f[2 * k + 1];
                         if (a.act) { v0 = gelu(v0); v1 = gelu(v1); }
-                        *reinterpret_cast<__nv_bfloat162 *>(a.y + p * a.ldy + co) = __floats2bfloat162_rn(v0, v1);
+                        const __nv_bfloat162 hb = __floats2bfloat162_rn(v0, v1);
+                        h[k] = *reinterpret_cast<const uint32_t *>(&hb);
                     }
+                    uint4 *d = reinterpret_cast<uint4 *>(a.y + p * a.ldy + cc);
+                    d[0] = make_uint4(h[0], h[1], h[2], h[3]);
+                    d[1] = make_uint4(h[4], h[5], h[6], h[7]);
                 }
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -774,11 +790,9 @@ T *dalloc(m2d_unet *n, long long count, cudaError_t &e)
     return (T *)p;
 }
 
-// tcgen05 kernel policy (m2d_unet_set_tensor_path): 0 never, 1 where it
-// measured faster than the mma.sync kernel (64 or more output channels, or
-// 48 or more input channels; the 16- and 32-channel layers are bound by their
-// epilogue, which the mma.sync kernel's many small CTAs hide better), 2
-// wherever the shape allows
+// tcgen05 kernel policy (m2d_unet_set_tensor_path): 0 never (mma.sync for
+// every convolution); 1 (default) and 2: wherever the image shape fits (even
+// height, width a multiple of 128), where it measured faster on every layer
 int g_tensor_tc = 1;
 
 // the 4-D tensor map of an activation view [img][H][W][channels 0..cin) with
@@ -817,7 +831,7 @@ cudaError_t launch_conv(int nimg, int H, int W, const bf16 *x, int ldx, const bf
     a.wtc = wtc;
     const bool tc_shape = W % kTcPix == 0 && H % kTcRows == 0 && cout % 16 == 0 && cout <= kTcMaxN && cin % 16 == 0;
     CUtensorMap xmap;
-    if (tc_shape && wtc && (g_tensor_tc == 2 || (g_tensor_tc == 1 && (cout >= 64 || cin >= 48))) &&
+    if (tc_shape && wtc && g_tensor_tc != 0 &&
         encode_halo_map(&xmap, x, ldx, cin, nimg, H, W)) {
         static int attr_device = -1;
         int dev = 0;

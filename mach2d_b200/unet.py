@@ -55,9 +55,9 @@ def _bind():
 
 
 def set_tensor_path(mode):
-    """Which convolutions run on the tcgen05 kernel: 0 none (mma.sync), 1 those
-    with 64 or more output or 48 or more input channels (the default), 2 every
-    one whose image shape allows it (even height, width a multiple of 128)."""
+    """Which convolutions run on the tcgen05 kernel: 0 none (mma.sync); 1 (the
+    default) or 2 every one whose image shape allows it (even height, width a
+    multiple of 128)."""
     check(_bind().m2d_unet_set_tensor_path(int(mode)))
 
 
