@@ -146,6 +146,20 @@ int m2d_norm_l1_9d(const int *nx, const int *ny, const double *var, const double
 int m2d_norm_l1_9d_relative(const int *nx, const int *ny, const double *var,
                             const double *b, const double *a, double *norm);
 
+/* ---- grid metrics: src/grid/mod_grid.f90 --------------------------------
+ * Same arguments as the reference subroutines (Fortran by-reference scalars,
+ * arrays of nx*ny doubles in host memory).  Every element of every output is
+ * written, as the reference zero- (or one-) fills its outputs first; the
+ * results are bitwise those of the reference's loops.  nx, ny >= 4. */
+int m2d_get_real_centroids_xy(const int *opt, const int *nx, const int *ny, const double *x,
+    const double *y, double *xp, double *yp);                                     /* :237-300 */
+int m2d_get_metrics(const int *nx, const int *ny, const double *x, const double *y,
+    const double *xp, const double *yp, double *xe, double *ye, double *xen, double *yen,
+    double *xk, double *yk, double *xke, double *yke, double *Jp, double *Je, double *Jn,
+    double *alphae, double *gamman, double *betae, double *betan);               /* :304-558 */
+int m2d_get_radius(const int *coord, const int *nx, const int *ny, const double *y,
+    const double *yp, double *radius, double *re, double *rn, double *rp);        /* :562-723 */
+
 /* ---- coefficient assembly and corrections: src/equations/mach2d_coef.f90 */
 int m2d_get_density_at_nodes(const int *nx, const int *ny, const double *Rg, const double *p,
                              const double *T, double *ro);                          /* :6-17 */
@@ -409,8 +423,10 @@ int m2d_ctx_field_device(m2d_ctx *ctx, const char *name, double **dptr, long *n)
 
 /* ---- batches of instances (no counterpart in the reference) ------------
  * n independent nozzle instances on one GPU, each a full context with its
- * own stream.  m2d_batch_iterate runs `iters` outer iterations of every
- * instance with `workers` host threads (<= 0: min(n, 16)), so that several
+ * own stream.  m2d_batch_create sets the instances up with `workers` host
+ * threads (<= 0: min(n, 16)); if one fails, none is kept and the call
+ * returns that failure.  m2d_batch_iterate runs `iters` outer iterations of
+ * every instance with the same threads, so that several
  * instances have kernels in flight at once; reps[k] (may be NULL) receives
  * instance k's last report.  An instance whose iteration fails stops there
  * (m2d_batch_status); the call returns the first failure.  Each instance's

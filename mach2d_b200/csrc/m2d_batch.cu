@@ -32,15 +32,28 @@ extern "C" int m2d_batch_create(const m2d_case *cases, int n, int device, int wo
     if (b->workers > n) b->workers = n;
     b->ctx.assign(n, nullptr);
     b->status.assign(n, M2D_OK);
+    // the instances are set up by the worker threads (the host part of each
+    // set-up, grid nodes and quasi-1D strips, runs in parallel; each device
+    // part runs on its instance's own stream)
+    std::vector<int> rc(n, M2D_OK);
+    std::vector<std::string> msg(n);
+    auto work = [&](int w) {
+        for (int k = w; k < n; k += b->workers) {
+            rc[k] = m2d_create(&cases[k], device, &b->ctx[k]);
+            if (rc[k] != M2D_OK) msg[k] = m2d_last_error();
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int w = 1; w < b->workers; w++) pool.emplace_back(work, w);
+    work(0);
+    for (auto &t : pool) t.join();
     for (int k = 0; k < n; k++) {
-        const int rc = m2d_create(&cases[k], device, &b->ctx[k]);
-        if (rc != M2D_OK) {
-            const std::string msg = std::string("m2d_batch_create: instance ") + std::to_string(k) + ": " +
-                                    m2d_last_error();
-            for (int q = 0; q < k; q++) m2d_destroy(b->ctx[q]);
+        if (rc[k] != M2D_OK) {
+            const std::string m = std::string("m2d_batch_create: instance ") + std::to_string(k) + ": " + msg[k];
+            for (m2d_ctx *c : b->ctx) if (c) m2d_destroy(c);
             delete b;
-            m2d_set_last_error_msg(msg.c_str());
-            return rc;
+            m2d_set_last_error_msg(m.c_str());
+            return rc[k];
         }
     }
     *out = b;

@@ -10,6 +10,7 @@
 #include <string>
 #include <vector>
 #include "m2d_fields.cuh"
+#include "m2d_grid.cuh"
 #include "m2d_solvers.cuh"
 #include "m2d_blomax.cuh"
 #include "m2d_thermo.cuh"
@@ -67,6 +68,14 @@ struct Stage {
     double *inout(double *h, size_t n)
     {
         double *d = in(h, n);
+        if (d) outs.push_back({d, h, n});
+        return d;
+    }
+    // an output the routine writes in full: no copy in
+    double *out(double *h, size_t n)
+    {
+        if (!h) { status = status ? status : ST_ARG; g_last_error = "null array argument"; return nullptr; }
+        double *d = alloc(n);
         if (d) outs.push_back({d, h, n});
         return d;
     }
@@ -810,6 +819,47 @@ int m2d_mixture_eval(const m2d_mixture *mix, double T, double *cp, double *mu, d
     if (kp) *kp = m2d::mix_kp(*mix, T);
     if (gm) *gm = m2d::mix_gm(*mix, T);
     return ST_OK;
+}
+
+// ---- grid metrics (src/grid/mod_grid.f90:237-723) ----
+int m2d_get_real_centroids_xy(const int *opt, const int *nx, const int *ny, const double *x,
+    const double *y, double *xp, double *yp)
+{
+    CHK;
+    if (!opt) return fail(ST_ARG, "get_real_centroids_xy: null opt");
+    Stage s; size_t N = ND_;
+    const double *dx = s.in(x, N), *dy = s.in(y, N);
+    double *dxp = s.out(xp, N), *dyp = s.out(yp, N);
+    if (s.status) return s.status;
+    return s.finish(launch_centroids(*opt, *nx, *ny, dx, dy, dxp, dyp, 0));
+}
+
+int m2d_get_metrics(const int *nx, const int *ny, const double *x, const double *y,
+    const double *xp, const double *yp, double *xe, double *ye, double *xen, double *yen,
+    double *xk, double *yk, double *xke, double *yke, double *Jp, double *Je, double *Jn,
+    double *alphae, double *gamman, double *betae, double *betan)
+{
+    CHK; Stage s; size_t N = ND_;
+    const double *dx = s.in(x, N), *dy = s.in(y, N), *dxp = s.in(xp, N), *dyp = s.in(yp, N);
+    Metrics m;
+    double **dm[] = {&m.xe, &m.ye, &m.xen, &m.yen, &m.xk, &m.yk, &m.xke, &m.yke, &m.Jp, &m.Je, &m.Jn,
+                     &m.alphae, &m.gamman, &m.betae, &m.betan};
+    double *hm[] = {xe, ye, xen, yen, xk, yk, xke, yke, Jp, Je, Jn, alphae, gamman, betae, betan};
+    for (int k = 0; k < 15; k++) *dm[k] = s.out(hm[k], N);
+    if (s.status) return s.status;
+    return s.finish(launch_metrics(*nx, *ny, dx, dy, dxp, dyp, m, 0));
+}
+
+int m2d_get_radius(const int *coord, const int *nx, const int *ny, const double *y,
+    const double *yp, double *radius, double *re, double *rn, double *rp)
+{
+    CHK;
+    if (!coord) return fail(ST_ARG, "get_radius: null coord");
+    Stage s; size_t N = ND_;
+    const double *dy = s.in(y, N), *dyp = s.in(yp, N);
+    double *dr = s.out(radius, N), *de = s.out(re, N), *dn = s.out(rn, N), *dp = s.out(rp, N);
+    if (s.status) return s.status;
+    return s.finish(launch_radius(*coord, *nx, *ny, dy, dyp, dr, de, dn, dp, 0));
 }
 
 int m2d_get_boundary_fields(const int *nx, const int *ny, const double *F, double *Fbn, double *Fbs,

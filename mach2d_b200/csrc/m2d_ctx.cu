@@ -9,6 +9,7 @@
 #include <cstring>
 #include <string>
 #include "m2d_fields.cuh"
+#include "m2d_grid.cuh"
 #include "m2d_setup.h"
 #include "m2d_solvers.cuh"
 #include "m2d_thermo.cuh"
@@ -125,6 +126,75 @@ static cudaError_t mixture_properties(m2d_ctx *x, bool boundary)
     return e;
 }
 
+// The instance set-up on the device (src/mach2d_main.f90:25-84): from the
+// grid nodes and the strips the host computed (m2d_setup.cpp), the centroids,
+// metrics and radii (mod_grid.f90:237-723), ap(:,3) = 1
+// (src/mod_mach2d_data.f90:403), the boundary-face flags and the internal-flow
+// initial guess (mod_intflow.f90:1240-1488) in the reference's order; the
+// inlet strips, which call pow, come back to the host once.  Then the
+// constant or MIXTURE properties and, with dtmodel = 1, the first time step
+// (tstepper_dt0_scarborough).  Only the nodes (2 N doubles) and O(nx + ny)
+// strips cross PCIe.
+static cudaError_t device_setup(m2d_ctx *x, const m2d_case &c, HostInstance &h)
+{
+    Fields &f = x->f;
+    const int nx = x->nx, ny = x->ny;
+    const size_t N = x->N;
+    cudaStream_t st = x->st;
+    cudaError_t e = cudaSuccess;
+    auto up = [&](double *d, const std::vector<double> &v) {
+        if (e == cudaSuccess) e = cudaMemcpyAsync(d, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice, st);
+    };
+    auto run = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
+    up(f.x, h.x);
+    up(f.y, h.y);
+    up(x->P, h.col);                  // 4 nx <= N doubles of TDMA scratch, cleared below
+    run(launch_fill(f.ap + 2 * N, (long long)N, 1.0, st));
+    run(launch_centroids(c.kcm, nx, ny, f.x, f.y, f.xp, f.yp, st));
+    const Metrics m = {f.xe, f.ye, f.xen, f.yen, f.xk, f.yk, f.xke, f.yke, f.Jp, f.Je, f.Jn,
+                       f.alphae, f.gamman, f.betae, f.betan};
+    run(launch_metrics(nx, ny, f.x, f.y, f.xp, f.yp, m, st));
+    run(launch_radius(c.coord, nx, ny, f.y, f.yp, f.radius, f.re, f.rn, f.rp, st));
+    run(launch_boundary_faces_flags(f, st));
+    run(launch_initial_columns(f, x->P, st));
+    run(launch_extrapolate_uv(f, c.modvis, st));
+    run(launch_initial_inlet_u(f, st));
+    std::vector<double> uin((size_t)ny, 0.0);
+    run(cudaMemcpyAsync(uin.data(), f.uin, (size_t)ny * sizeof(double), cudaMemcpyDeviceToHost, st));
+    run(cudaStreamSynchronize(st));
+    if (e != cudaSuccess) return e;
+    inlet_strips(c, h, uin);
+    up(f.vin, h.vin); up(f.pin, h.pin); up(f.Tin, h.Tin); up(f.Mw, h.Mw);
+    up(f.Tbe, h.Tbe); up(f.Tbw, h.Tbw); up(f.Tbn, h.Tbn); up(f.Tbs, h.Tbs);
+    run(launch_initial_pT_ghosts(f, st));
+    run(launch_velocities_at_boundary_faces(f, c.modvis, st));
+    run(launch_density_at_nodes(f, h.Rg, st));
+    run(launch_density_at_faces(f, c.beta, st));
+    // get_cp_mu_kappa_initialization (mod_thermophysical.f90:560-589): constant
+    // properties, or the MIXTURE model from the initial T and Tbn..Tbw
+    run(cudaMemcpyAsync(x->dmix, &c.mix, sizeof(m2d_mixture), cudaMemcpyHostToDevice, st));
+    if (c.ktm != 1) {
+        run(launch_fill(f.cp, (long long)N, h.Cpref, st));
+        if (c.modvis == 1) {
+            for (double *d : {f.vlp, f.vle, f.vln}) run(launch_fill(d, (long long)N, c.mu, st));
+            for (double *d : {f.kp, f.ke, f.kn}) run(launch_fill(d, (long long)N, c.kappa, st));
+        }
+    } else if (e == cudaSuccess) {
+        e = mixture_properties(x, false);
+    }
+    if (c.dtmodel == 1) {
+        RedArgs r;
+        memset(&r, 0, sizeof r);
+        r.kind = RED_DT0; r.nx = nx; r.ny = ny;
+        r.u = f.u; r.v = f.v; r.Jp = f.Jp;
+        run(launch_reduce(r, x->part, x->P, st));
+        run(cudaMemcpyAsync(&h.dt0, x->P, sizeof(double), cudaMemcpyDeviceToHost, st));
+    }
+    run(cudaMemsetAsync(x->P, 0, N * sizeof(double), st));
+    run(cudaStreamSynchronize(st));
+    return e;
+}
+
 extern "C" int m2d_create(const m2d_case *c, int device, m2d_ctx **out)
 {
     if (!c || !out) return ctx_fail(M2D_ERR_ARG, "m2d_create: null argument");
@@ -148,7 +218,9 @@ extern "C" int m2d_create(const m2d_case *c, int device, m2d_ctx **out)
     e = cudaStreamCreateWithFlags(&x->st, cudaStreamNonBlocking);
     if (e != cudaSuccess) { delete x; m2d_set_last_error(e, "cudaStreamCreate", __FILE__, __LINE__); return M2D_ERR_CUDA; }
     // one arena: planes + 9N x 3 + 5N + strips + solver scratch + reductions
-    const size_t nplanes = h.planes().size();
+#define M2D_COUNT(nm) +1
+    const size_t nplanes = 0 M2D_PLANES(M2D_COUNT);
+#undef M2D_COUNT
     const size_t strips = (size_t)9 * h.ny + 2 * (size_t)h.nx + 64;
     const size_t solver = 2 * msi_work_doubles(9, h.nx, h.ny) + msi_work_doubles(5, h.nx, h.ny) + 4 + 2 * N + 3 * 32;
     const size_t mixd = (sizeof(m2d_mixture) + sizeof(double) - 1) / sizeof(double);
@@ -181,28 +253,8 @@ extern "C" int m2d_create(const m2d_case *c, int device, m2d_ctx **out)
     e = cudaMallocHost(&x->hsc, S_COUNT * sizeof(double));
     if (e == cudaSuccess) e = cudaMallocHost(&x->hint, I_COUNT * sizeof(int));
     if (e != cudaSuccess) { m2d_destroy(x); m2d_set_last_error(e, "cudaMallocHost", __FILE__, __LINE__); return M2D_ERR_NOMEM; }
-    // ap(:,3) = 1 (src/mod_mach2d_data.f90:403)
-    {
-        std::vector<double> ap(5 * N, 0.0);
-        std::fill(ap.begin() + 2 * N, ap.begin() + 3 * N, 1.0);
-        e = cudaMemcpyAsync(f.ap, ap.data(), 5 * N * sizeof(double), cudaMemcpyHostToDevice, x->st);
-        for (auto &kv : h.planes()) {
-            long n; double *d = plane_ptr(x, kv.first, &n);
-            if (e == cudaSuccess) e = cudaMemcpyAsync(d, kv.second->data(), N * sizeof(double), cudaMemcpyHostToDevice, x->st);
-        }
-        const struct { double *d; std::vector<double> *v; } sv[] = {
-            {f.uin, &h.uin}, {f.vin, &h.vin}, {f.pin, &h.pin}, {f.Tin, &h.Tin}, {f.Mw, &h.Mw},
-            {f.plin, &h.plin}, {f.pina, &h.pina}, {f.Tbe, &h.Tbe}, {f.Tbw, &h.Tbw}, {f.Tbn, &h.Tbn},
-            {f.Tbs, &h.Tbs}};
-        for (auto &s : sv)
-            if (e == cudaSuccess) e = cudaMemcpyAsync(s.d, s.v->data(), s.v->size() * sizeof(double), cudaMemcpyHostToDevice, x->st);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(x->dmix, &c->mix, sizeof(m2d_mixture), cudaMemcpyHostToDevice, x->st);
-        // get_cp_mu_kappa_initialization for the MIXTURE model
-        // (mod_thermophysical.f90:560-589), from the initial T and Tbn..Tbw
-        if (e == cudaSuccess && c->ktm == 1) e = mixture_properties(x, false);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(x->st);
-        if (e != cudaSuccess) { m2d_destroy(x); m2d_set_last_error(e, "upload", __FILE__, __LINE__); return M2D_ERR_CUDA; }
-    }
+    e = device_setup(x, *c, h);
+    if (e != cudaSuccess) { m2d_destroy(x); m2d_set_last_error(e, "set-up", __FILE__, __LINE__); return M2D_ERR_CUDA; }
     Params &q = x->q;
     memset(&q, 0, sizeof q);
     q.modvis = c->modvis; q.coord = c->coord; q.beta = c->beta; q.Rg = h.Rg; q.gamma = h.gamma;

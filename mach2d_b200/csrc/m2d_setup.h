@@ -1,4 +1,5 @@
-// m2d_setup.h -- host-side instance set-up (grid, metrics, initial guess).
+// m2d_setup.h -- host-side part of the instance set-up (grid nodes and the
+// strips of the initial guess).
 #pragma once
 #include <utility>
 #include <vector>
@@ -17,33 +18,26 @@ namespace m2d {
     X(sup) X(cvp) X(svp) X(bu) X(bv) X(bt) X(bp) X(pl) X(due) X(dve) X(dun)    \
     X(dvn) X(de) X(dn)
 
+// what the host computes of one instance: the grid nodes and the strips of
+// the initial guess; everything else is computed on the device
 struct HostInstance {
     int nx = 0, ny = 0;
-#define M2D_DECL_VEC(name) std::vector<double> name;
-    M2D_PLANES(M2D_DECL_VEC)
-#undef M2D_DECL_VEC
-    std::vector<double> uin, vin, pin, Tin, Mw, plin, pina;   // ny
+    std::vector<double> x, y;                                 // N: grid nodes
+    std::vector<double> M1D, p1D, T1D, u1D;                   // nx: quasi-1D isentropic flow
+    std::vector<double> ue1D;                                 // nx: isentropic east-face u of column i
+    std::vector<double> col;                                  // 4 nx: p1D, T1D, u1D, ue1D of the columns
+    std::vector<double> uin, vin, pin, Tin, Mw;               // ny: inlet strips
     std::vector<double> Tbe, Tbw, Tbn, Tbs;                   // ny, ny, nx, nx
-    std::vector<double> M1D, p1D, T1D, u1D;                   // nx
     double Sg = 0, fm1D = 0, Fd1D = 0, Fpv1D = 0, Rg = 0, gamma = 0, Cpref = 0, Href = 0, dt0 = 0;
-
-    std::vector<std::pair<const char *, std::vector<double> *>> planes()
-    {
-        std::vector<std::pair<const char *, std::vector<double> *>> lst_;
-#define M2D_LIST_VEC(name) lst_.push_back({#name, &this->name});
-        M2D_PLANES(M2D_LIST_VEC)
-#undef M2D_LIST_VEC
-        return lst_;
-    }
 };
 
-// builds the grid, metrics and initial fields; returns 0 or an M2D_ERR_* code
+// the grid nodes, reference values and the column strips; returns 0 or an
+// M2D_ERR_* code
 int build_instance(const m2d_case &c, HostInstance &h);
+// the inlet strips (get_uin_vin_pin_Tin_Mw, mod_intflow.f90:968-1000) from
+// uin(j) = (u(1,j) + u(2,j)) / 2 of the extrapolated initial field, and Tbw
+void inlet_strips(const m2d_case &c, HostInstance &h, const std::vector<double> &uin);
 double mach_area(int kf, double ar, double gamma);
 double ramp_dt(int it, const m2d_case &c);
-void north_slip_host(int nx, int ny, const std::vector<double> &x, const std::vector<double> &xp,
-                     const std::vector<double> &xk, const std::vector<double> &yk,
-                     const std::vector<double> &u, const std::vector<double> &v,
-                     std::vector<double> &ubn, std::vector<double> &vbn);
 
 }  // namespace m2d

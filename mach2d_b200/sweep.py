@@ -38,16 +38,25 @@ def gather_results(local, n, group=None):
     return [merged[i] for i in range(n)]
 
 
-def run_shard(cases, indices, device, iters, graph=True):
+def run_shard(cases, indices, device, iters, graph=True, timings=None):
     """Advances the cases at `indices` as one batch on `device`: `iters` outer
     iterations each (or, with iters <= 0, each to its stopping iteration, at
-    most 100000).  Returns ({index: (it, normpl, fmi, fme, Fd, Cd)}, seconds)."""
+    most 100000).  Returns ({index: (it, normpl, fmi, fme, Fd, Cd)}, seconds).
+    With a dict `timings`, also records the batch set-up time in
+    timings["setup_s"] (grids, metrics and initial fields of every instance)."""
     import torch
 
     from .simplec import Batch
     if not indices:
+        if timings is not None:
+            timings["setup_s"] = 0.0
         return {}, 0.0
+    torch.cuda.synchronize(device)
+    t_setup = time.perf_counter()
     b = Batch([cases[i] for i in indices], device=device)
+    torch.cuda.synchronize(device)
+    if timings is not None:
+        timings["setup_s"] = time.perf_counter() - t_setup
     if graph:
         for s in b.instances:
             s.set_graph(True)

@@ -373,6 +373,8 @@ long orc_field(orc_state *s, const char *name, double **ptr)
     if (!strcmp(name, "Tin")) { *ptr = s->Tin; return s->ny; }
     if (!strcmp(name, "uin")) { *ptr = s->uin; return s->ny; }
     if (!strcmp(name, "Mw")) { *ptr = s->Mw; return s->ny; }
+    if (!strcmp(name, "vin")) { *ptr = s->vin; return s->ny; }
+    if (!strcmp(name, "pina")) { *ptr = s->pina; return s->ny; }
     if (!strcmp(name, "p1D")) { *ptr = s->p1D; return s->nx; }
     if (!strcmp(name, "M1D")) { *ptr = s->M1D; return s->nx; }
     return -1;

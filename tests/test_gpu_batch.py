@@ -3,7 +3,8 @@
 Each instance is a full context on its own stream, so the batch must give
 every instance exactly the results it gets when run alone (same kernels, same
 order of operations), whatever the number of host workers; and a failing
-instance must stop alone without disturbing the others.
+instance must stop alone without disturbing the others.  The instances are
+set up by the same worker threads; a set-up failure fails the whole batch.
 """
 import numpy as np
 import pytest
@@ -65,4 +66,17 @@ def test_batch_failure_stays_in_its_instance():
         reps = b.iterate(2)                             # instance 2 stays stopped, others go on
     assert reps is None
     assert b.instances[0].scalar("it") == 6 and b.instances[1].scalar("it") == 6
+    b.close()
+
+
+def test_batch_set_up_failure_names_the_instance_and_keeps_none():
+    # the instances are set up by the worker threads; one that cannot be
+    # set up (fewer than 3 real volumes) fails the whole batch
+    cases = _cases()
+    cases[3].nxr = 2
+    with pytest.raises(M2DError) as e:
+        Batch(cases, workers=3)
+    assert e.value.code == 2 and "instance 3" in str(e.value)
+    b = Batch(_cases()[:2], workers=2)                  # the device is still usable
+    assert b.iterate(1)[1].it == 1
     b.close()
