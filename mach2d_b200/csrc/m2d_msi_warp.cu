@@ -62,9 +62,9 @@ constexpr long long kBarSpinLimit = 1LL << 22;
 
 // a / b from y = RN(1/b): q0 = a y, then two corrections q += (a - q b) y
 // with exact FMA remainders (Markstein, IBM J. Res. Dev. 34, 1990).  With
-// |a|, |b| in [2^-500, 2^500] no intermediate leaves the normal range and the
+// |a|, |b| in [2^-500, 2^500) no intermediate leaves the normal range and the
 // result is the correctly rounded quotient; for a = 0 the first product a y
-// already is the IEEE quotient.  range_ok tells when these conditions hold.
+// already is the IEEE quotient.  range_bad is 0 when these conditions hold.
 __device__ __forceinline__ double div_recip(double a, double b, double y)
 {
     const double q0 = a * y;
@@ -73,15 +73,23 @@ __device__ __forceinline__ double div_recip(double a, double b, double y)
     const double r1 = fma(-q1, b, a);
     return (a == 0.0) ? q0 : fma(r1, y, q1);
 }
-__device__ __forceinline__ bool range_ok(double a, double b)
+// 1 when |x| lies outside [2^-500, 2^500) (zero, subnormals, Inf and NaN
+// included): the biased exponent outside [523, 1522].  Integer arithmetic
+// without branches, so the check does not split a recurrence step into
+// blocks the scheduler cannot overlap.
+__device__ __forceinline__ unsigned exp_out(double x)
 {
-    const double fa = fabs(a), fb = fabs(b);
-    return fb >= 0x1p-500 && fb <= 0x1p+500 && (fa == 0.0 || (fa >= 0x1p-500 && fa <= 0x1p+500));
+    const unsigned e = (unsigned)((unsigned long long)__double_as_longlong(x) >> 52) & 0x7ffu;
+    return (e - 523u) > 999u ? 1u : 0u;
+}
+__device__ __forceinline__ unsigned range_bad(double a, double b)
+{
+    return exp_out(b) | (exp_out(a) & (a != 0.0 ? 1u : 0u));
 }
 // n / d on the fast path: the IEEE quotient unless bad is raised
-__device__ __forceinline__ double div_fast(double n, double d, bool &bad)
+__device__ __forceinline__ double div_fast(double n, double d, unsigned &bad)
 {
-    bad = bad || !range_ok(n, d);
+    bad |= range_bad(n, d);
     return div_recip(n, d, __drcp_rn(d));
 }
 
@@ -382,7 +390,7 @@ __device__ double cluster_residual(cg::cluster_group &cl, const double *__restri
 template <int ND, bool FAST>
 __device__ __forceinline__ void lu_cell(const double (&cb)[ND], double alpha, const double *mw,
                                         const double *a1, const double *a2, const double *a3, double *l,
-                                        double *u, double &y1, bool &bad)
+                                        double *u, double &y1, unsigned &bad)
 {
     auto dv = [&](double n, double d) -> double { return FAST ? div_fast(n, d, bad) : n / d; };
     if (ND == 9) {
@@ -401,7 +409,7 @@ __device__ __forceinline__ void lu_cell(const double (&cb)[ND], double alpha, co
         if (FAST) {
             const double y = __drcp_rn(l1);
             y1 = y;
-            bad = bad || !range_ok(n0, l1) || !range_ok(n1, l1) || !range_ok(n2, l1) || !range_ok(b9, l1);
+            bad |= range_bad(n0, l1) | range_bad(n1, l1) | range_bad(n2, l1) | range_bad(b9, l1);
             u[0] = div_recip(n0, l1, y); u[1] = div_recip(n1, l1, y);
             u[2] = div_recip(n2, l1, y); u[3] = div_recip(b9, l1, y);
         } else {
@@ -422,7 +430,7 @@ __device__ __forceinline__ void lu_cell(const double (&cb)[ND], double alpha, co
         if (FAST) {
             const double y = __drcp_rn(l1);
             y1 = y;
-            bad = bad || !range_ok(n0, l1) || !range_ok(n1, l1) || !range_ok(n2, l1);
+            bad |= range_bad(n0, l1) | range_bad(n1, l1) | range_bad(n2, l1);
             u[0] = div_recip(n0, l1, y); u[1] = div_recip(n1, l1, y); u[2] = div_recip(n2, l1, y);
         } else {
             u[0] = n0 / l1; u[1] = n1 / l1; u[2] = n2 / l1;
@@ -633,14 +641,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                 }
             }
             const unsigned rbase = (unsigned)up_base * kLag;
-            bool bad = false;
+            unsigned bad = 0;
 #pragma unroll
             for (int pass = 0; pass < (EXACT ? 2 : 1); pass++) {
                 // pass 0: fast divisions; pass 1 (only if some cell of pass 0
                 // may differ from IEEE division): the batch again from its
                 // start state with IEEE division
                 if (pass == 1) {
-                    if (!__any_sync(kFull, bad)) break;
+                    if (!__any_sync(kFull, bad != 0u)) break;
 #pragma unroll
                     for (int q = 0; q < NU; q++) {
                         mw[q] = lu_save[fw][q][lane]; a1[q] = lu_save[fw][NU + q][lane];
@@ -672,11 +680,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                     TS l[NL], u[NU], y;
                     if constexpr (EXACT) {
                         if (pass == 0) {
-                            bool bc = false;
+                            unsigned bc = 0;
                             lu_cell<ND, true>(cb, alpha, mw, a1, a2, a3, l, u, y, bc);
-                            bad = bad || (valid && bc);
+                            bad |= valid ? bc : 0u;
                         } else {
-                            bool unused = false;
+                            unsigned unused = 0;
                             lu_cell<ND, false>(cb, alpha, mw, a1, a2, a3, l, u, y, unused);
                         }
                     } else {
@@ -741,14 +749,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                 if (b + NSTAGE - 1 < nbatch) stage_issue<NL + 2>(st, fp, line0, (b + NSTAGE - 1) * kLag - soff, SW);
                 const TS m0 = mine, b1 = a1, b2 = a2, b3 = a3;   // state at batch start
                 const unsigned rbase = (unsigned)up_base * kLag;   // ring position of step 0
-                bool bad = false;
+                unsigned bad = 0;
                 TS ob[kLag];   // results of the batch, stored after its last step
 #pragma unroll
                 for (int pass = 0; pass < (EXACT ? 2 : 1); pass++) {
                     if (pass == 1) {
                         // some quotient of pass 0 may differ from IEEE division:
                         // the batch again from its start state with IEEE division
-                        if (!__any_sync(kFull, bad)) break;
+                        if (!__any_sync(kFull, bad != 0u)) break;
                         mine = m0; a1 = b1; a2 = b2; a3 = b3;
                     }
                     // c: staged coefficients of the current step, rv: ring value
@@ -782,7 +790,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                             else num = c[0] + c[2] * mine + c[3] * a1 + c[4] * a2;
                             if (pass == 0) {
                                 wv = -div_recip(num, c[1], c[NL + 1]);
-                                bad = bad || (valid && !range_ok(num, c[1]));
+                                bad |= valid ? range_bad(num, c[1]) : 0u;
                             } else {
                                 wv = -(num / c[1]);
                             }
