@@ -158,6 +158,41 @@ __device__ __forceinline__ double shfl_up_v(double x)
                  "mov.b64 %0, {lo, hi};\n\t}" : "=d"(v) : "d"(x));
     return v;
 }
+// Predicated stores: no branch, so a store of one recurrence step can sit in
+// the same block as the next step's first instructions and overlap them.
+__device__ __forceinline__ void stg_if(double *p, double v, bool c)
+{
+    asm volatile("{\n\t.reg .pred q;\n\t.reg .u64 g;\n\tsetp.ne.u32 q, %2, 0;\n\t"
+                 "cvta.to.global.u64 g, %0;\n\t@q st.global.f64 [g], %1;\n\t}"
+                 ::"l"(p), "d"(v), "r"((unsigned)c));
+}
+__device__ __forceinline__ void stg_if(float *p, float v, bool c)
+{
+    asm volatile("{\n\t.reg .pred q;\n\t.reg .u64 g;\n\tsetp.ne.u32 q, %2, 0;\n\t"
+                 "cvta.to.global.u64 g, %0;\n\t@q st.global.f32 [g], %1;\n\t}"
+                 ::"l"(p), "f"(v), "r"((unsigned)c));
+}
+__device__ __forceinline__ void sts_if(unsigned addr, double v, bool c)
+{
+    asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %2, 0;\n\t@q st.shared.f64 [%0], %1;\n\t}"
+                 ::"r"(addr), "d"(v), "r"((unsigned)c));
+}
+__device__ __forceinline__ void sts_if(unsigned addr, float v, bool c)
+{
+    asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %2, 0;\n\t@q st.shared.f32 [%0], %1;\n\t}"
+                 ::"r"(addr), "f"(v), "r"((unsigned)c));
+}
+// 1 for a zero or non-finite pivot, from the bits (no branch)
+__device__ __forceinline__ unsigned pivot_bad(double x)
+{
+    const unsigned long long b = (unsigned long long)__double_as_longlong(x);
+    return ((b << 1) == 0ull || ((unsigned)(b >> 52) & 0x7ffu) == 0x7ffu) ? 1u : 0u;
+}
+__device__ __forceinline__ unsigned pivot_bad(float x)
+{
+    const unsigned b = (unsigned)__float_as_int(x);
+    return ((b << 1) == 0u || ((b >> 23) & 0xffu) == 0xffu) ? 1u : 0u;
+}
 __device__ __forceinline__ float shfl_up_v(float x)
 {
     float v;
@@ -625,6 +660,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
         TS mw[NU], a1[NU], a2[NU], a3[NU];
 #pragma unroll
         for (int q = 0; q < NU; q++) { mw[q] = 0; a1[q] = 0; a2[q] = 0; a3[q] = 0; }
+        unsigned piv = 0;                              // a zero or non-finite pivot was seen
+        const unsigned oup = smem_u32(&out_up[fw][0]);
         for (int b = 0; b < nbatch; b++) {
             const int tb = b * kLag;
             const int n = up_base + b;                          // global batch number on the channel
@@ -655,25 +692,60 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                         a2[q] = lu_save[fw][2 * NU + q][lane]; a3[q] = lu_save[fw][3 * NU + q][lane];
                     }
                 }
+                // Software-pipelined steps.  A step first issues its critical
+                // inputs (the shuffles of the previous step's u; lane 0's ring
+                // values were loaded one step ahead), then the previous step's
+                // predicated stores, then the next step's loads, then its
+                // arithmetic: no branch separates two steps.
+                TS cn[ND], rn[NU];
+                auto load_step = [&](int k2) {
+#pragma unroll
+                    for (int k = 0; k < ND; k++)
+                        cn[k] = lds_v<TS>(sbase + (unsigned)(bo + k * kBlock + k2 * kLine) * ES);
+                    const unsigned rs = (rbase + (unsigned)(tb + k2 - 1 - kLag)) & (kRing - 1);
+#pragma unroll
+                    for (int q = 0; q < NU; q++) rn[q] = lds_v<TS>(rup + (rs * NU + (unsigned)q) * ES);
+                };
+                // the previous step's results, stored during the next step
+                TS pl[NL], pu[NU], py = 0;
+                long long poff = 0;
+                bool pst = false, psend = false;
+                unsigned pws = 0;
+#pragma unroll
+                for (int k = 0; k < NL; k++) pl[k] = 0;
+#pragma unroll
+                for (int q = 0; q < NU; q++) pu[q] = 0;
+                auto store_prev = [&]() {
+                    // y = 1/dl1 (RN for FP64), the forward sweep's reciprocal pivot
+#pragma unroll
+                    for (int k = 0; k < NL; k++) stg_if(dlp + k * PS + poff, pl[k], pst);
+#pragma unroll
+                    for (int q = 0; q < NU; q++) stg_if(dup + q * PS + poff, pu[q], pst);
+                    stg_if(rl1 + poff, py, pst);
+#pragma unroll
+                    for (int q = 0; q < NU; q++) sts_if(oup + (pws * NU + (unsigned)q) * ES, pu[q], psend);
+                };
+                load_step(0);
 #pragma unroll
                 for (int kk = 0; kk < kLag; kk++) {
                     const int tau = tb + kk;
                     const int s = tau - soff;
                     const int i = s - 2 * lane;
                     const bool valid = row_ok && i >= 0 && i < nx;
+                    const int src = tau - 1 - kLag;
+                    TS v[NU];
+#pragma unroll
+                    for (int q = 0; q < NU; q++) v[q] = shfl_up_v(mw[q]);
                     TS cb[ND];
 #pragma unroll
-                    for (int k = 0; k < ND; k++)
-                        cb[k] = valid ? stage_mem[bo + k * kBlock + kk * kLine] : (TS)(k == DIAG ? 1 : 0);
-                    const int src = tau - 1 - kLag;
-                    const unsigned rs = (rbase + (unsigned)src) & (kRing - 1);
+                    for (int k = 0; k < ND; k++) cb[k] = valid ? cn[k] : (TS)(k == DIAG ? 1 : 0);
 #pragma unroll
                     for (int q = 0; q < NU; q++) {
-                        TS v = __shfl_up_sync(kFull, mw[q], 1);
-                        const TS r = ring_up[fw][rs * NU + q];
-                        if (lane == 0) v = (has_below && src >= 0) ? r : (TS)0;
-                        a3[q] = a2[q]; a2[q] = a1[q]; a1[q] = v;
+                        if (lane == 0) v[q] = (has_below && src >= 0) ? rn[q] : (TS)0;
+                        a3[q] = a2[q]; a2[q] = a1[q]; a1[q] = v[q];
                     }
+                    if (kk > 0) store_prev();
+                    if (kk + 1 < kLag) load_step(kk + 1);
                     // an invalid cell sees a unit row: all its divisions are by 1
                     // and its outputs are replaced by zeros below
                     const TS alpha = (valid && i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2) ? (TS)0.5 : (TS)0;
@@ -690,30 +762,28 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                     } else {
                         lu_cell_f<ND>(cb, alpha, mw, a1, a2, a3, l, u, y);
                     }
-                    if (valid && (!(fabs((double)l[0]) > 0.0) || !isfinite((double)l[0]))) bad_pivot = true;
+                    piv |= valid ? pivot_bad(l[0]) : 0u;
 #pragma unroll
                     for (int q = 0; q < NU; q++) u[q] = valid ? u[q] : (TS)0;
-                    if (has_rows && s >= 0 && s < SW) {
-                        // y = 1/dl1 (RN for FP64), the forward sweep's reciprocal pivot
 #pragma unroll
-                        for (int k = 0; k < NL; k++) SK(dlp + k * PS, s) = valid ? l[k] : (TS)0;
+                    for (int k = 0; k < NL; k++) pl[k] = valid ? l[k] : (TS)0;
 #pragma unroll
-                        for (int q = 0; q < NU; q++) SK(dup + q * PS, s) = u[q];
-                        SK(rl1, s) = valid ? y : (TS)0;
-                    }
+                    for (int q = 0; q < NU; q++) pu[q] = u[q];
+                    py = valid ? y : (TS)0;
+                    pst = has_rows && s >= 0 && s < SW;
+                    poff = wbase + (long long)s * kLine;
+                    psend = lane == 31 && send;
+                    pws = (rbase + (unsigned)tau) & (kRing - 1);
 #pragma unroll
                     for (int q = 0; q < NU; q++) mw[q] = u[q];
-                    if (lane == 31 && send) {
-                        const unsigned ws = (rbase + (unsigned)tau) & (kRing - 1);
-#pragma unroll
-                        for (int q = 0; q < NU; q++) out_up[fw][ws * NU + q] = u[q];
-                    }
                 }
+                store_prev();
             }
             if (lane == 31 && send) chan_send(up_ring_dst, up_full_dst, &out_up[fw][0], n, kLag * NU);
             if (lane == 0 && has_below && b >= 2) chan_release(up_empty_dst, n - 2);
         }
         if (lane == 0 && has_below && nbatch >= 2) chan_release(up_empty_dst, up_base + nbatch - 2);
+        if (piv) bad_pivot = true;
         fence_async_global();   // the sweeps read the factors with bulk copies
     }
     up_base += nbatch - 1;
