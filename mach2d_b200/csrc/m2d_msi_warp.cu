@@ -623,6 +623,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
     }
     const unsigned sbase = smem_u32(stage_mem);
     const unsigned rup = smem_u32(&ring_up[fw][0]), rdn = smem_u32(&ring_dn[fw][0]);
+    const unsigned oup1 = smem_u32(&out_up[fw][0]), odn1 = smem_u32(&out_dn[fw][0]);   // sweeps: one value per slot
     Stager<TS, NSTAGE, PMAX> st;
     st.mem = stage_mem;
     st.base = fw * NSTAGE * PMAX * kBlock;
@@ -830,7 +831,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                         mine = m0; a1 = b1; a2 = b2; a3 = b3;
                     }
                     // c: staged coefficients of the current step, rv: ring value
-                    // (lane 0's south-east neighbour); both loaded one step ahead
+                    // (lane 0's south-east neighbour); both loaded one step ahead.
+                    // Lane 31's value for the warp above is stored during the
+                    // next step (predicated, no branch between two steps).
+                    TS pw = 0;
                     TS c[NL + 2], rv;
 #pragma unroll
                     for (int k = 0; k < NL + 2; k++) c[k] = stage_mem[bo + k * kBlock];
@@ -843,6 +847,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                         const bool valid = row_ok && i >= 0 && i < nx;
                         const int src = tau - 1 - kLag;
                         TS v = shfl_up_v(mine);
+                        if (kk > 0)
+                            sts_if(oup1 + ((rbase + (unsigned)(tau - 1)) & (kRing - 1)) * ES, pw, lane == 31 && send);
                         TS cn[NL + 2], rvn = 0;
                         if (kk + 1 < kLag) {
 #pragma unroll
@@ -872,13 +878,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                         wv = valid ? wv : (TS)0;
                         ob[kk] = wv;
                         mine = wv;
-                        if (lane == 31 && send) out_up[fw][(rbase + (unsigned)tau) & (kRing - 1)] = wv;
+                        pw = wv;
                         if (kk + 1 < kLag) {
 #pragma unroll
                             for (int k = 0; k < NL + 2; k++) c[k] = cn[k];
                             rv = rvn;
                         }
                     }
+                    sts_if(oup1 + ((rbase + (unsigned)(tb + kLag - 1)) & (kRing - 1)) * ES, pw, lane == 31 && send);
                 }
                 if (lane == 31 && send) chan_send(up_ring_dst, up_full_dst, &out_up[fw][0], n, kLag);
                 if (lane == 0 && has_below && b >= 2) chan_release(up_empty_dst, n - 2);
@@ -921,6 +928,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                 // c: staged {w, du} of the current step, rv: ring value (lane
                 // 31's north-west neighbour); both loaded one step ahead
                 TS c[NU + 1], rv, ob[kLag];
+                TS pz = 0;   // lane 0's value for the warp below, stored during the next step
 #pragma unroll
                 for (int k = 0; k < NU + 1; k++) c[k] = stage_mem[bo + k * kBlock + (kLag - 1) * kLine];
                 rv = ring_dn[fw][(rbase + (unsigned)(tb - 1 - kLag)) & (kRing - 1)];
@@ -932,6 +940,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                     const bool valid = row_ok && i >= 0 && i < nx;
                     const int src = tau - 1 - kLag;
                     TS v = shfl_down_v(mine);
+                    if (kk > 0)
+                        sts_if(odn1 + ((rbase + (unsigned)(tau - 1)) & (kRing - 1)) * ES, pz, lane == 0 && send);
                     TS cn[NU + 1], rvn = 0;
                     if (kk + 1 < kLag) {
 #pragma unroll
@@ -953,13 +963,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                     z = valid ? z : (TS)0;
                     ob[kk] = z;
                     mine = z;
-                    if (lane == 0 && send) out_dn[fw][(rbase + (unsigned)tau) & (kRing - 1)] = z;
+                    pz = z;
                     if (kk + 1 < kLag) {
 #pragma unroll
                         for (int k = 0; k < NU + 1; k++) c[k] = cn[k];
                         rv = rvn;
                     }
                 }
+                sts_if(odn1 + ((rbase + (unsigned)(tb + kLag - 1)) & (kRing - 1)) * ES, pz, lane == 0 && send);
                 if (lane == 0 && send) chan_send(dn_ring_dst, dn_full_dst, &out_dn[fw][0], n, kLag);
                 if (lane == 31 && has_above && b >= 2) chan_release(dn_empty_dst, n - 2);
                 // the batch's lines of z
