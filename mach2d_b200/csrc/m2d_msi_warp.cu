@@ -821,7 +821,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                 const TS m0 = mine, b1 = a1, b2 = a2, b3 = a3;   // state at batch start
                 const unsigned rbase = (unsigned)up_base * kLag;   // ring position of step 0
                 unsigned bad = 0;
-                TS ob[kLag];   // results of the batch, stored after its last step
 #pragma unroll
                 for (int pass = 0; pass < (EXACT ? 2 : 1); pass++) {
                     if (pass == 1) {
@@ -847,8 +846,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                         const bool valid = row_ok && i >= 0 && i < nx;
                         const int src = tau - 1 - kLag;
                         TS v = shfl_up_v(mine);
-                        if (kk > 0)
+                        if (kk > 0) {
+                            // the previous step's w: to the warp above and to its slot
                             sts_if(oup1 + ((rbase + (unsigned)(tau - 1)) & (kRing - 1)) * ES, pw, lane == 31 && send);
+                            stg_if(wp + wbase + (long long)(s - 1) * kLine, pw, has_rows && s - 1 >= 0 && s - 1 < SW);
+                        }
                         TS cn[NL + 2], rvn = 0;
                         if (kk + 1 < kLag) {
 #pragma unroll
@@ -876,7 +878,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                             wv = -num * c[NL + 1];
                         }
                         wv = valid ? wv : (TS)0;
-                        ob[kk] = wv;
                         mine = wv;
                         pw = wv;
                         if (kk + 1 < kLag) {
@@ -886,16 +887,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                         }
                     }
                     sts_if(oup1 + ((rbase + (unsigned)(tb + kLag - 1)) & (kRing - 1)) * ES, pw, lane == 31 && send);
+                    {
+                        const int sl = tb + kLag - 1 - soff;
+                        stg_if(wp + wbase + (long long)sl * kLine, pw, has_rows && sl >= 0 && sl < SW);
+                    }
                 }
                 if (lane == 31 && send) chan_send(up_ring_dst, up_full_dst, &out_up[fw][0], n, kLag);
                 if (lane == 0 && has_below && b >= 2) chan_release(up_empty_dst, n - 2);
-                // the batch's lines of w
-                if (has_rows) {
-                    const int s0 = tb - soff;
-#pragma unroll
-                    for (int kk = 0; kk < kLag; kk++)
-                        if (s0 + kk >= 0 && s0 + kk < SW) SK(wp, s0 + kk) = ob[kk];
-                }
             }
             if (lane == 0 && has_below && nbatch >= 2) chan_release(up_empty_dst, up_base + nbatch - 2);
             fence_async_global();   // the backward sweep reads w with bulk copies
@@ -927,8 +925,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                 const unsigned rbase = (unsigned)dn_base * kLag;
                 // c: staged {w, du} of the current step, rv: ring value (lane
                 // 31's north-west neighbour); both loaded one step ahead
-                TS c[NU + 1], rv, ob[kLag];
-                TS pz = 0;   // lane 0's value for the warp below, stored during the next step
+                TS c[NU + 1], rv;
+                TS pz = 0;   // the previous step's z, stored during the next step
 #pragma unroll
                 for (int k = 0; k < NU + 1; k++) c[k] = stage_mem[bo + k * kBlock + (kLag - 1) * kLine];
                 rv = ring_dn[fw][(rbase + (unsigned)(tb - 1 - kLag)) & (kRing - 1)];
@@ -940,8 +938,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                     const bool valid = row_ok && i >= 0 && i < nx;
                     const int src = tau - 1 - kLag;
                     TS v = shfl_down_v(mine);
-                    if (kk > 0)
+                    if (kk > 0) {
+                        // the previous step's z: to the warp below and to its slot
                         sts_if(odn1 + ((rbase + (unsigned)(tau - 1)) & (kRing - 1)) * ES, pz, lane == 0 && send);
+                        stg_if(wp + wbase + (long long)(s + 1) * kLine, pz, has_rows && s + 1 >= 0 && s + 1 < SW);
+                    }
                     TS cn[NU + 1], rvn = 0;
                     if (kk + 1 < kLag) {
 #pragma unroll
@@ -961,7 +962,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                         if (ND == 9) z = fmaf(-c[4], a3, z);
                     }
                     z = valid ? z : (TS)0;
-                    ob[kk] = z;
                     mine = z;
                     pz = z;
                     if (kk + 1 < kLag) {
@@ -971,15 +971,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                     }
                 }
                 sts_if(odn1 + ((rbase + (unsigned)(tb + kLag - 1)) & (kRing - 1)) * ES, pz, lane == 0 && send);
+                {
+                    const int sl = Tmax - (tb + kLag - 1) - soff;
+                    stg_if(wp + wbase + (long long)sl * kLine, pz, has_rows && sl >= 0 && sl < SW);
+                }
                 if (lane == 0 && send) chan_send(dn_ring_dst, dn_full_dst, &out_dn[fw][0], n, kLag);
                 if (lane == 31 && has_above && b >= 2) chan_release(dn_empty_dst, n - 2);
-                // the batch's lines of z
-                if (has_rows) {
-                    const int s0 = Tmax - tb - soff;
-#pragma unroll
-                    for (int kk = 0; kk < kLag; kk++)
-                        if (s0 - kk >= 0 && s0 - kk < SW) SK(wp, s0 - kk) = ob[kk];
-                }
             }
             if (lane == 31 && has_above && nbatch >= 2) chan_release(dn_empty_dst, dn_base + nbatch - 2);
         }
