@@ -367,6 +367,68 @@ __device__ __forceinline__ double residual_cell(const double *__restrict__ a, co
     return v;
 }
 
+__device__ __forceinline__ void named_bar(unsigned id, unsigned count)
+{
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
+// The initial residual r = A x - b of this CTA's slice, computed by the
+// nhelp helper warps (hw = 0..nhelp-1) while the wavefront warps factorise.
+// The helpers run the 256 threads of cluster_residual as virtual threads
+// (virtual thread t takes cells lo + t + 256 k, in that order) and the same
+// tree over their sums, so the norm is bitwise the one cluster_residual
+// gives.  The CTA's sum goes to CTA 0's part[rank]; cluster_total combines
+// the CTAs after the next cluster barrier.
+template <int ND, typename TS>
+__device__ void helper_residual(cg::cluster_group &cl, const double *__restrict__ a, const double *__restrict__ b,
+                                const double *x, TS *r, int nx, int ny, int sw, double *red, double *part,
+                                int nhelp, int hw)
+{
+    const long long N = (long long)nx * ny;
+    const int C = (int)cl.num_blocks(), rank = (int)cl.block_rank();
+    const long long per = (N + C - 1) / C;
+    const long long lo = per * rank, hi = (lo + per < N) ? lo + per : N;
+    const int lane = threadIdx.x & 31;
+    const unsigned nthr = (unsigned)nhelp * 32u;
+    for (int vw = hw; vw < kThreads / 32; vw += nhelp) {
+        const int t = vw * 32 + lane;
+        double acc = 0.0;
+#pragma unroll 8
+        for (long long np = lo + t; np < hi; np += kThreads) {
+            const int j = (int)((unsigned)np / (unsigned)nx), i = (int)np - j * nx;   // N < 2^31
+            const double v = residual_cell<ND>(a, b, x, np, i, j, nx, ny, N);
+            r[skew_slot(i, j, sw)] = (TS)v;
+            acc = acc + v * v;
+        }
+        red[t] = acc;
+    }
+    fence_async_global();   // the forward sweep reads r with bulk copies
+    named_bar(1, nthr);
+    for (int s = kThreads / 2; s > 0; s >>= 1) {
+        for (int t = hw * 32 + lane; t < s; t += (int)nthr) red[t] = red[t] + red[t + s];
+        named_bar(1, nthr);
+    }
+    if (hw == 0 && lane == 0) {
+        double *p0 = cl.map_shared_rank(part, 0);
+        p0[rank] = red[0];
+    }
+}
+
+// After a cluster barrier: the sum of the CTAs' part[] in rank order,
+// identical in every thread
+__device__ double cluster_total(cg::cluster_group &cl, double *part)
+{
+    const int C = (int)cl.num_blocks(), rank = (int)cl.block_rank();
+    cl.sync();
+    if (rank == 0 && threadIdx.x == 0) {
+        double s = 0.0;
+        for (int c = 0; c < C; c++) s = s + part[c];
+        for (int c = 0; c < C; c++) cl.map_shared_rank(part, c)[kMaxCluster] = s;
+    }
+    cl.sync();
+    return part[kMaxCluster];
+}
+
 // Cluster-wide pass (this CTA takes a contiguous slice of cells): first
 // x += z when z (wavefront-major) is given, then r = A x - b stored
 // wavefront-major.  Returns the cluster-wide sum of r^2, identical in every
@@ -786,13 +848,18 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
         if (lane == 0 && has_below && nbatch >= 2) chan_release(up_empty_dst, up_base + nbatch - 2);
         if (piv) bad_pivot = true;
         fence_async_global();   // the sweeps read the factors with bulk copies
+    } else {
+        // meanwhile the helper warps compute the initial residual
+        helper_residual<ND, TS>(cl, a, S.b, x, rp, nx, ny, SW, red, part, kThreads / 32 - WPC, wl - WPC);
     }
     up_base += nbatch - 1;
     if (bad_pivot && L.err) atomicOr(L.err, ERR_NONFINITE_PIVOT);
     stamp(L, rank, 1);
 
     // ---- fb2d9 / fb2d5 (msi2d9-v03.f90:42-262, msi2d5-v03.f90:42-233)
-    const double rr0 = cluster_residual<ND, TS>(cl, a, S.b, x, nullptr, rp, nx, ny, SW, red, part);
+    // (the barrier in cluster_total also makes every row's factors and the
+    // residual final before the first forward sweep)
+    const double rr0 = cluster_total(cl, part);
     stamp(L, rank, 2);
     const double gammarp = L.tol * sqrt(rr0);
     const int cap = (L.nitm > 0) ? L.nitm : kMaxIterUnbounded;
