@@ -89,6 +89,14 @@ int m2d_msi_solve_device_timed(int nd, int nx, int ny, int nitm, double tol,
                                const double *d_a, const double *d_b, double *d_x,
                                double *d_work, void *stream, int *d_nit,
                                unsigned long long *d_times);
+/* Diagnostics: the FP64 solves factorise with reciprocal-based (Markstein)
+ * quotients and check every factor against IEEE division while the first
+ * sweeps run; when one differs (operands near the subnormal or overflow
+ * range), the factorisation is repeated with IEEE division before x changes.
+ * Returns how many factorisations were repeated on the current device since
+ * the library was loaded (-1 on a CUDA error).  No counterpart in the
+ * reference. */
+long long m2d_msi_lu_redo_count(void);
 
 /* No counterpart in the reference ("MSI_MIXED" in solvers_init).  The same
  * MSI iteration with the factorisation and both sweeps in FP32: the residual

@@ -248,6 +248,8 @@ int m2d_msi_solve_device_timed(int nd, int nx, int ny, int nitm, double tol, con
                                    m2d_msi_workspace_doubles(nd, nx, ny), stream, d_nit, d_times, 0);
 }
 
+long long m2d_msi_lu_redo_count(void) { return msi_lu_redo_count(); }
+
 static int tdma_host(int nd, const int *nx, const int *ny, const int *nitm, const double *a,
                      const double *b, double *x)
 {

@@ -86,12 +86,7 @@ __device__ __forceinline__ unsigned range_bad(double a, double b)
 {
     return exp_out(b) | (exp_out(a) & (a != 0.0 ? 1u : 0u));
 }
-// n / d on the fast path: the IEEE quotient unless bad is raised
-__device__ __forceinline__ double div_fast(double n, double d, unsigned &bad)
-{
-    bad |= range_bad(n, d);
-    return div_recip(n, d, __drcp_rn(d));
-}
+
 
 __device__ __forceinline__ void stamp(const MsiLaunch &L, int rank, int k)
 {
@@ -482,14 +477,15 @@ __device__ double cluster_residual(cg::cluster_group &cl, const double *__restri
 
 // One factorisation step of one cell (lu2d9 / lu2d5).  cb is the row of A
 // (a unit row for an invalid cell), mw the own row's previous u, a1/a2/a3
-// the row below's u at SE/S/SW.  FAST divides with div_fast and raises bad
-// when that may differ from IEEE division; otherwise it divides with '/'.
+// the row below's u at SE/S/SW.  FAST divides with Markstein quotients
+// (checked against IEEE division afterwards, verify_factors); otherwise it
+// divides with '/'.
 template <int ND, bool FAST>
 __device__ __forceinline__ void lu_cell(const double (&cb)[ND], double alpha, const double *mw,
                                         const double *a1, const double *a2, const double *a3, double *l,
-                                        double *u, double &y1, unsigned &bad)
+                                        double *u, double &y1)
 {
-    auto dv = [&](double n, double d) -> double { return FAST ? div_fast(n, d, bad) : n / d; };
+    auto dv = [&](double n, double d) -> double { return FAST ? div_recip(n, d, __drcp_rn(d)) : n / d; };
     if (ND == 9) {
         const double b1 = cb[0], b2 = cb[1], b3 = cb[2], b4 = cb[3], b5 = cb[4];
         const double b6 = cb[5], b7 = cb[6], b8 = cb[7], b9 = cb[8];
@@ -506,7 +502,6 @@ __device__ __forceinline__ void lu_cell(const double (&cb)[ND], double alpha, co
         if (FAST) {
             const double y = __drcp_rn(l1);
             y1 = y;
-            bad |= range_bad(n0, l1) | range_bad(n1, l1) | range_bad(n2, l1) | range_bad(b9, l1);
             u[0] = div_recip(n0, l1, y); u[1] = div_recip(n1, l1, y);
             u[2] = div_recip(n2, l1, y); u[3] = div_recip(b9, l1, y);
         } else {
@@ -527,7 +522,6 @@ __device__ __forceinline__ void lu_cell(const double (&cb)[ND], double alpha, co
         if (FAST) {
             const double y = __drcp_rn(l1);
             y1 = y;
-            bad |= range_bad(n0, l1) | range_bad(n1, l1) | range_bad(n2, l1);
             u[0] = div_recip(n0, l1, y); u[1] = div_recip(n1, l1, y); u[2] = div_recip(n2, l1, y);
         } else {
             u[0] = n0 / l1; u[1] = n1 / l1; u[2] = n2 / l1;
@@ -578,6 +572,60 @@ __device__ __forceinline__ void lu_cell_f(const float (&cb)[ND], float alpha, co
         y1 = y;
         l[0] = l1; l[1] = l2; l[2] = l3; l[3] = l4;
     }
+}
+
+// factorisations repeated with IEEE division on this device since load
+__device__ unsigned long long g_lu_redo = 0;
+
+// The helper warps' check of a Markstein factorisation: every real cell of
+// this CTA's row groups is factorised again from its row of A and the stored
+// u of its W, S, SE [and SW] neighbours (zero outside the grid, as in the
+// wavefront) with IEEE division, and its stored dl, du and 1/dl1 are
+// compared bit for bit.  If every cell matches, the stored factors are those
+// of the IEEE recurrence (induction over the wavefront order); otherwise
+// *vbad is set.  The cells are visited line by line of the wavefront-major
+// planes (lane l of line (w, s) is cell (s - 2l, 32w + l)), so the loads are
+// whole 256-byte lines: the cell's own factors, A and the W neighbour on the
+// line itself, the S, SE and SW neighbours on lines s-2, s-1, s-3 one lane
+// down (lane 0: lines s+62, s+63, s+61 of the row group below, lane 31).
+template <int ND>
+__device__ void verify_factors(const double *asp, const double *dl, const double *du, const double *rl, int nx,
+                               int ny, int sw, long long PS, int wg0, int nwg, int nhelp, int hw, unsigned *vbad)
+{
+    constexpr int NU = (ND == 9) ? 4 : 3;
+    constexpr int NL = (ND == 9) ? 5 : 4;
+    const int lane = threadIdx.x & 31;
+    unsigned diff = 0;
+    for (int idx = hw; idx < nwg * sw; idx += nhelp) {
+        const int wg = wg0 + idx / sw, s = idx % sw;
+        const int j = 32 * wg + lane, i = s - 2 * lane;
+        if (j >= ny || i < 0 || i >= nx) continue;
+        const long long P = ((long long)wg * sw + s) * kLine + lane;
+        double cb[ND];
+#pragma unroll
+        for (int k = 0; k < ND; k++) cb[k] = asp[k * PS + P];
+        const double alpha = (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2) ? 0.5 : 0.0;
+        // neighbours in the row below: lane - 1 of this group, or lane 31 of the group below
+        const long long B = (lane > 0) ? ((long long)wg * sw + s) * kLine + lane - 1
+                                       : ((long long)(wg - 1) * sw + s + 64) * kLine + 31;
+        const long long pS = B - 2 * kLine, pSE = B - kLine, pSW = B - 3 * kLine, pW = P - kLine;
+        double mw[NU], a1[NU], a2[NU], a3[NU];
+#pragma unroll
+        for (int q = 0; q < NU; q++) {
+            mw[q] = (i >= 1) ? du[q * PS + pW] : 0.0;
+            a2[q] = (j >= 1) ? du[q * PS + pS] : 0.0;
+            a1[q] = (j >= 1 && i + 1 <= nx - 1) ? du[q * PS + pSE] : 0.0;
+            a3[q] = (j >= 1 && i >= 1) ? du[q * PS + pSW] : 0.0;
+        }
+        double l[NL], u[NU], y;
+        lu_cell<ND, false>(cb, alpha, mw, a1, a2, a3, l, u, y);
+#pragma unroll
+        for (int k = 0; k < NL; k++) diff |= (__double_as_longlong(l[k]) != __double_as_longlong(dl[k * PS + P])) ? 1u : 0u;
+#pragma unroll
+        for (int q = 0; q < NU; q++) diff |= (__double_as_longlong(u[q]) != __double_as_longlong(du[q * PS + P])) ? 1u : 0u;
+        diff |= (__double_as_longlong(y) != __double_as_longlong(rl[P])) ? 1u : 0u;
+    }
+    if (diff) *vbad = 1u;
 }
 
 // A (plane-major, cell order) -> wavefront-major planes of element type TS for
@@ -635,7 +683,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
     __shared__ unsigned long long full_up[WPC][kSlots], empty_up[WPC][kSlots];
     __shared__ unsigned long long full_dn[WPC][kSlots], empty_dn[WPC][kSlots];
     __shared__ unsigned long long stage_bar[WPC][NSTAGE];
-    __shared__ TS lu_save[WPC][4 * NU][32];      // factorisation state at batch start
+    __shared__ unsigned vbad;                     // a factor differs from its IEEE value (helpers)
     __shared__ double red[kThreads];
     __shared__ double part[kMaxCluster + 1];
     extern __shared__ __align__(128) double stage_raw[];   // WPC x NSTAGE x PMAX x kBlock elements
@@ -675,6 +723,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
     const long long wbase = line0 * kLine + lane;
 #define SK(p, s) (p)[wbase + (long long)(s) * kLine]
 
+    if (threadIdx.x == 0) vbad = 0u;
     if (threadIdx.x < WPC) {
         for (int q = 0; q < kSlots; q++) {
             mbar_init(&full_up[threadIdx.x][q], 1); mbar_init(&empty_up[threadIdx.x][q], 1);
@@ -715,7 +764,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
     stamp(L, rank, 0);
 
     // ---- incomplete LU (lu2d9 msi2d9-v03.f90:277-432, lu2d5 msi2d5-v03.f90:247-330)
-    if (front) {
+    // run by the wavefront warps; IEEE = true divides with '/', false (FP64)
+    // with Markstein quotients, which the helper warps check afterwards
+    auto run_lu = [&](auto ieee_tag) {
+        constexpr bool IEEE = decltype(ieee_tag)::value;
         TS *ap[ND];
 #pragma unroll
         for (int k = 0; k < ND; k++) ap[k] = asp + k * PS;
@@ -733,124 +785,102 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
             if (send) chan_slot_free(&empty_up[fw][0], n, timed_out);
             const int bo = stage_wait(st, timed_out) + lane;
             if (b + NSTAGE - 1 < nbatch) stage_issue<ND>(st, ap, line0, (b + NSTAGE - 1) * kLag - soff, SW);
-            if (EXACT) {
+            const unsigned rbase = (unsigned)up_base * kLag;
+            // Software-pipelined steps.  A step first issues its critical
+            // inputs (the shuffles of the previous step's u; lane 0's ring
+            // values were loaded one step ahead), then the previous step's
+            // predicated stores, then the next step's loads, then its
+            // arithmetic: no branch separates two steps.
+            TS cn[ND], rn[NU];
+            auto load_step = [&](int k2) {
+#pragma unroll
+                for (int k = 0; k < ND; k++)
+                    cn[k] = lds_v<TS>(sbase + (unsigned)(bo + k * kBlock + k2 * kLine) * ES);
+                const unsigned rs = (rbase + (unsigned)(tb + k2 - 1 - kLag)) & (kRing - 1);
+#pragma unroll
+                for (int q = 0; q < NU; q++) rn[q] = lds_v<TS>(rup + (rs * NU + (unsigned)q) * ES);
+            };
+            // the previous step's results, stored during the next step
+            TS pl[NL], pu[NU], py = 0;
+            long long poff = 0;
+            bool pst = false, psend = false;
+            unsigned pws = 0;
+#pragma unroll
+            for (int k = 0; k < NL; k++) pl[k] = 0;
+#pragma unroll
+            for (int q = 0; q < NU; q++) pu[q] = 0;
+            auto store_prev = [&]() {
+                // y = 1/dl1 (RN for FP64), the forward sweep's reciprocal pivot
+#pragma unroll
+                for (int k = 0; k < NL; k++) stg_if(dlp + k * PS + poff, pl[k], pst);
+#pragma unroll
+                for (int q = 0; q < NU; q++) stg_if(dup + q * PS + poff, pu[q], pst);
+                stg_if(rl1 + poff, py, pst);
+#pragma unroll
+                for (int q = 0; q < NU; q++) sts_if(oup + (pws * NU + (unsigned)q) * ES, pu[q], psend);
+            };
+            load_step(0);
+#pragma unroll
+            for (int kk = 0; kk < kLag; kk++) {
+                const int tau = tb + kk;
+                const int s = tau - soff;
+                const int i = s - 2 * lane;
+                const bool valid = row_ok && i >= 0 && i < nx;
+                const int src = tau - 1 - kLag;
+                TS v[NU];
+#pragma unroll
+                for (int q = 0; q < NU; q++) v[q] = shfl_up_v(mw[q]);
+                TS cb[ND];
+#pragma unroll
+                for (int k = 0; k < ND; k++) cb[k] = valid ? cn[k] : (TS)(k == DIAG ? 1 : 0);
 #pragma unroll
                 for (int q = 0; q < NU; q++) {
-                    lu_save[fw][q][lane] = mw[q]; lu_save[fw][NU + q][lane] = a1[q];
-                    lu_save[fw][2 * NU + q][lane] = a2[q]; lu_save[fw][3 * NU + q][lane] = a3[q];
+                    if (lane == 0) v[q] = (has_below && src >= 0) ? rn[q] : (TS)0;
+                    a3[q] = a2[q]; a2[q] = a1[q]; a1[q] = v[q];
                 }
+                if (kk > 0) store_prev();
+                if (kk + 1 < kLag) load_step(kk + 1);
+                // an invalid cell sees a unit row: all its divisions are by 1
+                // and its outputs are replaced by zeros below
+                const TS alpha = (valid && i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2) ? (TS)0.5 : (TS)0;
+                TS l[NL], u[NU], y;
+                if constexpr (EXACT) lu_cell<ND, !IEEE>(cb, alpha, mw, a1, a2, a3, l, u, y);
+                else lu_cell_f<ND>(cb, alpha, mw, a1, a2, a3, l, u, y);
+                piv |= valid ? pivot_bad(l[0]) : 0u;
+#pragma unroll
+                for (int q = 0; q < NU; q++) u[q] = valid ? u[q] : (TS)0;
+#pragma unroll
+                for (int k = 0; k < NL; k++) pl[k] = valid ? l[k] : (TS)0;
+#pragma unroll
+                for (int q = 0; q < NU; q++) pu[q] = u[q];
+                py = valid ? y : (TS)0;
+                pst = has_rows && s >= 0 && s < SW;
+                poff = wbase + (long long)s * kLine;
+                psend = lane == 31 && send;
+                pws = (rbase + (unsigned)tau) & (kRing - 1);
+#pragma unroll
+                for (int q = 0; q < NU; q++) mw[q] = u[q];
             }
-            const unsigned rbase = (unsigned)up_base * kLag;
-            unsigned bad = 0;
-#pragma unroll
-            for (int pass = 0; pass < (EXACT ? 2 : 1); pass++) {
-                // pass 0: fast divisions; pass 1 (only if some cell of pass 0
-                // may differ from IEEE division): the batch again from its
-                // start state with IEEE division
-                if (pass == 1) {
-                    if (!__any_sync(kFull, bad != 0u)) break;
-#pragma unroll
-                    for (int q = 0; q < NU; q++) {
-                        mw[q] = lu_save[fw][q][lane]; a1[q] = lu_save[fw][NU + q][lane];
-                        a2[q] = lu_save[fw][2 * NU + q][lane]; a3[q] = lu_save[fw][3 * NU + q][lane];
-                    }
-                }
-                // Software-pipelined steps.  A step first issues its critical
-                // inputs (the shuffles of the previous step's u; lane 0's ring
-                // values were loaded one step ahead), then the previous step's
-                // predicated stores, then the next step's loads, then its
-                // arithmetic: no branch separates two steps.
-                TS cn[ND], rn[NU];
-                auto load_step = [&](int k2) {
-#pragma unroll
-                    for (int k = 0; k < ND; k++)
-                        cn[k] = lds_v<TS>(sbase + (unsigned)(bo + k * kBlock + k2 * kLine) * ES);
-                    const unsigned rs = (rbase + (unsigned)(tb + k2 - 1 - kLag)) & (kRing - 1);
-#pragma unroll
-                    for (int q = 0; q < NU; q++) rn[q] = lds_v<TS>(rup + (rs * NU + (unsigned)q) * ES);
-                };
-                // the previous step's results, stored during the next step
-                TS pl[NL], pu[NU], py = 0;
-                long long poff = 0;
-                bool pst = false, psend = false;
-                unsigned pws = 0;
-#pragma unroll
-                for (int k = 0; k < NL; k++) pl[k] = 0;
-#pragma unroll
-                for (int q = 0; q < NU; q++) pu[q] = 0;
-                auto store_prev = [&]() {
-                    // y = 1/dl1 (RN for FP64), the forward sweep's reciprocal pivot
-#pragma unroll
-                    for (int k = 0; k < NL; k++) stg_if(dlp + k * PS + poff, pl[k], pst);
-#pragma unroll
-                    for (int q = 0; q < NU; q++) stg_if(dup + q * PS + poff, pu[q], pst);
-                    stg_if(rl1 + poff, py, pst);
-#pragma unroll
-                    for (int q = 0; q < NU; q++) sts_if(oup + (pws * NU + (unsigned)q) * ES, pu[q], psend);
-                };
-                load_step(0);
-#pragma unroll
-                for (int kk = 0; kk < kLag; kk++) {
-                    const int tau = tb + kk;
-                    const int s = tau - soff;
-                    const int i = s - 2 * lane;
-                    const bool valid = row_ok && i >= 0 && i < nx;
-                    const int src = tau - 1 - kLag;
-                    TS v[NU];
-#pragma unroll
-                    for (int q = 0; q < NU; q++) v[q] = shfl_up_v(mw[q]);
-                    TS cb[ND];
-#pragma unroll
-                    for (int k = 0; k < ND; k++) cb[k] = valid ? cn[k] : (TS)(k == DIAG ? 1 : 0);
-#pragma unroll
-                    for (int q = 0; q < NU; q++) {
-                        if (lane == 0) v[q] = (has_below && src >= 0) ? rn[q] : (TS)0;
-                        a3[q] = a2[q]; a2[q] = a1[q]; a1[q] = v[q];
-                    }
-                    if (kk > 0) store_prev();
-                    if (kk + 1 < kLag) load_step(kk + 1);
-                    // an invalid cell sees a unit row: all its divisions are by 1
-                    // and its outputs are replaced by zeros below
-                    const TS alpha = (valid && i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2) ? (TS)0.5 : (TS)0;
-                    TS l[NL], u[NU], y;
-                    if constexpr (EXACT) {
-                        if (pass == 0) {
-                            unsigned bc = 0;
-                            lu_cell<ND, true>(cb, alpha, mw, a1, a2, a3, l, u, y, bc);
-                            bad |= valid ? bc : 0u;
-                        } else {
-                            unsigned unused = 0;
-                            lu_cell<ND, false>(cb, alpha, mw, a1, a2, a3, l, u, y, unused);
-                        }
-                    } else {
-                        lu_cell_f<ND>(cb, alpha, mw, a1, a2, a3, l, u, y);
-                    }
-                    piv |= valid ? pivot_bad(l[0]) : 0u;
-#pragma unroll
-                    for (int q = 0; q < NU; q++) u[q] = valid ? u[q] : (TS)0;
-#pragma unroll
-                    for (int k = 0; k < NL; k++) pl[k] = valid ? l[k] : (TS)0;
-#pragma unroll
-                    for (int q = 0; q < NU; q++) pu[q] = u[q];
-                    py = valid ? y : (TS)0;
-                    pst = has_rows && s >= 0 && s < SW;
-                    poff = wbase + (long long)s * kLine;
-                    psend = lane == 31 && send;
-                    pws = (rbase + (unsigned)tau) & (kRing - 1);
-#pragma unroll
-                    for (int q = 0; q < NU; q++) mw[q] = u[q];
-                }
-                store_prev();
-            }
+            store_prev();
             if (lane == 31 && send) chan_send(up_ring_dst, up_full_dst, &out_up[fw][0], n, kLag * NU);
             if (lane == 0 && has_below && b >= 2) chan_release(up_empty_dst, n - 2);
         }
         if (lane == 0 && has_below && nbatch >= 2) chan_release(up_empty_dst, up_base + nbatch - 2);
         if (piv) bad_pivot = true;
         fence_async_global();   // the sweeps read the factors with bulk copies
-    } else {
+    };
+    // helper warps: those on the SM sub-partitions (warp w runs on w % 4)
+    // that no wavefront warp uses, so that their work does not take issue
+    // slots or FP64 units from the recurrence
+    static_assert(WPC >= 1 && WPC <= 3, "wavefront warps must leave a sub-partition for the helpers");
+    const bool helper = (wl & 3) >= WPC;
+    const int nhelp = (kThreads / 32 / 4) * (4 - WPC);
+    const int hw = (wl >> 2) * (4 - WPC) + ((wl & 3) - WPC);
+    if (front) {
+        run_lu(std::false_type{});
+    } else if (helper) {
         // meanwhile the helper warps compute the initial residual
-        helper_residual<ND, TS>(cl, a, S.b, x, rp, nx, ny, SW, red, part, kThreads / 32 - WPC, wl - WPC);
+        helper_residual<ND, TS>(cl, a, S.b, x, rp, nx, ny, SW, red, part, nhelp, hw);
     }
     up_base += nbatch - 1;
     if (bad_pivot && L.err) atomicOr(L.err, ERR_NONFINITE_PIVOT);
@@ -863,6 +893,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
     stamp(L, rank, 2);
     const double gammarp = L.tol * sqrt(rr0);
     const int cap = (L.nitm > 0) ? L.nitm : kMaxIterUnbounded;
+    // while the first sweeps run, the helper warps check that every stored
+    // factor is the IEEE result of its stored inputs; the verdict is read
+    // before the first correction of x
+    if constexpr (EXACT) {
+        if (helper)
+            verify_factors<ND>(asp, dlp, dup, rl1, nx, ny, SW, PS, rank * WPC, WPC, nhelp, hw, &vbad);
+    }
+    bool lu_redone = !EXACT;
     int nit = 0;
     double rr = rr0;
     for (;;) {
@@ -1050,6 +1088,25 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
         dn_base += nbatch - 1;
         if (nit == 1) stamp(L, rank, 4);
         // var = z + var, then the new residual
+        if (!lu_redone) {
+            // the helpers' verdict on the Markstein factorisation: if any
+            // factor differs from IEEE division, factorise again with IEEE
+            // division and repeat the first iteration (x is still untouched)
+            cl.sync();
+            unsigned any = 0;
+            for (int c = 0; c < C; c++) any |= *cl.map_shared_rank(&vbad, c);
+            lu_redone = true;
+            if (any) {
+                if (rank == 0 && threadIdx.x == 0) atomicAdd(&g_lu_redo, 1ull);
+                cl.sync();   // every CTA has read the verdicts
+                if (front) run_lu(std::true_type{});
+                up_base += nbatch - 1;
+                if (bad_pivot && L.err) atomicOr(L.err, ERR_NONFINITE_PIVOT);
+                cl.sync();   // every row's factors are final
+                nit = 0;
+                continue;
+            }
+        }
         rr = cluster_residual<ND, TS>(cl, a, S.b, x, wp, rp, nx, ny, SW, red, part);
         if (nit == 1) stamp(L, rank, 5);
         if (sqrt(rr) < gammarp) break;
@@ -1075,6 +1132,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
 }
 
 bool msi_warp_supported(int ny) { return ny <= 1024; }
+
+long long msi_lu_redo_count()
+{
+    unsigned long long v = 0;
+    if (cudaMemcpyFromSymbol(&v, g_lu_redo, sizeof v) != cudaSuccess) return -1;
+    return (long long)v;
+}
 
 template <int ND, int WPC, int NSTAGE, typename TS>
 static size_t stage_bytes()

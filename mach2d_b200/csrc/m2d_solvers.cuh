@@ -54,6 +54,8 @@ size_t msi_smem_bytes(int nd, int ny);
 cudaError_t launch_msi(int nd, const MsiLaunch &L, int nsys, cudaStream_t st);
 // the warp-synchronous kernel used by launch_msi for ny <= 1024 (m2d_msi_warp.cu)
 bool msi_warp_supported(int ny);
+// factorisations the cluster kernel repeated with IEEE division (current device)
+long long msi_lu_redo_count();
 cudaError_t launch_msi_warp(int nd, const MsiLaunch &L, int nsys, cudaStream_t st);
 // the one-step-per-barrier kernel, any ny <= msi_max_ny() (m2d_msi.cu)
 cudaError_t launch_msi_generic(int nd, const MsiLaunch &L, int nsys, cudaStream_t st);

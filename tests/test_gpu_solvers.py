@@ -50,6 +50,33 @@ def test_msi_bitwise(nd, nx, ny, nitm, tol, seed):
 
 
 @pytest.mark.parametrize("nd", [9, 5])
+def test_msi_ieee_fallback_on_extreme_magnitudes(nd):
+    """A fifth of the equations scaled by 2^-1015 (the exact solution does not
+    change): the remainders of their factors' reciprocal-based (Markstein)
+    quotients fall into the subnormal range, where such a quotient need not
+    be the IEEE one.  Every factor is checked against IEEE division and the
+    factorisation repeated with it, so the solve stays bitwise the oracle's,
+    and the repetition is counted."""
+    nx, ny = 47, 70
+    a, b = random_dominant_planes(nd, nx, ny, seed=21)
+    rows = np.random.default_rng(22).random(nx * ny) < 0.2
+    scale = np.where(rows, 2.0 ** -1015, 1.0)
+    a = (a.reshape(nd, -1) * scale).reshape(-1).copy()
+    b = b * scale
+    from mach2d_b200._lib import lib
+    L = lib()
+    L.m2d_msi_lu_redo_count.restype = ctypes.c_longlong
+    before = L.m2d_msi_lu_redo_count()
+    x0 = np.random.default_rng(23).standard_normal(nx * ny)
+    xg, xo = x0.copy(), x0.copy()
+    nit_g = _gpu_msi(nd, nx, ny, 4, 1e-30, a, b, xg)
+    nit_o = orc(f"msi{nd}_solve", nx, ny, 4, 1e-30, a, b, xo)
+    assert nit_g == nit_o
+    assert np.array_equal(xg, xo), np.max(np.abs(xg - xo))
+    assert L.m2d_msi_lu_redo_count() > before
+
+
+@pytest.mark.parametrize("nd", [9, 5])
 def test_msi_more_rows_than_threads(nd):
     # ny > 1024: each thread owns two rows of the wavefront
     nx, ny = 9, 1100
