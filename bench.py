@@ -316,6 +316,24 @@ def run_ours(args):
     torch.cuda.synchronize()
     avg_ms = sum(a.elapsed_time(b) for a, b in durs) / len(durs)
     nit = int(nit_d.item())
+    # the same solve with the kernel's %globaltimer stamps: median duration
+    # of each phase (CTA 0's view), after the timed region
+    L.m2d_msi_solve_device_timed.argtypes = [ctypes.c_int] * 4 + [ctypes.c_double] + [ctypes.c_void_p] * 7
+    stamps = torch.zeros(7, dtype=torch.int64, device=f"cuda:{local}")
+    ph = []
+    with torch.cuda.stream(ks):
+        for k in range(8):
+            xk.zero_()
+            check(L.m2d_msi_solve_device_timed(5, sim.nx, sim.ny, 20, 1e-2, d_ap, d_bp, xk.data_ptr(),
+                                               work.data_ptr(), ks.cuda_stream, nit_d.data_ptr(),
+                                               stamps.data_ptr()))
+            ks.synchronize()
+            t = stamps.cpu().tolist()
+            if k >= 3:
+                ph.append([(t[q + 1] - t[q]) / 1e3 for q in range(6)])
+    names = ("factorisation", "initial_residual", "first_forward", "first_backward", "first_residual",
+             "remaining_iterations")
+    phases_us = {nm: sorted(col)[len(col) // 2] for nm, col in zip(names, zip(*ph))}
     alg = msi_algorithmic_bytes(5, N, nit)
     achieved = alg / (avg_ms / 1e3) / 1e9
     peak, peak_kind = peaks()
@@ -372,7 +390,7 @@ def run_ours(args):
                          "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind,
                          "traffic": traffic, "algorithmic_bytes_per_launch": alg,
-                         "launch_ms": avg_ms, "iterations_per_launch": nit},
+                         "launch_ms": avg_ms, "iterations_per_launch": nit, "phases_us": phases_us},
             "cpu_baseline": cpu,
             "batch": batch,
             "clocks": clk.summary(),
