@@ -362,106 +362,18 @@ __device__ __forceinline__ double residual_cell(const double *__restrict__ a, co
     return v;
 }
 
-// The cluster-wide pass after a sweep pair, by the CTA's own row groups
-// (wg0 .. wg0 + nwg - 1, the rows of its wavefront warps): x += z, then
-// r = A x - b.  z and r are wavefront-major, x, A and b cell-ordered, so
-// each warp works on tiles of 32 slots x 32 rows and transposes them
-// through shared memory (tile: 32 x 33 TS per warp): a line of z or r is
-// read or written whole, a row of x, A or b as 32 consecutive cells.
-// v^2 of every cell goes to v2 (cell order); the norm is then summed over
-// contiguous per-CTA slices of cells, thread t taking cells lo + t + 256 k in
-// order, the same slices as the helpers' initial residual.
-// Every row's sweep must be final (cluster barrier) before the call.
-template <int ND, typename TS>
-__device__ double cluster_residual_tiled(cg::cluster_group &cl, const double *__restrict__ a,
-                                         const double *__restrict__ b, double *x, const TS *z, TS *r,
-                                         int nx, int ny, int sw, int wg0, int nwg, TS *tile_all, double *v2,
-                                         double *red, double *part)
-{
-    const long long N = (long long)nx * ny;
-    const int C = (int)cl.num_blocks(), rank = (int)cl.block_rank();
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    TS *tile = tile_all + w * (32 * 33);
-    const int ntile = (sw + 31) / 32;
-    cl.sync();
-    // x += z
-    for (int u = w; u < nwg * ntile; u += kThreads / 32) {
-        const int g = wg0 + u / ntile, s0 = (u % ntile) * 32;
-        if (g * 32 >= ny) continue;
-#pragma unroll 4
-        for (int t = 0; t < 32; t++)
-            if (s0 + t < sw) tile[t * 33 + lane] = z[((long long)g * sw + s0 + t) * kLine + lane];
-        __syncwarp();
-        for (int l = 0; l < 32; l++) {
-            const int j = 32 * g + l, i = s0 - 2 * l + lane;
-            if (j < ny && i >= 0 && i < nx && s0 + lane < sw) {
-                const long long np = (long long)j * nx + i;
-                x[np] = (double)tile[lane * 33 + l] + x[np];
-            }
-        }
-        __syncwarp();
-    }
-    cl.sync();
-    // r = A x - b
-    for (int u = w; u < nwg * ntile; u += kThreads / 32) {
-        const int g = wg0 + u / ntile, s0 = (u % ntile) * 32;
-        if (g * 32 >= ny) continue;
-        for (int l = 0; l < 32; l++) {
-            const int j = 32 * g + l, i = s0 - 2 * l + lane;
-            TS rv = (TS)0;
-            if (j < ny && i >= 0 && i < nx && s0 + lane < sw) {
-                const long long np = (long long)j * nx + i;
-                const double v = residual_cell<ND>(a, b, x, np, i, j, nx, ny, N);
-                rv = (TS)v;
-                v2[np] = v * v;
-            }
-            tile[lane * 33 + l] = rv;
-        }
-        __syncwarp();
-#pragma unroll 4
-        for (int t = 0; t < 32; t++)
-            if (s0 + t < sw) r[((long long)g * sw + s0 + t) * kLine + lane] = tile[t * 33 + lane];
-        __syncwarp();
-    }
-    fence_async_global();   // the forward sweep reads r with bulk copies
-    cl.sync();              // every v^2 is in place
-    const long long per = (N + C - 1) / C;
-    const long long lo = per * rank, hi = (lo + per < N) ? lo + per : N;
-    double acc = 0.0;
-#pragma unroll 8
-    for (long long np = lo + threadIdx.x; np < hi; np += kThreads) acc = acc + v2[np];
-    red[threadIdx.x] = acc;
-    __syncthreads();
-    for (int s = kThreads / 2; s > 0; s >>= 1) {
-        if (threadIdx.x < s) red[threadIdx.x] = red[threadIdx.x] + red[threadIdx.x + s];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        double *p0 = cl.map_shared_rank(part, 0);
-        p0[rank] = red[0];
-    }
-    cl.sync();
-    if (rank == 0 && threadIdx.x == 0) {
-        double s = 0.0;
-        for (int c = 0; c < C; c++) s = s + part[c];
-        for (int c = 0; c < C; c++) cl.map_shared_rank(part, c)[kMaxCluster] = s;
-    }
-    cl.sync();
-    return part[kMaxCluster];
-}
-
 __device__ __forceinline__ void named_bar(unsigned id, unsigned count)
 {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
 }
 
-// The initial residual r = A x - b of this CTA's slice of cells, computed
-// by the nhelp helper warps (hw = 0..nhelp-1) while the wavefront warps
-// factorise.  The helpers run 256 virtual threads (virtual thread t takes
-// cells lo + t + 256 k, in that order) and a tree over their sums, the
-// slices and order of cluster_residual_tiled's norm.  The CTA's sum goes to
-// CTA 0's part[rank]; cluster_total combines the CTAs after the next
-// cluster barrier.
+// The initial residual r = A x - b of this CTA's slice, computed by the
+// nhelp helper warps (hw = 0..nhelp-1) while the wavefront warps factorise.
+// The helpers run the 256 threads of cluster_residual as virtual threads
+// (virtual thread t takes cells lo + t + 256 k, in that order) and the same
+// tree over their sums, so the norm is bitwise the one cluster_residual
+// gives.  The CTA's sum goes to CTA 0's part[rank]; cluster_total combines
+// the CTAs after the next cluster barrier.
 template <int ND, typename TS>
 __device__ void helper_residual(cg::cluster_group &cl, const double *__restrict__ a, const double *__restrict__ b,
                                 const double *x, TS *r, int nx, int ny, int sw, double *red, double *part,
@@ -502,6 +414,57 @@ __device__ void helper_residual(cg::cluster_group &cl, const double *__restrict_
 __device__ double cluster_total(cg::cluster_group &cl, double *part)
 {
     const int C = (int)cl.num_blocks(), rank = (int)cl.block_rank();
+    cl.sync();
+    if (rank == 0 && threadIdx.x == 0) {
+        double s = 0.0;
+        for (int c = 0; c < C; c++) s = s + part[c];
+        for (int c = 0; c < C; c++) cl.map_shared_rank(part, c)[kMaxCluster] = s;
+    }
+    cl.sync();
+    return part[kMaxCluster];
+}
+
+// Cluster-wide pass (this CTA takes a contiguous slice of cells): first
+// x += z when z (wavefront-major) is given, then r = A x - b stored
+// wavefront-major.  Returns the cluster-wide sum of r^2, identical in every
+// thread.  Starts with a cluster barrier: every row's sweep must be final.
+template <int ND, typename TS>
+__device__ double cluster_residual(cg::cluster_group &cl, const double *__restrict__ a,
+                                   const double *__restrict__ b, double *x, const TS *z, TS *r,
+                                   int nx, int ny, int sw, double *red, double *part)
+{
+    cl.sync();
+    const long long N = (long long)nx * ny;
+    const int C = (int)cl.num_blocks(), rank = (int)cl.block_rank();
+    const long long per = (N + C - 1) / C;
+    const long long lo = per * rank, hi = (lo + per < N) ? lo + per : N;
+    if (z) {
+#pragma unroll 8
+        for (long long np = lo + threadIdx.x; np < hi; np += kThreads) {
+            const int j = (int)((unsigned)np / (unsigned)nx), i = (int)np - j * nx;   // N < 2^31
+            x[np] = (double)z[skew_slot(i, j, sw)] + x[np];
+        }
+        cl.sync();
+    }
+    double acc = 0.0;
+#pragma unroll 8
+    for (long long np = lo + threadIdx.x; np < hi; np += kThreads) {
+        const int j = (int)((unsigned)np / (unsigned)nx), i = (int)np - j * nx;   // N < 2^31
+        const double v = residual_cell<ND>(a, b, x, np, i, j, nx, ny, N);
+        r[skew_slot(i, j, sw)] = (TS)v;
+        acc = acc + v * v;
+    }
+    fence_async_global();   // the forward sweep reads r with bulk copies
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = kThreads / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) red[threadIdx.x] = red[threadIdx.x] + red[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        double *p0 = cl.map_shared_rank(part, 0);
+        p0[rank] = red[0];
+    }
     cl.sync();
     if (rank == 0 && threadIdx.x == 0) {
         double s = 0.0;
@@ -910,8 +873,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
     // that no wavefront warp uses, so that their work does not take issue
     // slots or FP64 units from the recurrence
     static_assert(WPC >= 1 && WPC <= 3, "wavefront warps must leave a sub-partition for the helpers");
-    static_assert(WPC * NSTAGE * PMAX * kBlock >= (kThreads / 32) * 32 * 33,
-                  "the residual pass's tiles live in the staging blocks");
     const bool helper = (wl & 3) >= WPC;
     const int nhelp = (kThreads / 32 / 4) * (4 - WPC);
     const int hw = (wl >> 2) * (4 - WPC) + ((wl & 3) - WPC);
@@ -1146,10 +1107,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                 continue;
             }
         }
-        // the staging blocks are idle (every staged batch consumed) and the
-        // wavefront-major copy of A is no longer read: tiles and v^2 go there
-        rr = cluster_residual_tiled<ND, TS>(cl, a, S.b, x, wp, rp, nx, ny, SW, rank * WPC, WPC, stage_mem,
-                                            reinterpret_cast<double *>(asp), red, part);
+        rr = cluster_residual<ND, TS>(cl, a, S.b, x, wp, rp, nx, ny, SW, red, part);
         if (nit == 1) stamp(L, rank, 5);
         if (sqrt(rr) < gammarp) break;
         if (nit == cap) {
