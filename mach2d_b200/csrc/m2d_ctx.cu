@@ -451,7 +451,7 @@ static int issue_p_cycle(m2d_ctx *x, const Params &q, cudaStream_t s)
     KL(launch_p_ro_correction(f, 1, 1, s), 1);
     KL(launch_density_at_faces(f, x->c.beta, s), 1);
     RedArgs r = red(x, RED_MAXABS_ALL); r.x = f.pl;
-    KL(launch_reduce(r, x->part, x->dsc + S_MAXPL, s), 2);
+    KL(launch_reduce(r, x->part, x->dsc + S_MAXPL, s), 1);
     return M2D_OK;
 }
 
@@ -509,7 +509,7 @@ static int issue_iteration(m2d_ctx *x, bool capture, int *itp_used_out)
     if (c.ktm == 1) TRY(mixture_properties(x, true));
     {
         RedArgs r = red(x, RED_SUM_REAL); r.x = f.p;
-        KL(launch_reduce(r, x->part, x->dsc + S_PSUM, st), 2);
+        KL(launch_reduce(r, x->part, x->dsc + S_PSUM, st), 1);
     }
     KL(launch_g(f, q.Rg, st), 1);
     if (capture) {
@@ -535,13 +535,13 @@ static int issue_iteration(m2d_ctx *x, bool capture, int *itp_used_out)
         }
         {
             RedArgs r = red(x, RED_NORM_L1_9D); r.a = f.au; r.b = f.bu; r.x = f.u;
-            KL(launch_reduce(r, x->part, x->dsc + S_NU_A, st), 2);
+            KL(launch_reduce(r, x->part, x->dsc + S_NU_A, st), 1);
             r.kind = RED_SUM_ABS_B;
-            KL(launch_reduce(r, x->part, x->dsc + S_NU_B, st), 2);
+            KL(launch_reduce(r, x->part, x->dsc + S_NU_B, st), 1);
             r = red(x, RED_NORM_L1_9D); r.a = f.av; r.b = f.bv; r.x = f.v;
-            KL(launch_reduce(r, x->part, x->dsc + S_NV_A, st), 2);
+            KL(launch_reduce(r, x->part, x->dsc + S_NV_A, st), 1);
             r.kind = RED_SUM_ABS_B;
-            KL(launch_reduce(r, x->part, x->dsc + S_NV_B, st), 2);
+            KL(launch_reduce(r, x->part, x->dsc + S_NV_B, st), 1);
         }
         KL(launch_velocities_at_internal_faces(f, q.dt, st, q.dtp), 1);
         KL(launch_velocities_at_boundary_faces(f, c.modvis, st), 1);
@@ -568,7 +568,7 @@ static int issue_iteration(m2d_ctx *x, bool capture, int *itp_used_out)
         }
         {
             RedArgs r = red(x, RED_NORM_L1_5D); r.a = f.ap; r.b = f.bp; r.x = f.pl;
-            KL(launch_reduce(r, x->part, x->dsc + S_NP, st), 2);
+            KL(launch_reduce(r, x->part, x->dsc + S_NP, st), 1);
         }
         KL(launch_uv_nodes_correction(f, st), 1);
         KL(launch_extrapolate_uv(f, c.modvis, st), 1);
@@ -577,7 +577,7 @@ static int issue_iteration(m2d_ctx *x, bool capture, int *itp_used_out)
         RedArgs r = red(x, RED_MASS);
         r.rp = f.rp; r.re = f.re; r.rn = f.rn; r.Jp = f.Jp; r.ro = f.ro; r.roa = f.roa;
         r.ron = f.ron; r.roe = f.roe; r.Uce = f.Uce; r.Vcn = f.Vcn; r.dt = q.dt; r.dtp = q.dtp;
-        KL(launch_reduce(r, x->part, x->dsc + S_RMASS, st), 2);
+        KL(launch_reduce(r, x->part, x->dsc + S_RMASS, st), 1);
     }
     // T from total-enthalpy conservation for Euler with constant properties
     // only (src/mach2d_main.f90:357-359); otherwise the energy equation
@@ -592,21 +592,21 @@ static int issue_iteration(m2d_ctx *x, bool capture, int *itp_used_out)
         int rc = solve9(x, st, 1, a, b, v, is, rs);
         if (rc) return rc;
         RedArgs r = red(x, RED_NORM_L1_9D); r.a = f.at; r.b = f.bt; r.x = f.T;
-        KL(launch_reduce(r, x->part, x->dsc + S_NT_A, st), 2);
+        KL(launch_reduce(r, x->part, x->dsc + S_NT_A, st), 1);
         r.kind = RED_SUM_ABS_B;
-        KL(launch_reduce(r, x->part, x->dsc + S_NT_B, st), 2);
+        KL(launch_reduce(r, x->part, x->dsc + S_NT_B, st), 1);
     }
     KL(launch_density_at_nodes(f, q.Rg, st), 1);
     KL(launch_density_at_faces(f, c.beta, st), 1);
     if (c.dtmodel == 1) {
         RedArgs r = red(x, RED_MEAN_CC_9D); r.a = f.au;
-        KL(launch_reduce(r, x->part, x->dsc + S_CC_U, st), 2);
+        KL(launch_reduce(r, x->part, x->dsc + S_CC_U, st), 1);
         r.a = f.av;
-        KL(launch_reduce(r, x->part, x->dsc + S_CC_V, st), 2);
+        KL(launch_reduce(r, x->part, x->dsc + S_CC_V, st), 1);
         r.a = f.at;
-        KL(launch_reduce(r, x->part, x->dsc + S_CC_T, st), 2);
+        KL(launch_reduce(r, x->part, x->dsc + S_CC_T, st), 1);
         r = red(x, RED_MEAN_CC_5D); r.a = f.ap;
-        KL(launch_reduce(r, x->part, x->dsc + S_CC_P, st), 2);
+        KL(launch_reduce(r, x->part, x->dsc + S_CC_P, st), 1);
     }
     KL(launch_mass_flow_thrust(f, x->dsc + S_FMI, st), 1);
     if (capture) {

@@ -12,7 +12,8 @@ namespace m2d {
 
 static const int kParts = 296;     // 2 x 148 SMs
 static const int kThreads = 256;
-int red_parts() { return kParts; }
+// per-block partials, then one word for the count of finished blocks
+int red_parts() { return kParts + 1; }
 
 #define A9(a, np, k) (a)[(long long)((k) - 1) * N + (np)]
 
@@ -102,7 +103,11 @@ __device__ __forceinline__ double block_reduce(double v, int c)
     return sh[0];
 }
 
-__global__ void __launch_bounds__(kThreads) k_reduce_pass1(RedArgs r, double *part)
+// One launch: every block reduces its share into part[block]; the last
+// block to finish (a counter in part[kParts], back to zero afterwards)
+// combines the kParts partials in index order with the same tree, so the
+// result does not depend on which block finishes last.
+__global__ void __launch_bounds__(kThreads) k_reduce(RedArgs r, double *part, double *out)
 {
     const int c = combine_of(r.kind);
     double acc = ident(c);
@@ -119,26 +124,29 @@ __global__ void __launch_bounds__(kThreads) k_reduce_pass1(RedArgs r, double *pa
         }
     }
     double s = block_reduce(acc, c);
-    if (threadIdx.x == 0) part[blockIdx.x] = s;
-}
-
-__global__ void __launch_bounds__(kThreads) k_reduce_pass2(int kind, int nx, int ny, const double *part, double *out)
-{
-    const int c = combine_of(kind);
-    double acc = ident(c);
-    for (int k = threadIdx.x; k < kParts; k += kThreads) acc = comb(c, acc, part[k]);
-    double s = block_reduce(acc, c);
+    __shared__ bool last;
     if (threadIdx.x == 0) {
-        if (kind == RED_MEAN_CC_9D || kind == RED_MEAN_CC_5D) s = s / (double)((nx - 2) * (ny - 2));
-        if (kind == RED_DT0) s = s * 0.25;
+        part[blockIdx.x] = s;
+        __threadfence();
+        last = atomicAdd(reinterpret_cast<unsigned *>(part + kParts), 1u) == (unsigned)(kParts - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    acc = ident(c);
+    for (int k = threadIdx.x; k < kParts; k += kThreads) acc = comb(c, acc, __ldcg(part + k));
+    s = block_reduce(acc, c);
+    if (threadIdx.x == 0) {
+        if (r.kind == RED_MEAN_CC_9D || r.kind == RED_MEAN_CC_5D) s = s / (double)((r.nx - 2) * (r.ny - 2));
+        if (r.kind == RED_DT0) s = s * 0.25;
         *out = s;
+        *reinterpret_cast<unsigned *>(part + kParts) = 0u;
     }
 }
 
 cudaError_t launch_reduce(const RedArgs &r, double *part, double *out, cudaStream_t st)
 {
-    k_reduce_pass1<<<kParts, kThreads, 0, st>>>(r, part);
-    k_reduce_pass2<<<1, kThreads, 0, st>>>(r.kind, r.nx, r.ny, part, out);
+    k_reduce<<<kParts, kThreads, 0, st>>>(r, part, out);
     return cudaGetLastError();
 }
 
