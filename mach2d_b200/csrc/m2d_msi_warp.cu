@@ -25,10 +25,19 @@
 //     global-memory latency sits on the recurrence;
 //   * divisions on the recurrence use the divisor's correctly rounded
 //     reciprocal and two FMA corrections (Markstein's method), which yields
-//     the IEEE quotient whenever both operands lie in [2^-500, 2^500] (or the
-//     dividend is zero).  A batch in which any cell falls outside that range
-//     is recomputed with IEEE division before it is published;
-//   * the backward sweep writes the correction z; x += z and the residual
+//     the IEEE quotient whenever both operands lie in [2^-500, 2^500) (or the
+//     dividend is zero).  In the forward sweep a batch in which any cell
+//     falls outside that range is recomputed with IEEE division before it is
+//     published.  The factorisation tests nothing on the recurrence: the
+//     helper warps (those on the SM sub-partitions no wavefront warp uses)
+//     refactorise every cell with IEEE division from its stored inputs while
+//     the first sweeps run, and any difference repeats the factorisation
+//     with IEEE division before x changes;
+//   * a step is software-pipelined (critical shuffles first, then the
+//     previous step's predicated stores, then the next step's loads), so no
+//     branch separates two steps;
+//   * the helper warps also compute the initial residual during the
+//     factorisation; after each sweep pair x += z and the residual
 //     r = A x - b run as cluster-wide passes over all threads, as does the
 //     L2 norm of the stopping test (partial sums combined in a fixed order in
 //     CTA 0 and broadcast, so the stopping decision is deterministic).
