@@ -7,7 +7,7 @@
  *  1. Drop-ins for the reference's routines.  Each entry point takes the
  *     reference routine's argument list in the reference's order, with HOST
  *     pointers and every argument by reference, exactly what a Fortran
- *     `bind(C)` interface passes (see INTEGRATION.md).  Arrays use the
+ *     `bind(C)` interface passes.  Arrays use the
  *     reference layout: nx, ny count the ghost ring, cell (i,j) 1-based sits
  *     at offset nx*(j-1)+i-1, a coefficient matrix a(nx*ny,k) is stored
  *     diagonal after diagonal (9-diagonal order SW,S,SE,W,P,E,NW,N,NE;
@@ -98,6 +98,20 @@ int m2d_msi_solve_device_timed(int nd, int nx, int ny, int nitm, double tol,
  * reference. */
 long long m2d_msi_lu_redo_count(void);
 
+/* Test hook for failure detection, no counterpart in the reference (whose
+ * only failure check is the NaN test of src/mach2d_main.f90:424-436).  Every
+ * device-side wait of the MSI cluster kernel (warp-to-warp hand-offs, staged
+ * copies) and of the tcgen05 convolution is bounded by 4 s of %globaltimer
+ * time; when one runs out the kernel records it, stops waiting, runs to its
+ * end and the call returns M2D_ERR_TIMEOUT -- no trap, the context stays
+ * usable.  kernel = 1 (MSI cluster kernel) or 2 (tcgen05 convolution) makes
+ * the next launches of that kernel wait once more, on an mbarrier that
+ * nothing completes, bounded by limit_s seconds (<= 10), so that this wait
+ * runs out: the MSI solve then returns M2D_ERR_TIMEOUT from the host
+ * drop-ins and m2d_iterate, the convolution through m2d_unet_status.
+ * kernel = 0 (or limit_s = 0) switches the hook off. */
+int m2d_test_wait_hook(int kernel, double limit_s);
+
 /* No counterpart in the reference ("MSI_MIXED" in solvers_init).  The same
  * MSI iteration with the factorisation and both sweeps in FP32: the residual
  * r = A x - b, x, the norm and the stopping test |r| < tol |r0| stay FP64, so
@@ -122,10 +136,16 @@ int m2d_msi_solve_device_mixed(int nd, int nx, int ny, int nitm, double tol, con
  * Allocates nothing: the workspace is a 12 MiB array in the library's own
  * device memory, held on every GPU that loads the library until exit.  Limit:
  * nx*ny <= m2d_msi_noalloc_max_cells(nd) (157286 cells for nd = 9, 196607 for
- * nd = 5); larger grids return M2D_ERR_TOO_LARGE.  The first call on a device
- * looks up the array's device address (cudaGetSymbolAddress), so make it
- * before any stream capture.  All calls share the array: calls that overlap
- * on the GPU race and must be serialised by the caller. */
+ * nd = 5); larger grids return M2D_ERR_TOO_LARGE.  Every call looks up the
+ * array's device address on the current device (cudaGetSymbolAddress), so a
+ * device reset between calls leaves no stale address; the first call on a
+ * device also loads the device code there, so make it before any stream
+ * capture.  The fast cluster kernel runs only while its wavefront-major
+ * layout fits in the array (32*ceil(ny/32) * (nx + 62) <= 74898 for nd = 9,
+ * <= 104857 for nd = 5); other grids under the cell limit, 514 x 258 with
+ * nd = 9 among them, run the bitwise-equal but slower one-CTA kernel.  All
+ * calls share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller. */
 long m2d_msi_noalloc_max_cells(int nd);
 int m2d_msi_solve_device_noalloc(int nd, int nx, int ny, int nitm, double tol,
                                  const double *d_a, const double *d_b, double *d_x,
@@ -377,6 +397,15 @@ typedef struct m2d_case {
     int nan_policy;                         /* max() with the NaN of at = 0: 0 drop, 1 propagate */
     int ktm;                                /* 0 CONSTANT, 1 MIXTURE (thermophysical_initialization) */
     m2d_mixture mix;                        /* ktm = 1: the gas mixture (m2d_mixture_init) */
+    int modtur;                             /* 1 (with modvis = 1): Baldwin-Lomax eddy viscosity
+                                               (src/equations/blomax.f90:285-490), which the
+                                               reference compiles but never calls, evaluated at the
+                                               start of each outer iteration from the previous
+                                               flow and added to the transport coefficients:
+                                               mu + mu_t and k + cp mu_t / prt at the nodes, the
+                                               arithmetic face means of mu_t and cp mu_t at the
+                                               east and north faces, the wall faces laminar */
+    double prt;                             /* turbulent Prandtl number (modtur = 1) */
 } m2d_case;
 
 typedef struct m2d_report {
@@ -484,8 +513,9 @@ int m2d_unet_adam(m2d_unet *net, float lr, float beta1, float beta2, float eps, 
  * kernel); 1 (default) or 2 every one whose image has an even height and a
  * width that is a multiple of 128 (the others use the mma.sync kernel) */
 int m2d_unet_set_tensor_path(int mode);
-/* synchronises; *flags = device error word (2: a tensor-core wait ran out,
- * returned as M2D_ERR_TIMEOUT) */
+/* synchronises; *flags = device error word (8: a tensor-core kernel's
+ * bounded wait ran out, returned as M2D_ERR_TIMEOUT); the word is cleared
+ * after it is read */
 int m2d_unet_status(m2d_unet *net, int *flags);
 
 /* p' system <-> images.  d_a: 5 planes (S, W, P, E, N), d_stats: 16 doubles.

@@ -206,4 +206,46 @@ cudaError_t launch_blomax_fictitious(int nx, int ny, double *phi, cudaStream_t s
     return cudaGetLastError();
 }
 
+// One thread per cell; the arithmetic and its order are those of the
+// oracle's restatement, so the results are bitwise equal.
+__global__ void k_add_eddy(int nx, int ny, int ktm, double mu, double kappa, double prt,
+                           const double *__restrict__ vtp, const double *__restrict__ cp, double *vlp,
+                           double *vle, double *vln, double *kp, double *ke, double *kn)
+{
+    const long long np = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (np >= (long long)nx * ny) return;
+    const int j = (int)(np / nx) + 1, i = (int)(np - (long long)(j - 1) * nx) + 1;
+    const double mp = ktm ? vlp[np] : mu, me = ktm ? vle[np] : mu, mn = ktm ? vln[np] : mu;
+    const double kpl = ktm ? kp[np] : kappa, kel = ktm ? ke[np] : kappa, knl = ktm ? kn[np] : kappa;
+    const double tp = cp[np] * vtp[np];
+    vlp[np] = mp + vtp[np];
+    kp[np] = kpl + tp / prt;
+    if (i < nx) {
+        const double te = cp[np + 1] * vtp[np + 1];
+        vle[np] = me + 0.5 * (vtp[np] + vtp[np + 1]);
+        ke[np] = kel + 0.5 * (tp + te) / prt;
+    } else {
+        vle[np] = me;
+        ke[np] = kel;
+    }
+    if (j < ny - 1) {
+        const double tn = cp[np + nx] * vtp[np + nx];
+        vln[np] = mn + 0.5 * (vtp[np] + vtp[np + nx]);
+        kn[np] = knl + 0.5 * (tp + tn) / prt;
+    } else {
+        vln[np] = mn;
+        kn[np] = knl;
+    }
+}
+
+cudaError_t launch_add_eddy(int nx, int ny, int ktm, double mu, double kappa, double prt, const double *vtp,
+                            const double *cp, double *vlp, double *vle, double *vln, double *kp, double *ke,
+                            double *kn, cudaStream_t st)
+{
+    const long long N = (long long)nx * ny;
+    k_add_eddy<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(nx, ny, ktm, mu, kappa, prt, vtp, cp, vlp, vle, vln, kp,
+                                                           ke, kn);
+    return cudaGetLastError();
+}
+
 }  // namespace m2d

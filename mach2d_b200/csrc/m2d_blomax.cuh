@@ -17,5 +17,13 @@ cudaError_t launch_blomax(int nx, int ny, const BlConst &c, const double *x, con
                           const double *u, const double *v, double *vtp, cudaStream_t st);
 // get_eddy_viscosity_fictitious (blomax.f90:397-490)
 cudaError_t launch_blomax_fictitious(int nx, int ny, double *phi, cudaStream_t st);
+// the eddy viscosity into the transport coefficients (no reference call site:
+// blomax.f90 is never called): mu + mu_t and k + cp mu_t / prt at the nodes,
+// arithmetic face means of mu_t and cp mu_t at the east and north faces, the
+// wall faces (north of the last real row) and the outermost faces laminar;
+// ktm = 0 takes the laminar values from mu and kappa, ktm = 1 from the arrays
+cudaError_t launch_add_eddy(int nx, int ny, int ktm, double mu, double kappa, double prt, const double *vtp,
+                            const double *cp, double *vlp, double *vle, double *vln, double *kp, double *ke,
+                            double *kn, cudaStream_t st);
 
 }  // namespace m2d

@@ -145,6 +145,7 @@ int msi_solve_host(int nd, const int *nx, const int *ny, const int *nitm, const 
     cudaMemcpy(&hv[0], misc, sizeof(int), cudaMemcpyDeviceToHost);
     cudaMemcpy(&hv[1], misc + 3, sizeof(int), cudaMemcpyDeviceToHost);
     if (nit_out) *nit_out = hv[0];
+    if (hv[1] & ERR_SPIN_TIMEOUT) return fail(ST_TIMEOUT, "msi: a bounded device-side wait ran out");
     if (hv[1] & ERR_WAIT_TIMEOUT) return fail(ST_TIMEOUT, "msi: unbounded iteration reached its cap");
     if (hv[1] & ERR_NONFINITE_PIVOT) return fail(7, "msi: zero or non-finite pivot in the factorisation");
     return ST_OK;
@@ -167,6 +168,16 @@ int reduce_host(RedArgs r, double *out)
 extern "C" {
 
 int m2d_msi_max_ny(void) { return m2d::msi_max_ny(); }
+
+int m2d_test_wait_hook(int kernel, double limit_s)
+{
+    if (kernel < 0 || kernel > 2 || !(limit_s >= 0.0) || limit_s > 10.0)
+        return fail(ST_ARG, "m2d_test_wait_hook: kernel 0..2, limit 0..10 s");
+    const unsigned long long ns = (unsigned long long)(limit_s * 1e9);
+    m2d::set_msi_wait_hook(kernel == 1 ? ns : 0ull);
+    m2d::set_conv_wait_hook(kernel == 2 ? ns : 0ull);
+    return ST_OK;
+}
 
 int m2d_msi9_solve(const int *nx, const int *ny, const int *nitm, const double *tol,
                    const double *a, const double *b, double *x)

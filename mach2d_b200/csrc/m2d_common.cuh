@@ -46,9 +46,16 @@ enum {
 // device-side error word bits (written by kernels, read by the host)
 enum {
     ERR_NONFINITE_PIVOT = 1,
-    ERR_WAIT_TIMEOUT = 2,
+    ERR_WAIT_TIMEOUT = 2,      // an unbounded MSI iteration (nitm <= 0) reached its cap
     ERR_BAD_SHAPE = 4,
+    ERR_SPIN_TIMEOUT = 8,      // a bounded device-side wait (mbarrier, hand-off) ran out
 };
+
+// Test hooks (m2d_test_wait_hook): the next launches of the MSI cluster
+// kernel / the tcgen05 convolution make one extra wait, bounded by ns
+// nanoseconds, on an mbarrier that nothing completes (0 switches it off).
+void set_msi_wait_hook(unsigned long long ns);
+void set_conv_wait_hook(unsigned long long ns);
 
 }  // namespace m2d
 

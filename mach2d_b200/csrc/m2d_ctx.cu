@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include "m2d_blomax.cuh"
 #include "m2d_fields.cuh"
 #include "m2d_grid.cuh"
 #include "m2d_setup.h"
@@ -202,6 +203,8 @@ extern "C" int m2d_create(const m2d_case *c, int device, m2d_ctx **out)
     if (c->nxr < 3 || c->nyr < 3) return ctx_fail(M2D_ERR_ARG, "m2d_create: need at least 3x3 real volumes");
     if (c->solver != 1 && c->nyr + 2 > msi_max_ny()) return ctx_fail(M2D_ERR_TOO_LARGE, "m2d_create: ny exceeds m2d_msi_max_ny()");
     if (c->ktm != 0 && c->ktm != 1) return ctx_fail(M2D_ERR_ARG, "m2d_create: ktm must be 0 (CONSTANT) or 1 (MIXTURE)");
+    if (c->modtur != 0 && !(c->modtur == 1 && c->modvis == 1 && c->prt > 0.0 && c->nyr >= 3))
+        return ctx_fail(M2D_ERR_ARG, "m2d_create: modtur = 1 needs modvis = 1 and prt > 0");
     if (c->ktm == 1 && (c->mix.ngs < 1 || c->mix.ngs > M2D_MAX_SPECIES || !(c->mix.Rg > 0.0)))
         return ctx_fail(M2D_ERR_ARG, "m2d_create: ktm = 1 needs a mixture from m2d_mixture_init");
     HostInstance h;
@@ -507,6 +510,16 @@ static int issue_iteration(m2d_ctx *x, bool capture, int *itp_used_out)
     KL(launch_backup(f, st), 1);
     KL(launch_inlet_update(f, q, st), 1);
     if (c.ktm == 1) TRY(mixture_properties(x, true));
+    if (c.modvis == 1 && c.modtur == 1) {
+        // Baldwin-Lomax eddy viscosity from the previous iteration's flow
+        // (blomax.f90:285-490) added to the laminar transport coefficients
+        const BlConst blc;
+        KL(launch_blomax(x->nx, x->ny, blc, f.x, f.y, f.xp, f.yp, f.xk, f.yk, f.Jp, f.Jn, f.vln, f.ro, f.ron, f.u,
+                         f.v, f.vtp, st), 1);
+        KL(launch_blomax_fictitious(x->nx, x->ny, f.vtp, st), 1);
+        KL(launch_add_eddy(x->nx, x->ny, c.ktm, c.mu, c.kappa, c.prt, f.vtp, f.cp, f.vlp, f.vle, f.vln, f.kp, f.ke,
+                           f.kn, st), 1);
+    }
     {
         RedArgs r = red(x, RED_SUM_REAL); r.x = f.p;
         KL(launch_reduce(r, x->part, x->dsc + S_PSUM, st), 1);
@@ -707,6 +720,7 @@ extern "C" int m2d_iterate(m2d_ctx *x, m2d_report *rep)
         rep->rmass = x->rmass; rep->fmi = hs[S_FMI]; rep->fme = hs[S_FME]; rep->Fd = hs[S_FD];
         rep->itp_used = itp_used;
     }
+    if (x->hint[I_ERR] & ERR_SPIN_TIMEOUT) return ctx_fail(M2D_ERR_TIMEOUT, "m2d_iterate: a bounded device-side wait ran out");
     if (x->hint[I_ERR] & ERR_WAIT_TIMEOUT) return ctx_fail(M2D_ERR_TIMEOUT, "m2d_iterate: MSI iteration cap reached");
     if (std::isnan(x->norm)) return ctx_fail(M2D_ERR_NAN, "m2d_iterate: NaN detected");
     if (x->normpl < c.tolt && x->it_stop < 0) x->it_stop = it * 2;

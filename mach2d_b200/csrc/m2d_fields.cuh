@@ -20,6 +20,7 @@ struct Fields {
     double *cp, *vlp, *vle, *vln, *kp, *ke, *kn;
     double *cup, *sup, *cvp, *svp, *bu, *bv, *bt, *bp, *pl;
     double *due, *dve, *dun, *dvn, *de, *dn;
+    double *vtp;            // Baldwin-Lomax eddy viscosity at the nodes (modtur = 1)
     double *au, *av, *at;   // 9N each
     double *ap;             // 5N
     // boundary strips

@@ -14,8 +14,8 @@
 //     another CTA), completing on an mbarrier the consumer waits on; the
 //     consumer frees ring slots by arriving on the producer's mbarriers.  No
 //     warp waits for anything but its two neighbours, and every wait is
-//     bounded (on timeout the kernel records ERR_WAIT_TIMEOUT and runs to its
-//     end);
+//     bounded in %globaltimer time (on timeout the kernel records
+//     ERR_SPIN_TIMEOUT and runs to its end);
 //   * A (after a transposing pre-pass, k_skew_a), the factors, the residual
 //     and the sweep results live in "wavefront-major" planes: the 32 cells a
 //     warp touches in one step are one contiguous 256-byte line, so one batch
@@ -64,7 +64,7 @@ constexpr int kBlock = kLag * kLine;   // doubles of one plane for one batch (4 
 constexpr int kSlots = kRing / kLag;    // ring slots, one batch each
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kMaxIterUnbounded = 10000;
-constexpr long long kBarSpinLimit = 1LL << 22;
+constexpr unsigned long long kWaitLimitNs = 4000000000ull;   // bound of every wait (4 s of %globaltimer)
 }
 
 #define PL(p, k, np) (p)[(long long)((k) - 1) * N + (np)]
@@ -229,16 +229,29 @@ __device__ __forceinline__ void st_cluster(unsigned addr, double v)
 {
     asm volatile("st.shared::cluster.f64 [%0], %1;" ::"r"(addr), "d"(v));
 }
+__device__ __forceinline__ unsigned long long gtimer()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// true once phase `parity` of the mbarrier has completed; false when
+// limit_ns of %globaltimer time passed first
+__device__ __forceinline__ bool mbar_wait_for(unsigned long long *bar, unsigned parity, unsigned long long limit_ns)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = gtimer();
+    for (;;) {
+        for (int k = 0; k < 32; k++)
+            if (mbar_try_wait(bar, parity)) return true;
+        if (gtimer() - t0 > limit_ns) return false;
+    }
+}
 // all lanes: bounded wait for the completion of phase `parity` (after an
 // earlier timeout the warp no longer waits at all)
 __device__ __forceinline__ void mbar_wait(unsigned long long *bar, unsigned parity, bool &timed_out)
 {
-    if (!timed_out) {
-        long long k = 0;
-        while (!mbar_try_wait(bar, parity)) {
-            if (++k > kBarSpinLimit) { timed_out = true; break; }
-        }
-    }
+    if (!timed_out && !mbar_wait_for(bar, parity, kWaitLimitNs)) timed_out = true;
     __syncwarp();
 }
 __device__ __forceinline__ void bulk_s2s(unsigned dst, const void *src, unsigned bytes, unsigned bar)
@@ -294,10 +307,7 @@ __device__ __forceinline__ int stage_wait(Stager<TS, NSTAGE, PMAX> &st, bool &ti
 {
     const int q = st.consumed % NSTAGE;
     const unsigned parity = (unsigned)(st.consumed / NSTAGE) & 1u;
-    long long k = 0;
-    while (!mbar_try_wait(&st.bar[q], parity)) {
-        if (++k > kBarSpinLimit) { timed_out = true; break; }
-    }
+    if (!mbar_wait_for(&st.bar[q], parity, kWaitLimitNs)) timed_out = true;
     __syncwarp();
     st.consumed++;
     return st.block(q);
@@ -692,6 +702,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
     __shared__ unsigned long long full_up[WPC][kSlots], empty_up[WPC][kSlots];
     __shared__ unsigned long long full_dn[WPC][kSlots], empty_dn[WPC][kSlots];
     __shared__ unsigned long long stage_bar[WPC][NSTAGE];
+    __shared__ unsigned long long idle_bar;       // nothing ever arrives on it (test hook)
     __shared__ unsigned vbad;                     // a factor differs from its IEEE value (helpers)
     __shared__ double red[kThreads];
     __shared__ double part[kMaxCluster + 1];
@@ -732,7 +743,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
     const long long wbase = line0 * kLine + lane;
 #define SK(p, s) (p)[wbase + (long long)(s) * kLine]
 
-    if (threadIdx.x == 0) vbad = 0u;
+    if (threadIdx.x == 0) {
+        vbad = 0u;
+        mbar_init(&idle_bar, 1);
+    }
     if (threadIdx.x < WPC) {
         for (int q = 0; q < kSlots; q++) {
             mbar_init(&full_up[threadIdx.x][q], 1); mbar_init(&empty_up[threadIdx.x][q], 1);
@@ -768,7 +782,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
         up_empty_dst = cluster_addr(&empty_up[pw][0], pr);
     }
     cl.sync();   // mbarriers initialised before any use; A staged by k_skew_a
-    bool bad_pivot = false, timed_out = false;
+    bool bad_pivot = false, timed_out = false, hook_ran_out = false;
     int up_base = 0, dn_base = 0;       // batches sent so far on each channel
     stamp(L, rank, 0);
 
@@ -914,6 +928,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
     double rr = rr0;
     for (;;) {
         nit = nit + 1;
+        // test hook: wavefront warp 0 waits, bounded by L.hook_ns, on a
+        // barrier that nothing completes, then goes on as usual (its
+        // neighbours' own waits are bounded far above that, so every real
+        // hand-off still completes and no copy is left in flight)
+        if (L.hook_ns && nit == 1 && rank == 0 && wl == 0) {
+            if (!mbar_wait_for(&idle_bar, 0u, L.hook_ns)) hook_ran_out = true;
+            __syncwarp();
+        }
         // forward: L w = -r.  Staged planes {r, dl1..dlNL, 1/dl1}; step kk of
         // a batch is line kk of its block
         if (front) {
@@ -1131,7 +1153,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
         bool again = false;
         while (st.consumed < st.issued) (void)stage_wait(st, again);
     }
-    if (timed_out && L.err) atomicOr(L.err, ERR_WAIT_TIMEOUT);
+    if ((timed_out || hook_ran_out) && L.err) atomicOr(L.err, ERR_SPIN_TIMEOUT);
     if (rank == 0 && threadIdx.x == 0) {
         if (S.nit) *S.nit = nit;
         if (S.rr) { S.rr[0] = rr0; S.rr[1] = rr; }
@@ -1216,8 +1238,14 @@ static cudaError_t launch_nd(const MsiLaunch &L, int nsys, cudaStream_t st, bool
     return launch_cluster<ND, 2, 2, TS>(L, nsys, st, done);
 }
 
-cudaError_t launch_msi_warp(int nd, const MsiLaunch &L, int nsys, cudaStream_t st)
+// m2d_test_wait_hook's setting for the cluster kernel (0: off)
+static unsigned long long g_msi_hook_ns = 0;
+void set_msi_wait_hook(unsigned long long ns) { g_msi_hook_ns = ns; }
+
+cudaError_t launch_msi_warp(int nd, const MsiLaunch &L0, int nsys, cudaStream_t st)
 {
+    MsiLaunch L = L0;
+    L.hook_ns = g_msi_hook_ns;
     bool done = false;
     cudaError_t e;
     if (L.prec == 1)
@@ -1225,7 +1253,7 @@ cudaError_t launch_msi_warp(int nd, const MsiLaunch &L, int nsys, cudaStream_t s
     else
         e = nd == 9 ? launch_nd<9, double>(L, nsys, st, &done) : launch_nd<5, double>(L, nsys, st, &done);
     if (e != cudaSuccess || done) return e;
-    return launch_msi_generic(nd, L, nsys, st);
+    return launch_msi_generic(nd, L0, nsys, st);
 }
 
 }  // namespace m2d

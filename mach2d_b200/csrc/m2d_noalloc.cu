@@ -11,27 +11,30 @@
 // The array is a file-scope __device__ variable of kNoallocScratchDoubles
 // doubles (12 MiB): every GPU that loads the library holds it until the
 // process exits.  Host code cannot pass the symbol itself to a kernel (on the
-// host it names a host-side stand-in, not a device address), so the first
-// call on each device, with that device current, resolves the device address
-// with cudaGetSymbolAddress and caches it; make that first call before any
-// stream capture.  All calls on a device share the one array and it keeps
-// the last call's contents: the solver writes every scratch word before it
-// reads it (factors, residual, norms), so nothing needs clearing, but calls
-// that overlap on the GPU (two streams, or two host threads) race on it and
-// must be serialised by the caller.
-#include <mutex>
+// host it names a host-side stand-in, not a device address), so every call,
+// with the caller's device current, looks up the device address with
+// cudaGetSymbolAddress and passes that pointer on.  The first call on a
+// device also loads the library's device code there, so make it before any
+// stream capture.  Because the address is looked up again on every call, a
+// device reset between two calls (which reloads the device code, possibly at
+// another address) does not leave a stale pointer behind.  All calls on a
+// device share the one array and it keeps the last call's contents: the
+// solver writes every scratch word before it reads it (factors, residual,
+// norms), so nothing needs clearing, but calls that overlap on the GPU (two
+// streams, or two host threads) race on it and must be serialised by the
+// caller.  The cluster kernel runs only while its wavefront-major layout fits
+// in the array, that is while 32*ceil(ny/32) * (nx + 62) is at most 74,898
+// (9 diagonals) or 104,857 (5 diagonals); otherwise the one-CTA kernel,
+// bitwise equal but slower, runs.  At 514 x 258 (512 x 256 real cells) the
+// 9-diagonal solve therefore takes the one-CTA kernel.
 #include "m2d_solvers.cuh"
 #include "../../include/mach2d_b200.h"
 
 namespace {
 
 const long kNoallocScratchDoubles = 1572864;   // 12 MiB
-const int kMaxDevices = 64;
 
 __device__ __align__(256) double g_msi_scratch[kNoallocScratchDoubles];
-
-std::mutex g_mutex;
-double *g_scratch_addr[kMaxDevices] = {nullptr};
 
 }  // namespace
 
@@ -67,30 +70,15 @@ extern "C" int m2d_msi_solve_device_noalloc(int nd, int nx, int ny, int nitm, do
             : "msi_solve_device_noalloc: nx*ny exceeds the maximum of 196607 cells for the 5-diagonal solve");
         return M2D_ERR_TOO_LARGE;
     }
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) {
-        m2d_set_last_error(e, "cudaGetDevice", __FILE__, __LINE__);
+    // the device address of the array on the current device (looked up on
+    // every call: it allocates nothing and stays right across device resets)
+    void *ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_msi_scratch);
+    if (e != cudaSuccess || !ptr) {
+        m2d_set_last_error(e, "cudaGetSymbolAddress", __FILE__, __LINE__);
         return M2D_ERR_CUDA;
     }
-    if (dev < 0 || dev >= kMaxDevices) {
-        m2d_set_last_error_msg("msi_solve_device_noalloc: device ordinal out of range");
-        return M2D_ERR_ARG;
-    }
-    double *work = nullptr;
-    {
-        std::lock_guard<std::mutex> lock(g_mutex);
-        if (!g_scratch_addr[dev]) {
-            void *ptr = nullptr;
-            e = cudaGetSymbolAddress(&ptr, g_msi_scratch);
-            if (e != cudaSuccess || !ptr) {
-                m2d_set_last_error(e, "cudaGetSymbolAddress", __FILE__, __LINE__);
-                return M2D_ERR_CUDA;
-            }
-            g_scratch_addr[dev] = (double *)ptr;
-        }
-        work = g_scratch_addr[dev];
-    }
+    double *work = (double *)ptr;
     return m2d_msi_solve_device_ws(nd, nx, ny, nitm, tol, d_a, d_b, d_x, work, kNoallocScratchDoubles, stream,
                                    d_nit, nullptr, 0);
 }

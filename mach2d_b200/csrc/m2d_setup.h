@@ -16,7 +16,7 @@ namespace m2d {
     X(g) X(u) X(ua) X(v) X(va) X(ue) X(un) X(ve) X(vn) X(Uce) X(Vcn) X(uea)    \
     X(vea) X(una) X(vna) X(cp) X(vlp) X(vle) X(vln) X(kp) X(ke) X(kn) X(cup)   \
     X(sup) X(cvp) X(svp) X(bu) X(bv) X(bt) X(bp) X(pl) X(due) X(dve) X(dun)    \
-    X(dvn) X(de) X(dn)
+    X(dvn) X(de) X(dn) X(vtp)
 
 // what the host computes of one instance: the grid nodes and the strips of
 // the initial guess; everything else is computed on the device

@@ -41,6 +41,8 @@ struct MsiLaunch {
     size_t ws_cap;             // doubles each ws holds; 0 = at least msi_work_doubles()
     int prec;                  // 0: FP64 throughout (bitwise reference); 1: FP32 factors and
                                // sweeps inside the FP64 iteration (cluster kernel only)
+    unsigned long long hook_ns;  // test hook of the cluster kernel (set by launch_msi_warp from
+                                 // m2d_test_wait_hook; 0: off)
 };
 
 // Largest ny the one-CTA wavefront kernel accepts (its shared-memory ring

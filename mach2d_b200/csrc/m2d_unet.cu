@@ -90,8 +90,9 @@ struct ConvArgs {
     int accumulate;                // yf += result
     int act;                       // 1: y = gelu(result)
     int nimg, H, W, cin, cout;
-    int *err;                      // device error word (ERR_WAIT_TIMEOUT), may be null
+    int *err;                      // device error word (ERR_SPIN_TIMEOUT), may be null
     const bf16 *wtc;               // the weights in the tcgen05 staging order, or null
+    unsigned long long hook_ns;    // test hook: CTA 0's extra wait on an idle barrier (0: none)
 };
 
 template <int NT>
@@ -196,7 +197,7 @@ __global__ void __launch_bounds__(128) k_conv3x3(ConvArgs a)
 constexpr int kTcPix = 128, kTcHaloW = kTcPix + 2, kTcRows = 2, kTcHaloRows = kTcRows + 2;
 constexpr int kTcHaloBytes = 2 * kTcHaloRows * kTcHaloW * 16;
 constexpr int kTcMaxN = 256;
-constexpr unsigned kTcWaitCap = 1u << 24;
+constexpr unsigned long long kTcWaitNs = 4000000000ull;   // bound of every wait (4 s of %globaltimer)
 
 __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
 {
@@ -210,20 +211,36 @@ __device__ __forceinline__ uint32_t umma_idesc_bf16_f32(int M, int N)
     // N >> 3 at bit 17, M >> 4 at bit 24
     return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
-// bounded wait for the completion of phase `parity`; false when the cap ran out
-__device__ __forceinline__ bool tc_mbar_wait(unsigned long long *b, uint32_t parity)
+// bounded wait for the completion of phase `parity`: false when limit_ns of
+// %globaltimer time passed first, or when *abort (may be null) became nonzero
+__device__ __forceinline__ bool tc_mbar_wait(unsigned long long *b, uint32_t parity, unsigned long long limit_ns,
+                                             const volatile int *abort)
 {
     const uint32_t addr = smem_u32(b);
-    for (unsigned it = 0; it < kTcWaitCap; it++) {
+    unsigned long long t0 = 0;
+    for (unsigned it = 0;; it++) {
         uint32_t done;
         asm volatile("{\n\t.reg .pred p;\n\t"
                      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
                      "selp.u32 %0, 1, 0, p;\n\t}"
                      : "=r"(done) : "r"(addr), "r"(parity) : "memory");
         if (done) return true;
+        if ((it & 63u) == 0u) {
+            if (abort && *abort) return false;
+            unsigned long long t;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+            if (it == 0) t0 = t;
+            else if (t - t0 > limit_ns) return false;
+        }
     }
-    return false;
 }
+
+// Test hook (no counterpart in the reference): when nonzero, CTA 0 of the
+// next tcgen05 convolutions first waits on an mbarrier that nothing
+// completes, bounded by this many nanoseconds, before it issues any copy; the
+// wait runs out, the CTA sets ERR_SPIN_TIMEOUT and stops, and the host reads
+// M2D_ERR_TIMEOUT from m2d_unet_status.  Set by m2d_test_wait_hook.
+unsigned long long g_conv_hook_ns = 0;
 
 // ---- persistent, warp-specialised tcgen05 convolution fed by TMA
 // Each CTA loops over tiles (two 128-pixel row segments, as above).  One
@@ -280,7 +297,7 @@ __global__ void __launch_bounds__(kTcpThreads, 1) k_conv3x3_tcp(ConvArgs a, TcpS
                                                                const __grid_constant__ CUtensorMap xmap)
 {
     extern __shared__ __align__(1024) unsigned char tc_smem[];
-    __shared__ __align__(8) unsigned long long full[4], empty[4], tfull[2], tempty[2], mdone;
+    __shared__ __align__(8) unsigned long long full[4], empty[4], tfull[2], tempty[2], mdone, idle;
     __shared__ uint32_t tmem_slot;
     __shared__ volatile int s_abort;
     const int N = a.cout, S = sh.nstage, NB = sh.nbuf;
@@ -299,6 +316,7 @@ __global__ void __launch_bounds__(kTcpThreads, 1) k_conv3x3_tcp(ConvArgs a, TcpS
         for (int q = 0; q < S; q++) { tc_mbar_init_n(&full[q], 1); tc_mbar_init_n(&empty[q], 1); }
         for (int q = 0; q < NB; q++) { tc_mbar_init_n(&tfull[q], 1); tc_mbar_init_n(&tempty[q], 8); }
         tc_mbar_init_n(&mdone, 1);
+        tc_mbar_init_n(&idle, 1);   // nothing ever arrives on it (test hook)
         s_abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -309,9 +327,11 @@ __global__ void __launch_bounds__(kTcpThreads, 1) k_conv3x3_tcp(ConvArgs a, TcpS
     const uint32_t base = smem_u32(tc_smem);
     auto wait = [&](unsigned long long *b, uint32_t parity) {
         if (s_abort) return false;
-        if (tc_mbar_wait(b, parity)) return true;
-        s_abort = 1;
-        if (a.err) atomicOr(a.err, m2d::ERR_WAIT_TIMEOUT);
+        if (tc_mbar_wait(b, parity, kTcWaitNs, &s_abort)) return true;
+        if (!s_abort) {
+            s_abort = 1;
+            if (a.err) atomicOr(a.err, m2d::ERR_SPIN_TIMEOUT);
+        }
         return false;
     };
     auto tile_origin = [&](int t, int &img, int &gy0, int &gx0) {
@@ -323,6 +343,14 @@ __global__ void __launch_bounds__(kTcpThreads, 1) k_conv3x3_tcp(ConvArgs a, TcpS
 
     if (warp == 8) {
         // ---- staging (one lane): items (tile, chunk) in order, S in flight
+        if (lane == 0 && a.hook_ns && blockIdx.x == 0) {
+            // test hook: a wait that runs out before any copy is issued, so
+            // no copy is in flight when the CTA stops
+            if (!tc_mbar_wait(&idle, 0u, a.hook_ns, nullptr)) {
+                s_abort = 1;
+                if (a.err) atomicOr(a.err, m2d::ERR_SPIN_TIMEOUT);
+            }
+        }
         if (lane == 0) {
             const uint32_t item_bytes = (uint32_t)(2 * kTcHalfBytes + 9 * 2 * N * 16);
             long long it = 0;
@@ -386,7 +414,7 @@ __global__ void __launch_bounds__(kTcpThreads, 1) k_conv3x3_tcp(ConvArgs a, TcpS
             // every MMA this thread issued has completed before tensor memory is released
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
                          ::"r"(smem_u32(&mdone)) : "memory");
-            if (!tc_mbar_wait(&mdone, 0u) && a.err) atomicOr(a.err, m2d::ERR_WAIT_TIMEOUT);
+            if (!tc_mbar_wait(&mdone, 0u, kTcWaitNs, nullptr) && a.err) atomicOr(a.err, m2d::ERR_SPIN_TIMEOUT);
         }
         __syncwarp();
     } else {
@@ -740,6 +768,10 @@ inline unsigned grid_for(long long n, int block = 256)
 
 }  // namespace
 
+namespace m2d {
+void set_conv_wait_hook(unsigned long long ns) { g_conv_hook_ns = ns; }
+}  // namespace m2d
+
 // ------------------------------------------------------------------ network
 struct ConvLayer {
     int cin, cout, level;
@@ -829,6 +861,7 @@ cudaError_t launch_conv(int nimg, int H, int W, const bf16 *x, int ldx, const bf
     a.accumulate = accumulate; a.act = act; a.nimg = nimg; a.H = H; a.W = W; a.cin = cin; a.cout = cout;
     a.err = err;
     a.wtc = wtc;
+    a.hook_ns = g_conv_hook_ns;
     const bool tc_shape = W % kTcPix == 0 && H % kTcRows == 0 && cout % 16 == 0 && cout <= kTcMaxN && cin % 16 == 0;
     CUtensorMap xmap;
     if (tc_shape && wtc && g_tensor_tc != 0 &&
@@ -1509,6 +1542,7 @@ extern "C" int m2d_unet_status(m2d_unet *n, int *flags)
     cudaSetDevice(n->device);
     cudaError_t e = cudaDeviceSynchronize();
     if (e == cudaSuccess) e = cudaMemcpy(flags, n->err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && *flags) e = cudaMemset(n->err, 0, sizeof(int));   // read and clear
     if (e != cudaSuccess) { m2d_set_last_error(e, "m2d_unet_status", __FILE__, __LINE__); return M2D_ERR_CUDA; }
     return *flags ? M2D_ERR_TIMEOUT : M2D_OK;
 }

@@ -28,7 +28,7 @@ class Case(ctypes.Structure):
         ("dt1", ctypes.c_double), ("dt2", ctypes.c_double), ("it1", ctypes.c_int),
         ("it2", ctypes.c_int), ("h0", ctypes.c_double), ("mincc", ctypes.c_double),
         ("maxcc", ctypes.c_double), ("nan_policy", ctypes.c_int), ("ktm", ctypes.c_int),
-        ("mix", Mixture),
+        ("mix", Mixture), ("modtur", ctypes.c_int), ("prt", ctypes.c_double),
     ]
 
     @classmethod

@@ -153,3 +153,41 @@ void orc_get_eddy_viscosity_fictitious(int nx, int ny, double *phi)
     phi[IDX(1, ny)] = phi[IDX(2, ny - 1)];
     phi[IDX(nx, ny)] = phi[IDX(nx - 1, ny - 1)];
 }
+
+/* Wiring of the eddy viscosity into the momentum and energy equations, which
+ * the reference leaves out (it never calls get_eddy_viscosity_blomax; its
+ * post-processing zeroes vtp, mod_intflow_postp.f90:57,63).  Effective
+ * viscosity mu + mu_t and conductivity k + cp mu_t / Pr_t at the nodes; at
+ * the east and north faces the arithmetic means of mu_t and of cp mu_t of the
+ * two cells; the north faces of the last real row (the wall) and the faces
+ * past the last column or row keep the laminar values. */
+void orc_add_eddy_viscosity(int nx, int ny, int ktm, double mu, double kappa, double prt, const double *vtp,
+                            const double *cp, double *vlp, double *vle, double *vln, double *kp, double *ke,
+                            double *kn)
+{
+    for (int j = 1; j <= ny; j++)
+        for (int i = 1; i <= nx; i++) {
+            const long np = IDX(i, j);
+            const double mp = ktm ? vlp[np] : mu, me = ktm ? vle[np] : mu, mn = ktm ? vln[np] : mu;
+            const double kpl = ktm ? kp[np] : kappa, kel = ktm ? ke[np] : kappa, knl = ktm ? kn[np] : kappa;
+            const double tp = cp[np] * vtp[np];
+            vlp[np] = mp + vtp[np];
+            kp[np] = kpl + tp / prt;
+            if (i < nx) {
+                const double te = cp[np + 1] * vtp[np + 1];
+                vle[np] = me + 0.5 * (vtp[np] + vtp[np + 1]);
+                ke[np] = kel + 0.5 * (tp + te) / prt;
+            } else {
+                vle[np] = me;
+                ke[np] = kel;
+            }
+            if (j < ny - 1) {
+                const double tn = cp[np + nx] * vtp[np + nx];
+                vln[np] = mn + 0.5 * (vtp[np] + vtp[np + nx]);
+                kn[np] = knl + 0.5 * (tp + tn) / prt;
+            } else {
+                vln[np] = mn;
+                kn[np] = knl;
+            }
+        }
+}

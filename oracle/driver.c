@@ -21,7 +21,7 @@
     X(ua) X(v) X(va) X(ue) X(un) X(ve) X(vn) X(Uce) X(Vcn) X(cp) X(vlp) X(vle) \
     X(vln) X(kp) X(ke) X(kn) X(cup) X(sup) X(cvp) X(svp) X(uea) X(vea) X(una) \
     X(vna) X(bu) X(bv) X(bt) X(bp) X(pl) X(due) X(dve) X(dun) X(dvn) X(de) \
-    X(dn) X(fbe) X(fbn)
+    X(dn) X(fbe) X(fbn) X(vtp)
 
 struct orc_state {
     orc_case c;
@@ -37,6 +37,7 @@ struct orc_state {
     double dt, norm, normpl, rmass, p_avg;
     double Rg, gamma, Tref, Cpref, Href, fm1D, Fd1D, Fpv1D, Sg;
     int ktm, it_stop;
+    double *blwork;                                /* 9 (ny-2): Baldwin-Lomax line work */
 };
 
 int orc_nx(const orc_state *s) { return s->nx; }
@@ -76,6 +77,7 @@ orc_state *orc_create(const orc_case *c)
     s->Tbs = (double *)calloc((size_t)nx, sizeof(double));
     double **v1[] = {&s->uin, &s->vin, &s->pin, &s->Tin, &s->Mw, &s->plin, &s->pina};
     for (int k = 0; k < 7; k++) *v1[k] = (double *)calloc((size_t)ny, sizeof(double));
+    s->blwork = (double *)calloc(9 * (size_t)ny, sizeof(double));
     double **v2[] = {&s->M1D, &s->p1D, &s->T1D, &s->u1D};
     for (int k = 0; k < 4; k++) *v2[k] = (double *)calloc((size_t)nx, sizeof(double));
 
@@ -224,6 +226,7 @@ void orc_destroy(orc_state *s)
     free(s->Tbe); free(s->Tbw); free(s->Tbn); free(s->Tbs);
     free(s->uin); free(s->vin); free(s->pin); free(s->Tin); free(s->Mw); free(s->plin); free(s->pina);
     free(s->M1D); free(s->p1D); free(s->T1D); free(s->u1D);
+    free(s->blwork);
     free(s);
 }
 
@@ -252,6 +255,15 @@ int orc_iterate(orc_state *s, orc_report *rep)
             orc_transport_faces(&c->mix, nx, ny, 1, s->Tbn, s->Tbs, s->Tbe, s->Tbw, s->vlp, s->vle, s->vln);
             orc_transport_faces(&c->mix, nx, ny, 0, s->Tbn, s->Tbs, s->Tbe, s->Tbw, s->kp, s->ke, s->kn);
         }
+    }
+    /* Baldwin-Lomax eddy viscosity from the previous iteration's flow
+     * (blomax.f90:285-490), added to the laminar transport coefficients */
+    if (modvis == 1 && c->modtur == 1) {
+        orc_get_eddy_viscosity_blomax(nx, ny, s->x, s->y, s->xp, s->yp, s->xk, s->yk, s->Jp, s->Jn, s->vln,
+                                      s->ro, s->ron, s->u, s->v, s->vtp, s->blwork);
+        orc_get_eddy_viscosity_fictitious(nx, ny, s->vtp);
+        orc_add_eddy_viscosity(nx, ny, s->ktm, c->mu, c->kappa, c->prt, s->vtp, s->cp, s->vlp, s->vle, s->vln,
+                               s->kp, s->ke, s->kn);
     }
     /* get_average(p) */
     {

@@ -248,6 +248,8 @@ typedef struct orc_case {
     int nan_policy;
     int ktm;               /* 0 = CONSTANT, 1 = MIXTURE */
     orc_mixture mix;       /* ktm = 1 */
+    int modtur;            /* 1: Baldwin-Lomax eddy viscosity in the transport coefficients (modvis = 1) */
+    double prt;            /* turbulent Prandtl number (modtur = 1) */
 } orc_case;
 
 typedef struct orc_report {
@@ -277,6 +279,12 @@ void orc_get_eddy_viscosity_blomax(int nx, int ny, const double *x, const double
                                    const double *Jn, const double *vln, const double *ro, const double *ron,
                                    const double *u, const double *v, double *vtp, double *work);
 void orc_get_eddy_viscosity_fictitious(int nx, int ny, double *phi);
+/* the eddy viscosity into the transport coefficients (no reference call
+ * site: blomax.f90 is compiled but never used); ktm = 0 takes the laminar
+ * values from the constants mu, kappa, ktm = 1 from the arrays themselves */
+void orc_add_eddy_viscosity(int nx, int ny, int ktm, double mu, double kappa, double prt, const double *vtp,
+                            const double *cp, double *vlp, double *vle, double *vln, double *kp, double *ke,
+                            double *kn);
 
 /* ---- thermophysical model (thermo.c): mod_class_thermophysical_mixture.f90,
  *      mod_thermophysical.f90, mod_field_operations.f90.  orc_mixture has

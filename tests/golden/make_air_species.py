@@ -4,7 +4,7 @@ N2 0.78, O2 0.21) read from its mach2d_input/thermo_database.csv with the
 package's own parsers, so that the GPU tests can build that mixture without
 the reference tree.
 
-    python tests/golden/make_air_species.py /root/reference
+    python tests/golden/make_air_species.py <path of the reference checkout>
 """
 import json
 import os
@@ -29,4 +29,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {sys.argv[0]} <path of the reference checkout>")
+    main(sys.argv[1])

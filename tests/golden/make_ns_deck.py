@@ -5,7 +5,7 @@ adiabatic wall, FP64 MSI) run by the oracle to its stopping iteration: the
 case as read by mach2d_b200.ifile, every 100th report and the final
 integrals.
 
-    python tests/golden/make_ns_deck.py /root/reference
+    python tests/golden/make_ns_deck.py <path of the reference checkout>
 """
 import json
 import os
@@ -41,4 +41,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {sys.argv[0]} <path of the reference checkout>")
+    main(sys.argv[1])

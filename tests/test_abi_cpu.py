@@ -46,6 +46,17 @@ def test_bad_arguments_are_rejected_before_any_device_work():
     assert rc in (2, 6)
 
 
+def test_wait_hook_rejects_bad_arguments():
+    # the failure-detection test hook only sets host state; it is exercised on
+    # the GPU by test_gpu_wait_timeout.py
+    L = _lib.lib()
+    L.m2d_test_wait_hook.argtypes = [ctypes.c_int, ctypes.c_double]
+    assert L.m2d_test_wait_hook(3, 0.01) == 2
+    assert L.m2d_test_wait_hook(1, 20.0) == 2
+    assert L.m2d_test_wait_hook(1, -1.0) == 2
+    assert L.m2d_test_wait_hook(0, 0.0) == 0
+
+
 def test_msi_max_ny_fits_shared_memory():
     assert _lib.lib().m2d_msi_max_ny() >= 1026
 

@@ -1,0 +1,101 @@
+"""Parity at the two Euler workloads the benchmark times, against the oracle's
+committed fixtures (tests/golden/bench_workloads.json, made by
+tests/golden/make_bench_golden.py) and, for the 512x256 case, the oracle run
+alongside.
+
+* C01 cosine nozzle, 512x256 real volumes, FP64 MSI, each outer iteration one
+  captured CUDA graph (the benchmark's throughput workload): the first 20
+  iterations.  Every report column of src/mach2d_main.f90:495-516 agrees to a
+  relative 1e-9 (the global sums run in a different order), the p' cycles of
+  every iteration are equal, and the fields after iteration 20 agree to 1e-9
+  of their magnitude.
+* C01 cosine nozzle, 80x40, to the reference's stopping rule (normpl < tolt =
+  1e-10 first at it, stop at 2 it; src/mach2d_main.f90:307,441-443) with
+  FP64 MSI (solver 0) and with FP32 factors and sweeps inside the FP64
+  iteration (solver 2).  The converged Cd = fme / fm1D
+  (src/user/internal_flow/mod_intflow_postp.f90:1211), the mass flow rates,
+  the thrust and the wall pressure p(i, ny-1) (mod_intflow_postp.f90:430-445)
+  agree with the FP64 oracle to the relative tolerance 1e-6 of the
+  integrals' specification.  Solver 0 also stops at the oracle's iteration.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from _oracle import OracleCase
+from mach2d_b200.simplec import Case, Simplec
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden", "bench_workloads.json")
+COLS = ("dt", "norm", "normpl", "rmass", "fmi", "fme", "Fd")
+RTOL_ITER = 1e-9        # report columns and fields after many iterations (sum order only)
+RTOL_INTEGRAL = 1e-6    # converged integrals vs the FP64 oracle
+
+
+def _gold(key):
+    return json.load(open(GOLD))[key]
+
+
+def _rel(a, b):
+    return abs(a - b) / max(abs(b), 1e-300)
+
+
+def test_bench_workload_512x256_first_20_iterations():
+    gold = _gold("c01_euler_512x256_first20")
+    case = Case.from_dict(gold["case"])
+    g = Simplec(case)
+    g.set_graph(True)
+    o = OracleCase(case)
+    for row in gold["history"]:
+        r = g.iterate()
+        rc, ro = o.iterate()
+        assert rc == 0
+        assert r.it == row[0] == ro.it
+        assert r.itp_used == row[8] == ro.itp_used, r.it
+        for k, c in enumerate(COLS, start=1):
+            assert _rel(getattr(r, c), row[k]) < RTOL_ITER or abs(row[k]) < 1e-12, (r.it, c)
+            # the fixture is the oracle's own output for this case
+            assert getattr(ro, c) == row[k], (r.it, c)
+    for f, s in gold["field_checksums"].items():
+        fg, fo = g.field(f), o.field(f)
+        assert np.max(np.abs(fg - fo)) <= RTOL_ITER * s["max_abs"], f
+        assert _rel(float(np.abs(fg).sum()), s["abs_sum"]) < RTOL_ITER, f
+    g.close()
+
+
+def _converged(solver):
+    gold = _gold("c01_euler_80x40_converged")
+    case = Case.from_dict(gold["case"])
+    case.solver = solver
+    g = Simplec(case)
+    g.set_graph(True)
+    rep = g.run(200000)
+    fmi, fme, Fd, Cd, pwall = g.integrals()
+    g.close()
+    return gold["final"], rep, (fmi, fme, Fd, Cd, np.asarray(pwall))
+
+
+def _check_integrals(fin, rep, ints):
+    fmi, fme, Fd, Cd, pwall = ints
+    assert rep.normpl < 1e-10
+    assert _rel(Cd, fin["Cd"]) < RTOL_INTEGRAL
+    assert _rel(fmi, fin["fmi"]) < RTOL_INTEGRAL and _rel(fme, fin["fme"]) < RTOL_INTEGRAL
+    assert _rel(Fd, fin["Fd"]) < RTOL_INTEGRAL
+    pw = np.asarray(fin["pwall"])
+    assert np.max(np.abs(pwall - pw)) <= RTOL_INTEGRAL * np.max(np.abs(pw))
+
+
+def test_config1_converged_integrals_fp64():
+    fin, rep, ints = _converged(0)
+    assert rep.it == fin["it"]              # same stopping iteration (it_stop = 2 it)
+    _check_integrals(fin, rep, ints)
+
+
+def test_config1_converged_integrals_fp32_sweeps():
+    fin, rep, ints = _converged(2)
+    # FP32 factors change each p' solve within its tolerance, so the stopping
+    # iteration may move slightly; the converged integrals may not
+    assert abs(rep.it - fin["it"]) <= 0.02 * fin["it"]
+    _check_integrals(fin, rep, ints)

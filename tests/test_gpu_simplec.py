@@ -111,6 +111,25 @@ def test_mixture_navier_stokes():
                   fields=("u", "v", "p", "T", "ro") + PROPS)
 
 
+TURB = ("vtp", "vlp", "vle", "vln", "kp", "ke", "kn")
+
+
+def test_navier_stokes_baldwin_lomax():
+    """modtur = 1: the Baldwin-Lomax eddy viscosity (device exp in the van
+    Driest damping, 1e-12) from the previous flow, added to the constant
+    laminar mu and k every iteration, as the oracle wires it."""
+    g, o = _compare_runs(euler_cosine_case(24, 12, modvis=1, Twall=900.0, modtur=1, prt=0.9), 15,
+                         fields=("u", "v", "p", "T", "ro") + TURB)
+    vt = o.field("vtp")
+    assert vt.max() > 0.0                 # the model is active, not a zero field
+    assert np.all(g.field("vle") >= 1.0e-5 * (1 - 1e-15))
+
+
+def test_mixture_navier_stokes_baldwin_lomax():
+    _compare_runs(euler_cosine_case(24, 12, modvis=1, Twall=900.0, ktm=1, mix=_air(), modtur=1, prt=0.9), 12,
+                  fields=("u", "v", "p", "T", "ro", "cp") + TURB)
+
+
 def test_tdma_solver_path():
     _compare_runs(n01_case(solver=1, nitm_u=3, nitm_p=5), 15)
 

@@ -186,3 +186,39 @@ def test_mixture_euler_solves_the_energy_equation():
     real[1:-1, 1:-1] = True
     real = real.reshape(-1)
     assert np.std(cp[real]) > 0 and np.all((T[real] > 200) & (T[real] < 1100))
+
+
+def test_oracle_reproduces_bench_workload_fixture():
+    """The first 3 outer iterations of the 512x256 C01 Euler workload are
+    bitwise the committed fixture's (tests/golden/make_bench_golden.py)."""
+    from mach2d_b200.simplec import Case
+    gold = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "bench_workloads.json")))
+    g = gold["c01_euler_512x256_first20"]
+    o = OracleCase(Case.from_dict(g["case"]))
+    for row in g["history"][:3]:
+        rc, r = o.iterate()
+        assert rc == 0
+        assert [r.it, r.dt, r.norm, r.normpl, r.rmass, r.fmi, r.fme, r.Fd, r.itp_used] == row
+    fin = gold["c01_euler_80x40_converged"]["final"]
+    assert fin["it"] == 2 * (fin["it"] // 2) and fin["normpl"] < 1e-10
+    assert 1.0 < fin["Cd"] < 1.01
+
+
+def test_baldwin_lomax_wiring_in_the_oracle_iteration():
+    """modtur = 1 adds mu_t (>= 0) to the laminar viscosity at nodes and faces
+    and keeps the wall faces laminar; modtur = 0 leaves vtp zero."""
+    case = euler_cosine_case(24, 12, modvis=1, Twall=900.0, modtur=1, prt=0.9)
+    o = OracleCase(case)
+    for _ in range(6):
+        rc, _ = o.iterate()
+        assert rc == 0
+    vtp, vle, vln, vlp = (o.field(f) for f in ("vtp", "vle", "vln", "vlp"))
+    nx, ny = o.nx, o.ny
+    assert vtp.max() > 0.0 and vtp.min() >= 0.0
+    assert np.array_equal(vlp, case.mu + vtp)
+    wall = [(ny - 2) * nx + i for i in range(nx)]
+    assert np.all(vln[wall] == case.mu)
+    assert np.all(vle >= case.mu)
+    o2 = OracleCase(euler_cosine_case(24, 12, modvis=1, Twall=900.0))
+    o2.iterate()
+    assert not o2.field("vtp").any()

@@ -52,6 +52,21 @@ def _solve_both(L, nd, nx, ny, nitm, tol, a, b):
 
 
 @pytest.mark.parametrize("nd", [9, 5])
+def test_noalloc_one_cta_fallback_matches_allocating_entry_point(nd):
+    # 400 x 300 is under the cell limit, but its wavefront-major layout
+    # (21 or 15 planes of 320 x 462) does not fit in the array, so the
+    # noalloc call runs the one-CTA kernel while the allocating call, with a
+    # full workspace, runs the cluster kernel; the two are bitwise equal
+    L = _bind()
+    nx, ny = 400, 300
+    assert nx * ny <= L.m2d_msi_noalloc_max_cells(nd)
+    a, b = dirichlet_system(nd, nx, ny, seed=33)
+    x_ref, x_new, nit = _solve_both(L, nd, nx, ny, 5, 1e-6, a, b)
+    assert nit[0] == nit[1] and nit[0] >= 1
+    assert np.array_equal(x_ref, x_new)
+
+
+@pytest.mark.parametrize("nd", [9, 5])
 def test_noalloc_solve_matches_allocating_entry_point_twice(nd):
     L = _bind()
     # two calls in a row on the shared scratch, different sizes and systems
