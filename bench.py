@@ -40,6 +40,11 @@ import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+# Many instances' captured iterations are in flight at once in the batch and
+# sweep figures; with the default 8 hardware work queues, streams share queues
+# and serialise.  Read when the process creates its CUDA context, so set here,
+# before torch or the library touches the device.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 NXR, NYR = 512, 256
 HBM_FALLBACK_GBS = 6650.0
@@ -62,6 +67,8 @@ def parse():
                          "profilers that do not look inside conditional graph nodes)")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the time-to-residual, FP32-sweep and learned-correction figures")
+    ap.add_argument("--ttr-cap", type=float, default=300.0,
+                    help="wall-time cap (s) of each 512x256 time-to-residual run (0: skip them)")
     return ap.parse_args()
 
 
@@ -164,6 +171,44 @@ def cpu_sample(args, seconds, skip=0):
     return args.nxr * args.nyr * n / dt, n, dt
 
 
+def _cpu_worker(nxr, nyr, skip, seconds, q):
+    """One process of the all-cores CPU baseline: its own instance of the
+    workload, `skip` untimed iterations, then iterations for about `seconds`."""
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from _oracle import OracleCase
+    from mach2d_b200.simplec import euler_cosine_case
+    o = OracleCase(euler_cosine_case(nxr, nyr))
+    for _ in range(skip):
+        o.iterate()
+    t0 = time.perf_counter()
+    n = 0
+    while time.perf_counter() - t0 < seconds:
+        o.iterate()
+        n += 1
+    q.put((n, time.perf_counter() - t0))
+
+
+def cpu_sample_all_cores(args, seconds, skip=0):
+    """The serial CPU restatement on every host core at once: one process per
+    core, each advancing its own instance of the workload (the reference's
+    build is serial, so independent runs are how it uses more cores).
+    Processes are started with `spawn`.  Returns (aggregate cell-updates/s,
+    processes, iterations)."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    nproc = os.cpu_count() or 1
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_cpu_worker, args=(args.nxr, args.nyr, skip, seconds, q)) for _ in range(nproc)]
+    for pr in procs:
+        pr.start()
+    res = [q.get() for _ in procs]
+    for pr in procs:
+        pr.join()
+    rate = sum(args.nxr * args.nyr * n / t for n, t in res)
+    return rate, nproc, sum(n for n, _ in res)
+
+
 def run_reference(args):
     """The reference arm: the serial CPU restatement on the same iterations
     the GPU arm times -- W untimed warm-up iterations from the initial guess,
@@ -211,6 +256,25 @@ def msi_algorithmic_bytes(nd, N, nit):
     return 8 * N * (lu + res + nit * it)
 
 
+# FP64 bytes per cell of the non-MSI work of one Euler outer iteration (each
+# distinct plane read once and written once per kernel, 8 B): u and v
+# assembly 2 x 200, SIMPLEC d-coefficients 240, face velocities 320, nodal
+# velocity correction 224, mass check 80, T from H and the densities 88,
+# Scarborough coefficient means 256, boundary strips and backups 24; per p'
+# cycle: p' coefficients 128 and source 120, face correction 184, p / rho /
+# face-rho correction 96, max|p'| 8
+STEP_FIXED_B = 1632
+P_CYCLE_B = 536
+
+
+def step_algorithmic_bytes(N, nit_u, nit_v, nit_p, itp):
+    """Algorithmic HBM bytes of one outer iteration with the MSI iteration
+    counts the device reported (the two MSI9 solves, itp p' cycles of one
+    MSI5 solve each)."""
+    return (N * STEP_FIXED_B + msi_algorithmic_bytes(9, N, nit_u) + msi_algorithmic_bytes(9, N, nit_v)
+            + itp * (N * P_CYCLE_B + msi_algorithmic_bytes(5, N, nit_p)))
+
+
 def run_ours(args):
     import ctypes
 
@@ -246,11 +310,13 @@ def run_ours(args):
     l0 = sim.scalar("launches")
     itp = []
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    counts = []
     with ClockSampler(local) as clk:
         e0.record(st)
         for _ in range(args.steps):
             r = sim.iterate()
             itp.append(r.itp_used)
+            counts.append((sim.scalar("nit_u"), sim.scalar("nit_v"), sim.scalar("nit_p"), r.itp_used))
         e1.record(st)
         torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
@@ -345,6 +411,10 @@ def run_ours(args):
     alg = msi_algorithmic_bytes(5, N, nit)
     achieved = alg / (avg_ms / 1e3) / 1e9
     peak, peak_kind = peaks()
+    # the whole outer iteration: the byte model with the device's own
+    # iteration counts, over the device time of the timed steps
+    step_bytes = sum(step_algorithmic_bytes(N, *c) for c in counts) / len(counts)
+    step_gbs = step_bytes * world / (ms / args.steps / 1e3) / 1e9
     traffic = None
     prof = os.path.join(ROOT, "profiles", "msi5_traffic.json")
     if os.path.exists(prof):
@@ -364,8 +434,12 @@ def run_ours(args):
         b.iterate(bsteps)
         torch.cuda.synchronize()
         bdt = time.perf_counter() - t0
+        bgbs = args.batch * bsteps * step_bytes / bdt / 1e9
         batch = {"instances": args.batch, "steps": bsteps,
                  "value": args.batch * bsteps * args.nxr * args.nyr / bdt, "unit": "cell-updates/s",
+                 "roofline_step": {"achieved": bgbs, "peak": peak, "unit": "GB/s", "frac": bgbs / peak,
+                                   "note": "the single instance's bytes per outer iteration x instances x steps "
+                                           "/ wall time"},
                  "timing": "host wall clock around m2d_batch_iterate with device synchronisation",
                  "note": "independent instances of the same workload, one context and stream each"}
         b.close()
@@ -382,6 +456,10 @@ def run_ours(args):
         cpu = {"value": v, "unit": "cell-updates/s", "cores": 1, "kind": "port",
                "sample": f"outer iterations {args.warmup + 1}..{args.warmup + nsamp} ({secs:.1f} s) of the same "
                          f"{args.nxr}x{args.nyr} case, serial C restatement of the reference"}
+        va, nprocs, na = cpu_sample_all_cores(args, 10.0, skip=args.warmup)
+        cpu["all_cores"] = {"value": va, "unit": "cell-updates/s", "cores": nprocs, "kind": "port",
+                            "sample": f"{nprocs} processes, one per host core, each its own instance of the same "
+                                      f"case ({na} iterations in about 10 s); reported baseline only"}
 
     if rank == 0:
         line = {
@@ -398,7 +476,14 @@ def run_ours(args):
                          "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind,
                          "traffic": traffic, "algorithmic_bytes_per_launch": alg,
-                         "launch_ms": avg_ms, "iterations_per_launch": nit, "phases_us": phases_us},
+                         "launch_ms": avg_ms, "iterations_per_launch": nit, "phases_us": phases_us,
+                         "step": {"achieved": step_gbs, "peak": peak, "unit": "GB/s", "frac": step_gbs / peak,
+                                  "bytes_per_step": step_bytes, "ms_per_step": ms / args.steps,
+                                  "mean_counts": {k: sum(c[q] for c in counts) / len(counts) for q, k in
+                                                  enumerate(("nit_u", "nit_v", "nit_p", "p_cycles"))},
+                                  "model": f"{STEP_FIXED_B} B/cell + 2 MSI9 solves + p' cycles x "
+                                           f"({P_CYCLE_B} B/cell + MSI5 solve), MSI solves as "
+                                           "msi_algorithmic_bytes, N = nx*ny with the ghost ring"}},
             "cpu_baseline": cpu,
             "batch": batch,
             "clocks": clk.summary(),
@@ -510,6 +595,8 @@ def run_extras(args, local):
         res["learned_fp32"].append(time.perf_counter() - t0)
         nits["learned_fp32"].append(r.nit)
         ratio.append(r.r1 / r.r0)
+    if args.ttr_cap > 0:
+        out["time_to_residual_512x256"] = run_ttr512(local, one, args.ttr_cap)
     one.close()
     out["isolated_system"] = run_isolated(local)
     out["learned"] = {
@@ -520,6 +607,66 @@ def run_extras(args, local):
         "p_solve_ms_median": {k: 1e3 * float(np.median(v)) for k, v in res.items()},
         "msi_iterations_mean": {k: float(np.mean(v)) for k, v in nits.items()},
         "tolerance": "p' solve to |r| < 1e-2 |r0| (nitm_p = 20), host clock per solve"}
+    return out
+
+
+def run_ttr512(local, net, cap_s, tol=1e-8):
+    """Time to the outer residual normpl < 1e-8 (src/mach2d_main.f90:307) of
+    the C01 Euler nozzle at 512x256 (the turbulent Navier-Stokes case of this
+    size stops with a NaN in both implementations, so the same-size Euler
+    nozzle stands in for it), from the initial guess: plain FP64 MSI and FP32
+    factors and sweeps (each iteration one captured graph), and the learned
+    p' correction with FP32 sweeps (solver 3, the network trained on this
+    workload's p' systems; host-driven iterations).  Each run is capped at
+    cap_s seconds.  Integrals at the first iteration below 1e-8 are compared
+    with the FP64 oracle's at its own first such iteration
+    (tests/golden/ttr512_c01_euler.json, make_ttr512_golden.py)."""
+    import numpy as np
+    import torch
+
+    from mach2d_b200.simplec import Simplec, euler_cosine_case
+    ref = None
+    fx = os.path.join(ROOT, "tests", "golden", "ttr512_c01_euler.json")
+    if os.path.exists(fx):
+        ref = json.load(open(fx)).get("first_below")
+    out = {"case": "C01 Euler 512x256, tolt 1e-8, SCARBOROUGH; stands in for the 512x256 Navier-Stokes case, "
+                   "which stops with a NaN (both implementations)",
+           "cap_s": cap_s, "oracle_first_below_it": ref["it"] if ref else None}
+    for key, solver in (("plain_fp64", 0), ("fp32_sweeps", 2), ("learned_fp32", 3)):
+        g = Simplec(euler_cosine_case(512, 256, solver=solver, tolt=tol), device=local)
+        if solver == 3:
+            g.set_unet(net)
+        else:
+            g.set_graph(True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r, reached = None, False
+        while time.perf_counter() - t0 < cap_s:
+            r = g.iterate()
+            if r.normpl < tol:
+                reached = True
+                break
+        secs = time.perf_counter() - t0
+        fmi, fme, Fd, Cd, pw = g.integrals()
+        e = {"seconds": secs, "iterations": r.it, "reached": reached, "normpl": r.normpl, "Cd": Cd,
+             "ms_per_iteration": 1e3 * secs / r.it}
+        if solver == 3:
+            e["learned_calls"] = g.scalar("learned_calls")
+            e["learned_accepted"] = g.scalar("learned_accepted")
+        if ref and reached:
+            pr = np.asarray(ref["pwall"])
+            e["rel_err_vs_oracle"] = {"Cd": abs(Cd - ref["Cd"]) / abs(ref["Cd"]),
+                                      "fmi": abs(fmi - ref["fmi"]) / abs(ref["fmi"]),
+                                      "fme": abs(fme - ref["fme"]) / abs(ref["fme"]),
+                                      "Fd": abs(Fd - ref["Fd"]) / abs(ref["Fd"]),
+                                      "pwall_max": float(np.max(np.abs(pw - pr)) / np.max(np.abs(pr)))}
+        out[key] = e
+        g.close()
+    p = out["plain_fp64"]
+    for key in ("fp32_sweeps", "learned_fp32"):
+        q = out[key]
+        if p["reached"] and q["reached"]:
+            out[f"speedup_{key}_vs_plain_fp64"] = p["seconds"] / q["seconds"]
     return out
 
 
@@ -609,9 +756,40 @@ def run_isolated(local, nx=1026, ny=514, tol=1e-12):
         call("tdma_line", n, np.ascontiguousarray(aw[k]), np.ascontiguousarray(ap[k]), np.ascontiguousarray(ae[k]),
              np.ascontiguousarray(d[k]), xo)
         err = max(err, float(np.max(np.abs(xo - xg[k]))))
-    out["tdma_lines"] = {"lines": nl, "n": n, "gpu_host_api_ms": 1e3 * tg, "cpu_oracle_serial_ms":
-                         1e3 * (time.perf_counter() - t0), "max_abs_difference": err,
-                         "note": "the GPU time is that of the host call m2d_tdma_lines, copies in and out included"}
+    cpu_ms = 1e3 * (time.perf_counter() - t0)
+    # device time of the kernels themselves (CUDA events, inputs resident):
+    # method 0 the sequential recurrence (bitwise), method 1 cyclic reduction;
+    # algorithmic bytes 40 per unknown (aw, ap, ae, d in, x out)
+    L.m2d_tdma_lines_device.argtypes = [ctypes.c_int, ctypes.c_int] + [ctypes.c_void_p] * 6 + [ctypes.c_int,
+                                                                                                ctypes.c_void_p]
+    tl = [torch.from_numpy(np.ascontiguousarray(v)).to(dev) for v in (aw, ap, ae, d)]
+    xw = torch.empty(2 * n * nl, dtype=torch.float64, device=dev)
+    xd = torch.zeros(nl, n, dtype=torch.float64, device=dev)
+    peak, peak_kind = peaks()
+    dev_ms, diff = {}, {}
+    for method, key in ((0, "recurrence"), (1, "cyclic_reduction")):
+        ts = []
+        for rep in range(8):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            check(L.m2d_tdma_lines_device(n, nl, *[v.data_ptr() for v in tl], xd.data_ptr(), xw.data_ptr(), method,
+                                          None))
+            e1.record()
+            torch.cuda.synchronize()
+            if rep >= 3:
+                ts.append(e0.elapsed_time(e1))
+        dev_ms[key] = min(ts)
+        diff[key] = float(np.max(np.abs(xd.cpu().numpy() - xg)) / np.max(np.abs(xg)))
+    alg = 40.0 * n * nl
+    out["tdma_lines"] = {"lines": nl, "n": n, "gpu_host_api_ms": 1e3 * tg, "cpu_oracle_serial_ms": cpu_ms,
+                         "max_abs_difference": err,
+                         "gpu_device_ms": dev_ms,
+                         "relative_difference_to_recurrence": diff,
+                         "roofline": {k: {"achieved_gbs": alg / (v / 1e3) / 1e9, "frac": alg / (v / 1e3) / 1e9 / peak,
+                                          "peak_gbs": peak, "peak_source": peak_kind} for k, v in dev_ms.items()},
+                         "algorithmic_bytes": alg,
+                         "note": "gpu_host_api_ms: the host call m2d_tdma_lines, copies in and out included; "
+                                 "gpu_device_ms: the kernel alone on resident inputs (best of 5 after 3 warm-ups)"}
     return out
 
 
@@ -646,7 +824,7 @@ def run_sweep(local, n, iters, world=1, rank=0):
         import torch.distributed as dist
         dist.barrier()
     tm = {}
-    res, secs = run_shard(cases, mine, local, iters, timings=tm)
+    res, secs = run_shard(cases, mine, local, iters, timings=tm, tune=2)
     setup = tm["setup_s"]
     if world > 1:
         t = torch.tensor([secs, setup], device=f"cuda:{local}", dtype=torch.float64)
@@ -659,9 +837,12 @@ def run_sweep(local, n, iters, world=1, rank=0):
             "real_cells": cells, "ranks": world, "scaling": "strong", "seconds_max_over_ranks": secs,
             "setup_seconds_max_over_ranks": setup,
             "Cd_mean_after": sum(cds) / len(cds),
+            "msi_schedule": tm.get("schedule"),
             "note": "independent Euler nozzles of the seeded sweep distribution sharded over the ranks by cells, "
-                    "FP32 sweeps, one captured graph per instance iteration; batch set-up (grids, metrics and "
-                    "initial fields on the device) timed apart"}
+                    "FP32 sweeps, one captured graph per instance iteration with every instance's graph in flight "
+                    "at once; the MSI schedule autotuned on the batch's first iterations (rank 0's choice shown), "
+                    "then the timed iterations; batch set-up (grids, metrics and initial fields on the device) "
+                    "timed apart"}
 
 
 def main():

@@ -164,6 +164,15 @@ int m2d_tdma5_solve(const int *nx, const int *ny, const int *nitm, const double 
  * i at offset l*n + i; aw, ap, ae the W, P, E coefficients, d the rhs. */
 int m2d_tdma_lines(const int *n, const int *nlines, const double *aw, const double *ap,
                    const double *ae, const double *d, double *x);
+/* The same batch on device arrays (layout as above), asynchronous on
+ * `stream`.  method 0: the sequential recurrence of the reference's line
+ * sweep, one line per thread, bitwise m2d_tdma_lines; d_work holds 2 n
+ * nlines doubles.  method 1 (no counterpart in the reference): parallel
+ * cyclic reduction, one thread block per line in shared memory, n <= 2048
+ * (else M2D_ERR_TOO_LARGE), d_work unused; its rounding differs from the
+ * recurrence's (about 1e-15 relative on diagonally dominant lines). */
+int m2d_tdma_lines_device(int n, int nlines, const double *d_aw, const double *d_ap, const double *d_ae,
+                          const double *d_d, double *d_x, double *d_work, int method, void *stream);
 
 /* norms: src/solvers/mod_solvers.f90:91-277.  `norm` is in/out (the routines
  * add to it); the sums run in a fixed tree order on the GPU. */
@@ -434,7 +443,9 @@ int m2d_set_fields(m2d_ctx *ctx, int count, const char *const *names, const doub
 int m2d_get_fields(m2d_ctx *ctx, int count, const char *const *names, double *const *host,
                    const long *n);
 /* named scalars: dt, norm, normpl, rmass, p_avg, Href, Cpref, fm1D, Fd1D,
- * Fpv1D, Sg, it, it_stop */
+ * Fpv1D, Sg, it, it_stop; and of the last iteration itp_used and the MSI
+ * iterations nit_u, nit_v, nit_p (last p' cycle), nit_T; launches (kernels
+ * started so far), learned_calls, learned_accepted, solver, msi_schedule */
 int m2d_get_scalar(const m2d_ctx *ctx, const char *name, double *out);
 /* post-processing integrals (src/user/internal_flow/mod_intflow.f90:1591-1643,
  * mod_intflow_postp.f90:1211 Cd = fme/fm1D, :430-445,1454-1465 wall pressure
@@ -457,6 +468,14 @@ int m2d_ctx_set_unet(m2d_ctx *ctx, struct m2d_unet *net);
  * Results are bitwise those of the default mode (0).  Not with solver 3. */
 int m2d_ctx_set_graph(m2d_ctx *ctx, int on);
 int m2d_ctx_field_device(m2d_ctx *ctx, const char *name, double **dptr, long *n);
+/* The wavefront schedule of the context's MSI solves, no counterpart in the
+ * reference: 0 automatic (one wavefront warp per SM when the thread-block
+ * cluster fits, else two), 1 one warp per SM with 4 staging stages, 2 two
+ * warps per SM with 2 stages (half the SMs per solve), 3 the one-CTA kernel
+ * (FP64 solvers only; with FP32 sweeps it means 0).  A schedule that cannot
+ * run falls back to the one-CTA kernel.  All schedules give the same
+ * iterates; a captured iteration is captured again on its next call. */
+int m2d_ctx_set_msi_schedule(m2d_ctx *ctx, int variant);
 
 /* ---- batches of instances (no counterpart in the reference) ------------
  * n independent nozzle instances on one GPU, each a full context with its
@@ -475,6 +494,23 @@ int m2d_batch_size(const m2d_batch *b, int *n);
 int m2d_batch_ctx(m2d_batch *b, int k, m2d_ctx **ctx);
 int m2d_batch_iterate(m2d_batch *b, int iters, m2d_report *reps);
 int m2d_batch_status(const m2d_batch *b, int k, int *status);
+/* Instances whose iterations run as captured graphs (m2d_ctx_set_graph on
+ * m2d_batch_ctx) are advanced with every graph in flight at once: each
+ * iteration launches all of them, then waits for each.  Each instance has its
+ * own stream; for more than a few instances set the environment variable
+ * CUDA_DEVICE_MAX_CONNECTIONS=32 before the process's first CUDA call, so
+ * that the streams do not share the default 8 hardware queues (256 uneven
+ * nozzles: 131 M cell-updates/s with 8, 310 M with 32 on one B200).
+ * m2d_batch_set_msi_schedule: m2d_ctx_set_msi_schedule on every instance.
+ * m2d_batch_autotune: the schedule autotuner -- runs the batch's next
+ * 1 + iters iterations with each candidate schedule (1, 2, and 3 when every
+ * instance solves in FP64), times the last iters of each on the host clock,
+ * keeps the fastest (*chosen, may be NULL) and writes each candidate's
+ * milliseconds per iteration to ms_per_iter[variant] (4 doubles, may be
+ * NULL; -1 for schedules not tried).  Schedules give the same iterates, so
+ * the tuned run's results equal an untuned one's. */
+int m2d_batch_set_msi_schedule(m2d_batch *b, int variant);
+int m2d_batch_autotune(m2d_batch *b, int iters, int *chosen, double *ms_per_iter);
 
 /* ===================== 3. learned p' preconditioner ======================
  * No counterpart in the reference.  A 4-level U-Net (3x3 convolutions with
@@ -557,6 +593,33 @@ int m2d_pprime_solve_cycles(m2d_unet *net, int nx, int ny, int m, int max_cycles
                             const double *d_a, const double *d_b, double *d_x, const double *d_Jp,
                             double *d_work, int prec, void *stream, m2d_learned_report *rep);
 int m2d_batch_destroy(m2d_batch *b);
+
+/* ===================== 4. flexible GMRES (no counterpart in the reference) =====
+ * The reference iterates MSI as a stationary method (x += (LU)^-1 (b - A x),
+ * fb2d9 / fb2d5).  m2d_fgmres_solve keeps MSI's incomplete factorisation
+ * (computed once per call) as the right preconditioner of flexible GMRES
+ * (Saad 1993) with restart length `restart` (1..32), to |b - A x| <= tol |b|
+ * or maxit preconditioner applications (then M2D_ERR_TIMEOUT).  prec 0: MSI
+ * with FP64 factors; 1: FP32 factors and sweeps; 2 (nd = 5): the learned
+ * correction of `net` (images covering the real cells; Jp for its features)
+ * followed by one FP32 MSI step from it, z = N(v) + (LU)^-1 (v - A N(v)).
+ * All device pointers; x is the initial guess on entry; d_work holds
+ * m2d_fgmres_workspace_doubles(nd, nx, ny, restart) doubles, 16-byte
+ * aligned.  Synchronises `stream` once per Krylov step (the Hessenberg
+ * least-squares problem is solved on the host); dot products are FP64 in a
+ * fixed order, so a solve is reproducible bit for bit. */
+typedef struct m2d_fgmres_report {
+    int iterations;              /* Krylov steps = preconditioner applications */
+    int msi_applications;        /* MSI forward/backward sweep pairs */
+    int learned_applications;    /* network corrections (prec 2) */
+    int cycles;                  /* restart cycles */
+    int converged;
+    double rel_residual;         /* |b - A x| / |b| of the returned x, recomputed */
+} m2d_fgmres_report;
+long m2d_fgmres_workspace_doubles(int nd, int nx, int ny, int restart);
+int m2d_fgmres_solve(int nd, int nx, int ny, int restart, int maxit, double tol, const double *d_a,
+                     const double *d_b, double *d_x, int prec, m2d_unet *net, const double *d_Jp,
+                     double *d_work, void *stream, m2d_fgmres_report *rep);
 
 #ifdef __cplusplus
 }

@@ -294,6 +294,24 @@ int m2d_tdma_lines(const int *n, const int *nlines, const double *aw, const doub
     return s.finish(launch_tdma_lines(*n, *nlines, daw, dap, dae, dd, dx, P, Q, 0));
 }
 
+int m2d_tdma_lines_device(int n, int nlines, const double *d_aw, const double *d_ap, const double *d_ae,
+                          const double *d_d, double *d_x, double *d_work, int method, void *stream)
+{
+    if (n < 1 || nlines < 1 || !d_aw || !d_ap || !d_ae || !d_d || !d_x || (method != 0 && method != 1))
+        return fail(ST_ARG, "tdma_lines_device: bad arguments");
+    cudaError_t e;
+    if (method == 0) {
+        if (!d_work) return fail(ST_ARG, "tdma_lines_device: method 0 needs d_work (2 n nlines doubles)");
+        const size_t M = (size_t)n * nlines;
+        e = launch_tdma_lines(n, nlines, d_aw, d_ap, d_ae, d_d, d_x, d_work, d_work + M, (cudaStream_t)stream);
+    } else {
+        if (!tdma_lines_pcr_supported(n)) return fail(ST_TOO_LARGE, "tdma_lines_device: cyclic reduction needs n <= 2048");
+        e = launch_tdma_lines_pcr(n, nlines, d_aw, d_ap, d_ae, d_d, d_x, (cudaStream_t)stream);
+    }
+    if (e != cudaSuccess) { m2d_set_last_error(e, "tdma_lines_device launch", __FILE__, __LINE__); return ST_CUDA; }
+    return ST_OK;
+}
+
 int m2d_norm_l1_5d(const int *nx, const int *ny, const double *var, const double *b,
                    const double *a, double *norm)
 {

@@ -62,6 +62,7 @@ struct m2d_ctx {
     double Href = 0, Cpref = 0, fm1D = 0, Fd1D = 0, Fpv1D = 0, Sg = 0;
     int it = 0, it_stop = -1, itp_used = 0;
     long long launches = 0;   // kernels launched by m2d_iterate so far
+    int msi_variant = 0;      // MSI wavefront schedule (MsiLaunch::variant)
 };
 
 static int ctx_fail(int code, const char *msg)
@@ -309,6 +310,7 @@ static int solve9(m2d_ctx *x, cudaStream_t s, int nsys, double *const *a, double
         memset(&L, 0, sizeof L);
         L.nx = x->nx; L.ny = x->ny; L.nitm = c.nitm_u; L.tol = c.tol_u;
         L.prec = (c.solver >= 2) ? 1 : 0;
+        L.variant = x->msi_variant;
         L.err = x->dint + I_ERR;
         for (int k = 0; k < nsys; k++) {
             L.s[k].a = a[k]; L.s[k].b = b[k]; L.s[k].x = v[k];
@@ -342,6 +344,7 @@ static int solve5(m2d_ctx *x, cudaStream_t s)
         memset(&L, 0, sizeof L);
         L.nx = x->nx; L.ny = x->ny; L.nitm = c.nitm_p; L.tol = c.tol_p;
         L.prec = (c.solver >= 2) ? 1 : 0;
+        L.variant = x->msi_variant;
         L.err = x->dint + I_ERR;
         L.s[0].a = x->f.ap; L.s[0].b = x->f.bp; L.s[0].x = x->f.pl;
         L.s[0].ws = x->ws5;
@@ -444,17 +447,18 @@ __global__ void k_ctx_finish(double *dsc, StepCtl k)
 static int issue_p_cycle(m2d_ctx *x, const Params &q, cudaStream_t s)
 {
     Fields &f = x->f;
-    KL(launch_p_assembly(f, q, ASM_COEF, s), 1);
+    Params qc = q;
+    qc.maxpl = x->dsc + S_MAXPL;    // zeroed by the coefficient pass, maximised by the update
+    KL(launch_p_assembly(f, qc, ASM_COEF, s), 1);
     KL(launch_set_bcpl(f, s), 1);
     KL(launch_p_assembly(f, q, ASM_SRC, s), 1);
     int rc = solve5(x, s);
     if (rc) return rc;
-    KL(launch_velocity_correction_at_faces(f, s), 1);
-    KL(launch_velocities_at_boundary_faces(f, x->c.modvis, s), 1);
-    KL(launch_p_ro_correction(f, 1, 1, s), 1);
+    // face corrections, boundary faces, p and rho corrections and max|p'|
+    // in one pass (bitwise the separate kernels'), then the face densities,
+    // which need the corrected rho of the neighbours
+    KL(launch_p_cycle_update(f, x->c.modvis, x->dsc + S_MAXPL, s), 1);
     KL(launch_density_at_faces(f, x->c.beta, s), 1);
-    RedArgs r = red(x, RED_MAXABS_ALL); r.x = f.pl;
-    KL(launch_reduce(r, x->part, x->dsc + S_MAXPL, s), 1);
     return M2D_OK;
 }
 
@@ -660,6 +664,22 @@ static int build_graph(m2d_ctx *x)
     return M2D_OK;
 }
 
+extern "C" int m2d_ctx_set_msi_schedule(m2d_ctx *x, int variant)
+{
+    if (!x || variant < 0 || variant > 3) return ctx_fail(M2D_ERR_ARG, "m2d_ctx_set_msi_schedule: variant 0..3");
+    TRY(cudaSetDevice(x->device));
+    if (variant != x->msi_variant && x->exec) {
+        // the captured iteration holds the old schedule's launches
+        TRY(cudaStreamSynchronize(x->st));
+        cudaGraphExecDestroy(x->exec);
+        cudaGraphDestroy(x->graph);
+        x->exec = nullptr;
+        x->graph = nullptr;
+    }
+    x->msi_variant = variant;
+    return M2D_OK;
+}
+
 extern "C" int m2d_ctx_set_graph(m2d_ctx *x, int on)
 {
     if (!x) return ctx_fail(M2D_ERR_ARG, "m2d_ctx_set_graph: null context");
@@ -678,41 +698,12 @@ extern "C" int m2d_ctx_set_graph(m2d_ctx *x, int on)
     return M2D_OK;
 }
 
-extern "C" int m2d_iterate(m2d_ctx *x, m2d_report *rep)
+// The report and the checks that close an iteration, once its scalars are
+// in the pinned mirrors (src/mach2d_main.f90:420-443)
+static int finish_iteration(m2d_ctx *x, int it, int itp_used, m2d_report *rep)
 {
-    if (!x) return ctx_fail(M2D_ERR_ARG, "m2d_iterate: null context");
-    TRY(cudaSetDevice(x->device));
     const m2d_case &c = x->c;
-    cudaStream_t st = x->st;
-    const int it = ++x->it;
-    int itp_used = 0;
     const double *hs = x->hsc;
-    if (x->graph_on) {
-        if (!x->exec) {
-            int rc = build_graph(x);
-            if (rc) { x->it--; return rc; }
-        }
-        TRY(cudaGraphLaunch(x->exec, st));
-        TRY(cudaMemcpyAsync(x->hsc, x->dsc, S_COUNT * sizeof(double), cudaMemcpyDeviceToHost, st));
-        TRY(cudaMemcpyAsync(x->hint, x->dint, I_COUNT * sizeof(int), cudaMemcpyDeviceToHost, st));
-        TRY(cudaStreamSynchronize(st));
-        itp_used = x->hint[I_ITP];
-        x->launches += x->launches_fixed + x->launches_body * x->hint[I_ITP_TOTAL];
-        x->p_avg = hs[S_PAVG];
-        x->normpl = hs[S_NORMPL];
-        x->norm = hs[S_NORM];
-        x->dt = hs[S_DT];
-    } else {
-        int rc = issue_iteration(x, false, &itp_used);
-        if (rc) return rc;
-        TRY(cudaMemcpyAsync(x->hsc, x->dsc, S_COUNT * sizeof(double), cudaMemcpyDeviceToHost, st));
-        TRY(cudaMemcpyAsync(x->hint, x->dint, I_COUNT * sizeof(int), cudaMemcpyDeviceToHost, st));
-        TRY(cudaStreamSynchronize(st));
-        double norm, dtn;
-        ctl_finish(step_ctl(c), hs, it, x->dt, &norm, &dtn);
-        x->norm = norm;
-        x->dt = dtn;
-    }
     x->rmass = hs[S_RMASS];
     x->itp_used = itp_used;
     if (rep) {
@@ -725,6 +716,68 @@ extern "C" int m2d_iterate(m2d_ctx *x, m2d_report *rep)
     if (std::isnan(x->norm)) return ctx_fail(M2D_ERR_NAN, "m2d_iterate: NaN detected");
     if (x->normpl < c.tolt && x->it_stop < 0) x->it_stop = it * 2;
     return M2D_OK;
+}
+
+// Captured iterations in two halves, so that a batch can keep every
+// instance's iteration in flight at once: the first queues the iteration's
+// graph and the copies of its scalars on the instance's stream and returns;
+// the second waits for that stream and closes the iteration.  m2d_iterate in
+// graph mode is the two back to back.
+bool ctx_graph_on(const m2d_ctx *x) { return x && x->graph_on; }
+
+int ctx_iterate_launch(m2d_ctx *x)
+{
+    TRY(cudaSetDevice(x->device));
+    ++x->it;
+    if (!x->exec) {
+        int rc = build_graph(x);
+        if (rc) { x->it--; return rc; }
+    }
+    cudaStream_t st = x->st;
+    TRY(cudaGraphLaunch(x->exec, st));
+    TRY(cudaMemcpyAsync(x->hsc, x->dsc, S_COUNT * sizeof(double), cudaMemcpyDeviceToHost, st));
+    TRY(cudaMemcpyAsync(x->hint, x->dint, I_COUNT * sizeof(int), cudaMemcpyDeviceToHost, st));
+    return M2D_OK;
+}
+
+int ctx_iterate_complete(m2d_ctx *x, m2d_report *rep)
+{
+    TRY(cudaSetDevice(x->device));
+    TRY(cudaStreamSynchronize(x->st));
+    const double *hs = x->hsc;
+    const int itp_used = x->hint[I_ITP];
+    x->launches += x->launches_fixed + x->launches_body * x->hint[I_ITP_TOTAL];
+    x->p_avg = hs[S_PAVG];
+    x->normpl = hs[S_NORMPL];
+    x->norm = hs[S_NORM];
+    x->dt = hs[S_DT];
+    return finish_iteration(x, x->it, itp_used, rep);
+}
+
+extern "C" int m2d_iterate(m2d_ctx *x, m2d_report *rep)
+{
+    if (!x) return ctx_fail(M2D_ERR_ARG, "m2d_iterate: null context");
+    if (x->graph_on) {
+        const int rc = ctx_iterate_launch(x);
+        if (rc) return rc;
+        return ctx_iterate_complete(x, rep);
+    }
+    TRY(cudaSetDevice(x->device));
+    const m2d_case &c = x->c;
+    cudaStream_t st = x->st;
+    const int it = ++x->it;
+    int itp_used = 0;
+    const double *hs = x->hsc;
+    int rc = issue_iteration(x, false, &itp_used);
+    if (rc) return rc;
+    TRY(cudaMemcpyAsync(x->hsc, x->dsc, S_COUNT * sizeof(double), cudaMemcpyDeviceToHost, st));
+    TRY(cudaMemcpyAsync(x->hint, x->dint, I_COUNT * sizeof(int), cudaMemcpyDeviceToHost, st));
+    TRY(cudaStreamSynchronize(st));
+    double norm, dtn;
+    ctl_finish(step_ctl(c), hs, it, x->dt, &norm, &dtn);
+    x->norm = norm;
+    x->dt = dtn;
+    return finish_iteration(x, it, itp_used, rep);
 }
 
 extern "C" int m2d_run(m2d_ctx *x, int itmax, m2d_report *last)
@@ -801,7 +854,8 @@ extern "C" int m2d_get_scalar(const m2d_ctx *x, const char *name, double *out)
         {"it_stop", (double)x->it_stop}, {"itp_used", (double)x->itp_used},
         {"launches", (double)x->launches}, {"nit_u", (double)x->hint[I_NIT_U]}, {"nit_v", (double)x->hint[I_NIT_V]},
         {"nit_p", (double)x->hint[I_NIT_P]}, {"nit_T", (double)x->hint[I_NIT_T]},
-        {"learned_calls", (double)x->learned_calls}, {"learned_accepted", (double)x->learned_accepted}};
+        {"learned_calls", (double)x->learned_calls}, {"learned_accepted", (double)x->learned_accepted},
+        {"solver", (double)x->c.solver}, {"msi_schedule", (double)x->msi_variant}};
     for (auto &t : tab)
         if (!strcmp(name, t.nm)) { *out = t.v; return M2D_OK; }
     return ctx_fail(M2D_ERR_ARG, "m2d_get_scalar: unknown scalar");

@@ -33,6 +33,7 @@ struct Params {
     int modvis, coord;
     double beta, dt, Rg, gamma, p0, T0, Cpref, Href, Twall;
     const double *dtp;     // when set, dt is read from this device word (captured iterations)
+    double *maxpl;         // when set, the p' coefficient pass zeroes it for k_p_cycle_update's max|p'|
 };
 
 // what = bit 1: coefficients, bit 2: source (lets one kernel serve both the
@@ -52,6 +53,12 @@ cudaError_t launch_internal_simplec(const Fields &f, cudaStream_t st);
 cudaError_t launch_p_ro_correction(const Fields &f, int do_p, int do_ro, cudaStream_t st);
 cudaError_t launch_uv_nodes_correction(const Fields &f, cudaStream_t st);
 cudaError_t launch_velocity_correction_at_faces(const Fields &f, cudaStream_t st);
+// the p' cycle's update after the solve, in one pass: the face velocities
+// corrected with p' (mach2d_coef.f90:1679-1758) or, on the boundary faces,
+// set by the internal-flow strips (mod_intflow.f90:692-787), p += p' and
+// rho += g p' (mach2d_coef.f90:1602-1624), and max|p'| over every cell into
+// *maxpl (zeroed earlier in the cycle; NaN counts as 0, as fmax drops it)
+cudaError_t launch_p_cycle_update(const Fields &f, int modvis, double *maxpl, cudaStream_t st);
 cudaError_t launch_boundary_faces_flags(const Fields &f, cudaStream_t st);
 cudaError_t launch_set_bcu(const Fields &f, int modvis, cudaStream_t st);
 cudaError_t launch_set_bcv(const Fields &f, int modvis, cudaStream_t st);

@@ -282,6 +282,7 @@ __global__ void __launch_bounds__(kMaxThreads) k_msi(MsiLaunch L)
 cudaError_t launch_msi(int nd, const MsiLaunch &L, int nsys, cudaStream_t st)
 {
     if (L.ny > msi_max_ny() || L.nx < 3 || L.ny < 3) return cudaErrorInvalidValue;
+    if (L.variant == 3 && L.prec == 0) return launch_msi_generic(nd, L, nsys, st);
     if (msi_warp_supported(L.ny)) return launch_msi_warp(nd, L, nsys, st);
     return launch_msi_generic(nd, L, nsys, st);
 }
@@ -486,6 +487,72 @@ cudaError_t launch_tdma_lines(int n, int nlines, const double *aw, const double 
                               double *Q, cudaStream_t st)
 {
     k_tdma_lines<<<(nlines + 63) / 64, 64, 0, st>>>(n, nlines, aw, ap, ae, d, x, P, Q);
+    return cudaGetLastError();
+}
+
+// Parallel cyclic reduction, one CTA per line, the line's four coefficient
+// arrays in shared memory (ping-pong between two copies).  With the line
+// written aw_i x_{i-1} + ap_i x_i + ae_i x_{i+1} = d_i, a step of stride s
+// eliminates x_{i-s} and x_{i+s} from row i with rows i-s and i+s:
+//   k1 = aw_i / ap_{i-s},  k2 = ae_i / ap_{i+s}   (0 past the line's ends)
+//   aw'_i = -aw_{i-s} k1,  ae'_i = -ae_{i+s} k2
+//   ap'_i = ap_i - ae_{i-s} k1 - aw_{i+s} k2
+//   d'_i  = d_i - d_{i-s} k1 - d_{i+s} k2
+// so after ceil(log2 n) steps every row holds one unknown: x_i = d_i / ap_i
+// (Hockney's cyclic reduction in its parallel form).  Global loads and
+// stores are whole coalesced lines.  The rounding differs from the
+// sequential Thomas algorithm (k_tdma_lines); for diagonally dominant lines
+// the two agree to about 1e-15 relative.
+constexpr int kPcrThreads = 256;
+constexpr int kPcrMaxN = 2048;
+
+__global__ void __launch_bounds__(kPcrThreads) k_tdma_lines_pcr(int n, int nlines, const double *__restrict__ aw,
+                                                                const double *__restrict__ ap,
+                                                                const double *__restrict__ ae,
+                                                                const double *__restrict__ d, double *x)
+{
+    extern __shared__ double pcr[];   // 2 copies x {aw, ap, ae, d} x n
+    const int l = blockIdx.x;
+    if (l >= nlines) return;
+    const long long o = (long long)l * n;
+    double *A0 = pcr, *B0 = A0 + n, *C0 = B0 + n, *D0 = C0 + n;
+    double *A1 = D0 + n, *B1 = A1 + n, *C1 = B1 + n, *D1 = C1 + n;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        A0[i] = aw[o + i]; B0[i] = ap[o + i]; C0[i] = ae[o + i]; D0[i] = d[o + i];
+    }
+    __syncthreads();
+    for (int sft = 1; sft < n; sft <<= 1) {
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const int im = i - sft, ip = i + sft;
+            const double k1 = im >= 0 ? A0[i] / B0[im] : 0.0;
+            const double k2 = ip < n ? C0[i] / B0[ip] : 0.0;
+            const double am = im >= 0 ? A0[im] : 0.0, cm = im >= 0 ? C0[im] : 0.0, dm = im >= 0 ? D0[im] : 0.0;
+            const double ap_ = ip < n ? A0[ip] : 0.0, cp = ip < n ? C0[ip] : 0.0, dp = ip < n ? D0[ip] : 0.0;
+            A1[i] = -am * k1;
+            C1[i] = -cp * k2;
+            B1[i] = B0[i] - cm * k1 - ap_ * k2;
+            D1[i] = D0[i] - dm * k1 - dp * k2;
+        }
+        __syncthreads();
+        double *t;
+        t = A0; A0 = A1; A1 = t;
+        t = B0; B0 = B1; B1 = t;
+        t = C0; C0 = C1; C1 = t;
+        t = D0; D0 = D1; D1 = t;
+    }
+    for (int i = threadIdx.x; i < n; i += blockDim.x) x[o + i] = D0[i] / B0[i];
+}
+
+bool tdma_lines_pcr_supported(int n) { return n >= 1 && n <= kPcrMaxN; }
+
+cudaError_t launch_tdma_lines_pcr(int n, int nlines, const double *aw, const double *ap, const double *ae,
+                                  const double *d, double *x, cudaStream_t st)
+{
+    if (!tdma_lines_pcr_supported(n) || nlines < 1) return cudaErrorInvalidValue;
+    const size_t smem = (size_t)8 * n * sizeof(double);
+    cudaError_t e = cudaFuncSetAttribute(k_tdma_lines_pcr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_tdma_lines_pcr<<<nlines, kPcrThreads, smem, st>>>(n, nlines, aw, ap, ae, d, x);
     return cudaGetLastError();
 }
 

@@ -900,12 +900,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
     const int nhelp = (kThreads / 32 / 4) * (4 - WPC);
     const int hw = (wl >> 2) * (4 - WPC) + ((wl & 3) - WPC);
     if (front) {
-        run_lu(std::false_type{});
+        if (!L.reuse_lu) run_lu(std::false_type{});
     } else if (helper) {
         // meanwhile the helper warps compute the initial residual
         helper_residual<ND, TS>(cl, a, S.b, x, rp, nx, ny, SW, red, part, nhelp, hw);
     }
-    up_base += nbatch - 1;
+    if (!L.reuse_lu) up_base += nbatch - 1;
     if (bad_pivot && L.err) atomicOr(L.err, ERR_NONFINITE_PIVOT);
     stamp(L, rank, 1);
 
@@ -920,10 +920,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
     // factor is the IEEE result of its stored inputs; the verdict is read
     // before the first correction of x
     if constexpr (EXACT) {
-        if (helper)
+        if (helper && !L.reuse_lu)
             verify_factors<ND>(asp, dlp, dup, rl1, nx, ny, SW, PS, rank * WPC, WPC, nhelp, hw, &vbad);
     }
-    bool lu_redone = !EXACT;
+    bool lu_redone = !EXACT || L.reuse_lu;   // reused factors were checked when they were made
     int nit = 0;
     double rr = rr0;
     for (;;) {
@@ -1212,11 +1212,15 @@ static cudaError_t launch_cluster(const MsiLaunch &L, int nsys, cudaStream_t st,
         return cudaSuccess;
     }
     *fits = true;
-    // A into wavefront-major order first (all systems, whole GPU)
-    const dim3 sg((unsigned)((L.nx + kSkewPad + kSkewTile - 1) / kSkewTile), (unsigned)nwarps, (unsigned)(nsys * ND));
-    k_skew_a<ND, TS><<<sg, 256, 0, st>>>(L);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
+    // A into wavefront-major order first (all systems, whole GPU), unless the
+    // factors (made from that copy) are reused
+    if (!L.reuse_lu) {
+        const dim3 sg((unsigned)((L.nx + kSkewPad + kSkewTile - 1) / kSkewTile), (unsigned)nwarps,
+                      (unsigned)(nsys * ND));
+        k_skew_a<ND, TS><<<sg, 256, 0, st>>>(L);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
     return cudaLaunchKernelEx(&cfg, kern, L);
 }
 
@@ -1232,9 +1236,13 @@ static cudaError_t launch_nd(const MsiLaunch &L, int nsys, cudaStream_t st, bool
     const bool room = L.ws_cap == 0 || L.ws_cap >= msi_cluster_work_doubles(ND, L.nx, L.ny);
     const bool small = (long long)L.nx * L.ny < (1LL << 31);   // 32-bit cell indices in the passes
     if (!(aligned && room && small)) return cudaSuccess;
-    // fewest wavefront warps per CTA (one SM per warp) whose cluster fits
-    cudaError_t e = launch_cluster<ND, 1, 4, TS>(L, nsys, st, done);
-    if (e != cudaSuccess || *done) return e;
+    // fewest wavefront warps per CTA (one SM per warp) whose cluster fits,
+    // unless the caller asked for one schedule
+    cudaError_t e = cudaSuccess;
+    if (L.variant != 2) {
+        e = launch_cluster<ND, 1, 4, TS>(L, nsys, st, done);
+        if (e != cudaSuccess || *done || L.variant == 1) return e;
+    }
     return launch_cluster<ND, 2, 2, TS>(L, nsys, st, done);
 }
 

@@ -43,6 +43,16 @@ struct MsiLaunch {
                                // sweeps inside the FP64 iteration (cluster kernel only)
     unsigned long long hook_ns;  // test hook of the cluster kernel (set by launch_msi_warp from
                                  // m2d_test_wait_hook; 0: off)
+    int reuse_lu;              // 1: the workspaces already hold these systems' incomplete factors
+                               // (an earlier launch on the same A, sizes, precision and schedule,
+                               // workspace untouched since): the cluster kernel skips the transpose
+                               // of A and the factorisation.  The one-CTA kernel always factorises;
+                               // the results are the same either way.
+    int variant;               // wavefront schedule: 0 automatic (one wavefront warp per SM when the
+                               // cluster fits, else two), 1 one warp per SM (4 staging stages),
+                               // 2 two warps per SM (2 stages), 3 the one-CTA kernel (FP64 only);
+                               // a schedule that cannot run falls back to the one-CTA kernel.  Every
+                               // schedule gives the same iterates.
 };
 
 // Largest ny the one-CTA wavefront kernel accepts (its shared-memory ring
@@ -71,5 +81,10 @@ cudaError_t launch_tdma(int nd, int nx, int ny, int nitm, const double *a, const
 cudaError_t launch_tdma_lines(int n, int nlines, const double *aw, const double *ap,
                               const double *ae, const double *d, double *x, double *P,
                               double *Q, cudaStream_t st);
+// the same lines by parallel cyclic reduction, one CTA per line (n <= 2048);
+// not bitwise equal to the sequential recurrence
+bool tdma_lines_pcr_supported(int n);
+cudaError_t launch_tdma_lines_pcr(int n, int nlines, const double *aw, const double *ap, const double *ae,
+                                  const double *d, double *x, cudaStream_t st);
 
 }  // namespace m2d

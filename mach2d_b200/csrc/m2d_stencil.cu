@@ -379,6 +379,7 @@ __global__ void k_p_assembly(Fields f, Params q, int what)
     const int nx = f.nx, ny = f.ny;
     const long long N = (long long)nx * ny;
     CELL_IJ
+    if (q.maxpl && (what & ASM_COEF) && i == 1 && j == 1) *q.maxpl = 0.0;   // k_p_cycle_update's max|p'|
     if (i < 2 || i > nx - 1 || j < 2 || j > ny - 1) return;
     const long long np = IDX(i, j), nps = np - nx, npn = np + nx, npw = np - 1, npe = np + 1;
     const double *re = f.re, *rn = f.rn, *Uce = f.Uce, *Vcn = f.Vcn, *g = f.g;
@@ -563,6 +564,79 @@ __global__ void k_velocity_correction_faces(Fields f)
         f.Vcn[np] = vn * f.xk[np] - un * f.yk[np] + f.dn[np] * (pl[np] - pl[npn]);
         f.un[np] = un + f.dun[np] * (pl[npn] - pl[np]);
         f.vn[np] = vn + f.dvn[np] * (pl[np] - pl[npn]);
+    }
+}
+
+__device__ __forceinline__ void north_slip_inner(const Fields &f, int i, double &ub, double &vb);
+
+// The p' cycle's update after the solve, fused: every face the reference's
+// get_velocity_correction_at_faces_with_pl corrects (mach2d_coef.f90:
+// 1679-1758) and intflow_velocities_at_boundary_faces then overwrites on the
+// boundary (mod_intflow.f90:692-787) gets its final value directly (the
+// boundary formula on the faces of columns 1 and nx-1 and rows 1 and ny-1,
+// the correction elsewhere); then p += p', rho += g p' (:1602-1624); then
+// max|p'| over all cells: block maxima combined with atomicMax on the bit
+// patterns of non-negative doubles (order-independent, so deterministic).
+// Each expression is the separate kernels', so the results are bitwise
+// theirs.
+__global__ void k_p_cycle_update(Fields f, int modvis, double *maxpl)
+{
+    const int nx = f.nx, ny = f.ny;
+    CELL_IJ
+    double m = 0.0;
+    if (i <= nx && j <= ny) {
+        const long long np = IDX(i, j);
+        const double *pl = f.pl, *u = f.u, *v = f.v;
+        if (j >= 2 && j <= ny - 1 && i <= nx - 1) {
+            const long long npe = np + 1;
+            if (i == 1) {
+                const double ue = (u[np] + u[npe]) / 2.0, ve = 0.0;
+                f.ue[np] = ue; f.ve[np] = ve;
+                f.Uce[np] = ue * f.ye[np] - ve * f.xe[np];
+            } else if (i == nx - 1) {
+                const double ue = (u[np] + u[npe]) / 2.0, ve = (v[np] + v[npe]) / 2.0;
+                f.ue[np] = ue; f.ve[np] = ve;
+                f.Uce[np] = ue * f.ye[np] - ve * f.xe[np];
+            } else {
+                const double ue = f.ue[np], ve = f.ve[np];
+                f.Uce[np] = ue * f.ye[np] - ve * f.xe[np] + f.de[np] * (pl[np] - pl[npe]);
+                f.ue[np] = ue + f.due[np] * (pl[np] - pl[npe]);
+                f.ve[np] = ve + f.dve[np] * (pl[npe] - pl[np]);
+            }
+        }
+        if (j <= ny - 1 && i >= 2 && i <= nx - 1) {
+            const long long npn = np + nx;
+            if (j == 1) {
+                f.un[np] = (u[np] + u[npn]) / 2.0;
+                f.vn[np] = 0.0;
+                f.Vcn[np] = 0.0;
+            } else if (j == ny - 1) {
+                double ub = 0.0, vb = 0.0;
+                if (modvis == 0) north_slip_inner(f, i, ub, vb);
+                f.un[np] = ub; f.vn[np] = vb; f.Vcn[np] = 0.0;
+            } else {
+                const double un = f.un[np], vn = f.vn[np];
+                f.Vcn[np] = vn * f.xk[np] - un * f.yk[np] + f.dn[np] * (pl[np] - pl[npn]);
+                f.un[np] = un + f.dun[np] * (pl[npn] - pl[np]);
+                f.vn[np] = vn + f.dvn[np] * (pl[np] - pl[npn]);
+            }
+        }
+        const double p1 = pl[np];
+        f.p[np] = f.p[np] + p1;
+        f.ro[np] = f.ro[np] + p1 * f.g[np];
+        m = fmax(0.0, fabs(p1));
+    }
+    // block maximum, then one atomic per block
+    __shared__ double wmax[8];
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    const int w = threadIdx.y, lane = threadIdx.x;
+    if (lane == 0) wmax[w] = m;
+    __syncthreads();
+    if (w == 0) {
+        m = lane < 8 ? wmax[lane] : 0.0;
+        for (int o = 4; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (lane == 0 && maxpl)
+            atomicMax(reinterpret_cast<unsigned long long *>(maxpl), (unsigned long long)__double_as_longlong(m));
     }
 }
 
@@ -1042,6 +1116,8 @@ cudaError_t launch_uv_nodes_correction(const Fields &f, cudaStream_t st)
 { k_uv_nodes_correction<<<grid2d(f.nx, f.ny), kBlock2d, 0, st>>>(f); return cudaGetLastError(); }
 cudaError_t launch_velocity_correction_at_faces(const Fields &f, cudaStream_t st)
 { k_velocity_correction_faces<<<grid2d(f.nx, f.ny), kBlock2d, 0, st>>>(f); return cudaGetLastError(); }
+cudaError_t launch_p_cycle_update(const Fields &f, int modvis, double *maxpl, cudaStream_t st)
+{ k_p_cycle_update<<<grid2d(f.nx, f.ny), kBlock2d, 0, st>>>(f, modvis, maxpl); return cudaGetLastError(); }
 cudaError_t launch_boundary_faces_flags(const Fields &f, cudaStream_t st)
 { k_boundary_faces_flags<<<grid2d(f.nx, f.ny), kBlock2d, 0, st>>>(f); return cudaGetLastError(); }
 cudaError_t launch_set_bcu(const Fields &f, int modvis, cudaStream_t st)

@@ -1414,6 +1414,30 @@ extern "C" long m2d_msi_workspace_doubles(int nd, int nx, int ny);
 // only if it lowers |b - A x|; then the MSI iteration (at least one, as in
 // plain MSI), whose stopping test stays relative to the residual before the
 // correction.
+namespace m2d {
+// x_out = x + the network's correction for the 5-diagonal system A x = b
+// (features of r = b - A x), with no acceptance test: the preconditioner of
+// the flexible GMRES (m2d_krylov.cu).  x_out must not alias x.
+cudaError_t unet_correct(m2d_unet *n, int nx, int ny, const double *d_a, const double *d_b, const double *d_x,
+                         double *d_xout, const double *d_Jp, cudaStream_t st)
+{
+    if (!image_fits(nx, ny, n->H, n->W)) return cudaErrorInvalidValue;
+    const int H = n->H, W = n->W;
+    const long long N = (long long)nx * ny;
+    double *s = n->stats;
+    k_residual5<<<grid_for(N), 256, 0, st>>>(nx, ny, d_a, d_b, d_x, n->r);
+    k_sys_stats<<<1, kStatThreads, 0, st>>>(nx, ny, d_a, n->r, d_Jp, s, 1);
+    k_features<<<grid_for((long long)H * W), 256, 0, st>>>(nx, ny, H, W, d_a, n->r, d_Jp, s, n->feat);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = forward(n, 1, n->feat, n->yout, false, st);
+    if (e == cudaSuccess) {
+        k_apply<<<grid_for(N), 256, 0, st>>>(nx, ny, H, W, d_a, d_b, n->yout, s, d_x, d_xout);
+        e = cudaGetLastError();
+    }
+    return e;
+}
+}  // namespace m2d
+
 extern "C" int m2d_pprime_solve_learned(m2d_unet *n, int nx, int ny, int nitm, double tol, const double *d_a,
                                         const double *d_b, double *d_x, const double *d_Jp, double *d_work, int prec,
                                         void *stream, m2d_learned_report *rep)

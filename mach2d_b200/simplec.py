@@ -180,6 +180,13 @@ class Simplec:
                             self.scalar("Sg"), rcg, ig, gamma, c.p0, self.scalar("Fpv1D"), self.scalar("Fd1D"),
                             self.scalar("fm1D"), rep.fme)
 
+    def set_msi_schedule(self, variant):
+        """m2d_ctx_set_msi_schedule: 0 automatic, 1 one wavefront warp per SM,
+        2 two per SM, 3 the one-CTA kernel (same iterates)."""
+        L = lib()
+        L.m2d_ctx_set_msi_schedule.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        check(L.m2d_ctx_set_msi_schedule(self._ctx, int(variant)))
+
     def set_graph(self, on=True):
         """Run each outer iteration as one captured CUDA graph (m2d_ctx_set_graph)."""
         L = lib()
@@ -311,6 +318,24 @@ class Batch:
         L.m2d_batch_iterate.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(Report)]
         check(L.m2d_batch_iterate(self._b, int(iters), reps))
         return list(reps)
+
+    def set_msi_schedule(self, variant):
+        """m2d_batch_set_msi_schedule: the MSI wavefront schedule of every instance."""
+        L = lib()
+        L.m2d_batch_set_msi_schedule.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        check(L.m2d_batch_set_msi_schedule(self._b, int(variant)))
+
+    def autotune(self, iters=2):
+        """m2d_batch_autotune: runs the batch's next iterations with each
+        candidate MSI schedule and keeps the fastest.  Returns (chosen,
+        {schedule: ms per batch iteration})."""
+        L = lib()
+        L.m2d_batch_autotune.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                         ctypes.POINTER(ctypes.c_double)]
+        chosen = ctypes.c_int()
+        ms = (ctypes.c_double * 4)()
+        check(L.m2d_batch_autotune(self._b, int(iters), ctypes.byref(chosen), ms))
+        return chosen.value, {v: ms[v] for v in range(4) if ms[v] >= 0}
 
     def close(self):
         if self._b:

@@ -132,3 +132,43 @@ def _mat(a, k, n):
     if a.size != k * n:
         raise ValueError(f"coefficient array must hold {k} planes of {n}")
     return a
+
+
+class FgmresReport:
+    """m2d_fgmres_report of include/mach2d_b200.h."""
+
+    def __init__(self, raw):
+        for k in ("iterations", "msi_applications", "learned_applications", "cycles", "converged", "rel_residual"):
+            setattr(self, k, getattr(raw, k))
+
+
+def fgmres(nd, nx, ny, a, b, x, tol, prec=0, restart=30, maxit=1000, net=None, Jp=None, work=None, stream=None):
+    """Flexible GMRES with the MSI factorisation (prec 0 FP64, 1 FP32) or the
+    learned correction plus one FP32 MSI step (prec 2, nd = 5) as its
+    preconditioner (m2d_fgmres_solve).  a, b, x, Jp: CUDA float64 tensors in
+    the reference layout; x is updated in place.  Returns an FgmresReport;
+    raises M2DError unless |b - A x| <= tol |b| within maxit steps."""
+    import ctypes
+
+    import torch
+
+    from ._lib import check, lib
+
+    class _Rep(ctypes.Structure):
+        _fields_ = [("iterations", ctypes.c_int), ("msi_applications", ctypes.c_int),
+                    ("learned_applications", ctypes.c_int), ("cycles", ctypes.c_int), ("converged", ctypes.c_int),
+                    ("rel_residual", ctypes.c_double)]
+
+    L = lib()
+    L.m2d_fgmres_workspace_doubles.restype = ctypes.c_long
+    L.m2d_fgmres_workspace_doubles.argtypes = [ctypes.c_int] * 4
+    L.m2d_fgmres_solve.argtypes = ([ctypes.c_int] * 5 + [ctypes.c_double] + [ctypes.c_void_p] * 3 + [ctypes.c_int]
+                                   + [ctypes.c_void_p] * 4 + [ctypes.POINTER(_Rep)])
+    if work is None:
+        work = torch.empty(L.m2d_fgmres_workspace_doubles(nd, nx, ny, restart), dtype=torch.float64,
+                           device=x.device)
+    rep = _Rep()
+    check(L.m2d_fgmres_solve(nd, nx, ny, restart, maxit, tol, a.data_ptr(), b.data_ptr(), x.data_ptr(), prec,
+                             None if net is None else net._h, None if Jp is None else Jp.data_ptr(),
+                             work.data_ptr(), stream, ctypes.byref(rep)))
+    return FgmresReport(rep)

@@ -38,12 +38,16 @@ def gather_results(local, n, group=None):
     return [merged[i] for i in range(n)]
 
 
-def run_shard(cases, indices, device, iters, graph=True, timings=None):
+def run_shard(cases, indices, device, iters, graph=True, timings=None, tune=0):
     """Advances the cases at `indices` as one batch on `device`: `iters` outer
     iterations each (or, with iters <= 0, each to its stopping iteration, at
     most 100000).  Returns ({index: (it, normpl, fmi, fme, Fd, Cd)}, seconds).
     With a dict `timings`, also records the batch set-up time in
-    timings["setup_s"] (grids, metrics and initial fields of every instance)."""
+    timings["setup_s"] (grids, metrics and initial fields of every instance).
+    With tune > 0 (and graph), the batch's MSI schedule is first autotuned on
+    the batch's own next iterations (m2d_batch_autotune, `tune` timed
+    iterations per candidate; the schedules give the same iterates), and
+    timings["schedule"] records the choice and the candidates' times."""
     import torch
 
     from .simplec import Batch
@@ -60,6 +64,11 @@ def run_shard(cases, indices, device, iters, graph=True, timings=None):
     if graph:
         for s in b.instances:
             s.set_graph(True)
+        if tune > 0:
+            chosen, ms = b.autotune(tune)
+            if timings is not None:
+                timings["schedule"] = {"chosen": chosen, "ms_per_batch_iteration": ms,
+                                       "tuning_iterations": (1 + tune) * len(ms)}
     torch.cuda.synchronize(device)
     t0 = time.perf_counter()
     if iters > 0:

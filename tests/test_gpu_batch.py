@@ -80,3 +80,62 @@ def test_batch_set_up_failure_names_the_instance_and_keeps_none():
     b = Batch(_cases()[:2], workers=2)                  # the device is still usable
     assert b.iterate(1)[1].it == 1
     b.close()
+
+
+def test_concurrent_captured_batch_equals_solo_runs():
+    """Every instance's captured iteration in flight at once (graph mode):
+    each instance still gets bitwise the results of running it alone."""
+    iters = 10
+    b = Batch(_cases(), workers=1)
+    for s in b.instances:
+        s.set_graph(True)
+    reps = b.iterate(iters)
+    for k, case in enumerate(_cases()):
+        solo = Simplec(case)
+        for _ in range(iters):
+            r = solo.iterate()
+        for c in REPORT:
+            assert getattr(reps[k], c) == getattr(r, c), (k, c)
+        for f in FIELDS:
+            assert np.array_equal(b.instances[k].field(f), solo.field(f)), (k, f)
+        solo.close()
+    b.close()
+
+
+@pytest.mark.parametrize("solver,variants", [(0, (0, 1, 2, 3)), (2, (0, 1, 2))])
+def test_msi_schedules_give_the_same_iterates(solver, variants):
+    case = euler_cosine_case(96, 70, solver=solver)          # three row groups of 32
+    runs = []
+    for v in variants:
+        g = Simplec(case)
+        g.set_msi_schedule(v)
+        g.set_graph(v % 2 == 0)
+        reps = [g.iterate() for _ in range(6)]
+        runs.append(([tuple(getattr(r, c) for c in REPORT) for r in reps], [g.field(f) for f in FIELDS]))
+        g.close()
+    for hist, fields in runs[1:]:
+        assert hist == runs[0][0]
+        for a, b in zip(fields, runs[0][1]):
+            assert np.array_equal(a, b)
+
+
+def test_autotuned_batch_equals_untuned_batch():
+    cases = _cases()
+    tuned = Batch(cases, workers=2)
+    plain = Batch(cases, workers=2)
+    for s in tuned.instances + plain.instances:
+        s.set_graph(True)
+    chosen, ms = tuned.autotune(1)
+    assert chosen in ms and set(ms) == {1, 2, 3}
+    done = int(tuned.instances[0].scalar("it"))
+    assert done == 2 * len(ms)
+    r_t = tuned.iterate(4)
+    r_p = plain.iterate(done + 4)
+    for k in range(len(cases)):
+        for c in REPORT:
+            assert getattr(r_t[k], c) == getattr(r_p[k], c), (k, c)
+        for f in FIELDS:
+            assert np.array_equal(tuned.instances[k].field(f), plain.instances[k].field(f)), (k, f)
+        assert tuned.instances[k].scalar("msi_schedule") == chosen
+    tuned.close()
+    plain.close()

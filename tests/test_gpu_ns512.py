@@ -9,6 +9,9 @@ last bit, and the run amplifies such differences slowly), the p' cycle
 counts agree exactly, and the run stops with a NaN at the same iteration as
 the oracle's: the Scarborough time step grows past what the scheme
 tolerates, a property of the algorithm that both implementations share.
+The same holds with the Baldwin-Lomax eddy viscosity wired in (modtur = 1,
+Pr_t = 0.9; fixture ns512_bl_mixture_trace.json): the configuration the
+turbulent 512 x 256 case specifies.
 """
 import json
 import os
@@ -23,17 +26,18 @@ pytestmark = pytest.mark.gpu
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
 
 
-def _case():
+def _case(modtur):
     d = json.load(open(os.path.join(GOLD, "air_species.json")))
     mix = mixture_init(d["base"], d["fractions"], d["Mi"], d["cpi"], d["mui"], d["kpi"])
     return euler_cosine_case(512, 256, modvis=1, kg=2, a1=1e-6, p0=2e6, T0=1500.0, Twall=-1.0, ktm=1, mix=mix,
-                             solver=0)
+                             solver=0, modtur=modtur, prt=0.9)
 
 
-def test_ns512_mixture_history_matches_oracle():
-    gold = json.load(open(os.path.join(GOLD, "ns512_mixture_trace.json")))
+@pytest.mark.parametrize("modtur,trace", [(0, "ns512_mixture_trace.json"), (1, "ns512_bl_mixture_trace.json")])
+def test_ns512_mixture_history_matches_oracle(modtur, trace):
+    gold = json.load(open(os.path.join(GOLD, trace)))
     rows = {r[0]: r for r in gold["every25"]}
-    g = Simplec(_case())
+    g = Simplec(_case(modtur))
     stop = None
     for it in range(1, gold["nan_at"] + 1 if gold["nan_at"] else 3001):
         try:

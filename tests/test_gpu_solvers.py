@@ -117,6 +117,37 @@ def test_tdma_lines_bitwise():
         assert np.array_equal(x[l], xo)
 
 
+@pytest.mark.parametrize("n,nlines", [(1024, 512), (1000, 37), (7, 5), (2048, 3)])
+def test_tdma_lines_device_both_methods(n, nlines):
+    """m2d_tdma_lines_device: method 0 (the sequential recurrence) bitwise the
+    oracle's line sweep; method 1 (parallel cyclic reduction) within 1e-12
+    of it relative to max|x| (the isolated-system lines, aP = 1.05 (|aW| +
+    |aE|), are strongly diagonally dominant)."""
+    import ctypes
+
+    import torch
+    from mach2d_b200._lib import check, lib
+    dev = torch.device("cuda:0")
+    aw, ap, ae, d = tdma_lines_system(n=n, nlines=nlines, seed=n + nlines)
+    xo = np.zeros((nlines, n))
+    for l in range(nlines):
+        orc("tdma_line", n, aw[l].copy(), ap[l].copy(), ae[l].copy(), d[l].copy(), xo[l])
+    L = lib()
+    L.m2d_tdma_lines_device.argtypes = [ctypes.c_int, ctypes.c_int] + [ctypes.c_void_p] * 6 + [ctypes.c_int,
+                                                                                                ctypes.c_void_p]
+    t = [torch.from_numpy(np.ascontiguousarray(v)).to(dev) for v in (aw, ap, ae, d)]
+    work = torch.empty(2 * n * nlines, dtype=torch.float64, device=dev)
+    for method in (0, 1):
+        x = torch.zeros(nlines, n, dtype=torch.float64, device=dev)
+        check(L.m2d_tdma_lines_device(n, nlines, *[v.data_ptr() for v in t], x.data_ptr(), work.data_ptr(), method,
+                                      None))
+        xg = x.cpu().numpy()
+        if method == 0:
+            assert np.array_equal(xg, xo)
+        else:
+            assert np.max(np.abs(xg - xo)) <= 1e-12 * np.max(np.abs(xo))
+
+
 def test_norms_match_oracle():
     nx, ny = 60, 31
     a9, b = random_dominant_planes(9, nx, ny, seed=5)
