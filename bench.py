@@ -427,6 +427,8 @@ def run_ours(args):
     if world == 1 and args.batch > 0:
         from mach2d_b200.simplec import Batch
         b = Batch([make_case(args.nxr, args.nyr) for _ in range(args.batch)], device=local)
+        for inst in b.instances:
+            inst.set_graph(True)       # every instance's captured iteration in flight at once
         b.iterate(max(1, args.warmup))
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -441,7 +443,8 @@ def run_ours(args):
                                    "note": "the single instance's bytes per outer iteration x instances x steps "
                                            "/ wall time"},
                  "timing": "host wall clock around m2d_batch_iterate with device synchronisation",
-                 "note": "independent instances of the same workload, one context and stream each"}
+                 "note": "independent instances of the same workload, one context and stream each, every "
+                         "instance's captured iteration in flight at once"}
         b.close()
 
     extras = {}
@@ -528,6 +531,8 @@ def run_extras(args, local):
 
     # time to the stopping residual (normpl < 1e-10 first at it, stop at 2 it) of the 80x40 nozzle
     ttr = {"case": "C01 Euler 80x40, tolt 1e-10, SCARBOROUGH", "metric": "seconds to the stopping iteration"}
+    fin = json.load(open(os.path.join(ROOT, "tests", "golden", "bench_workloads.json")))["c01_euler_80x40_converged"][
+        "final"]
     for solver, key in ((0, "gpu_fp64"), (2, "gpu_fp32_sweeps")):
         g = Simplec(euler_cosine_case(80, 40, solver=solver), device=local)
         g.set_graph(True)
@@ -535,9 +540,17 @@ def run_extras(args, local):
         t0 = time.perf_counter()
         rep = g.run(200000)
         torch.cuda.synchronize()
-        ttr[key] = {"seconds": time.perf_counter() - t0, "iterations": rep.it, "normpl": rep.normpl,
-                    "Cd": g.integrals()[3]}
+        fmi, fme, Fd, Cd, pw = g.integrals()
+        pr = np.asarray(fin["pwall"])
+        ttr[key] = {"seconds": time.perf_counter() - t0, "iterations": rep.it, "normpl": rep.normpl, "Cd": Cd,
+                    "rel_err_vs_oracle": {"Cd": abs(Cd - fin["Cd"]) / abs(fin["Cd"]),
+                                          "fmi": abs(fmi - fin["fmi"]) / abs(fin["fmi"]),
+                                          "fme": abs(fme - fin["fme"]) / abs(fin["fme"]),
+                                          "Fd": abs(Fd - fin["Fd"]) / abs(fin["Fd"]),
+                                          "pwall_max": float(np.max(np.abs(pw - pr)) / np.max(np.abs(pr)))}}
         g.close()
+    ttr["oracle_converged"] = {"iterations": fin["it"], "Cd": fin["Cd"],
+                               "fixture": "tests/golden/bench_workloads.json (make_bench_golden.py)"}
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from _oracle import OracleCase
     o = OracleCase(euler_cosine_case(80, 40))
@@ -599,6 +612,8 @@ def run_extras(args, local):
         out["time_to_residual_512x256"] = run_ttr512(local, one, args.ttr_cap)
     one.close()
     out["isolated_system"] = run_isolated(local)
+    out["krylov"] = run_krylov(local)
+    out["config3"] = run_config3(args, local)
     out["learned"] = {
         "train": {"pairs": pairs.n, "steps": 300, "batch": 8, "seconds": train_s, "loss_first": hist[0],
                   "loss_last50": float(np.mean(hist[-50:]))},
@@ -607,6 +622,59 @@ def run_extras(args, local):
         "p_solve_ms_median": {k: 1e3 * float(np.median(v)) for k, v in res.items()},
         "msi_iterations_mean": {k: float(np.mean(v)) for k, v in nits.items()},
         "tolerance": "p' solve to |r| < 1e-2 |r0| (nitm_p = 20), host clock per solve"}
+    return out
+
+
+def config3_case(solver):
+    """The turbulent 512x256 case: C01 nozzle, Navier-Stokes, MIXTURE air,
+    Baldwin-Lomax eddy viscosity (Pr_t 0.9), geometric wall clustering with a
+    1e-6 m first cell, p0 = 2 MPa, T0 = 1500 K, adiabatic wall."""
+    from mach2d_b200.simplec import euler_cosine_case
+    from mach2d_b200.thermo import mixture_init
+    d = json.load(open(os.path.join(ROOT, "tests", "golden", "air_species.json")))
+    mix = mixture_init(d["base"], d["fractions"], d["Mi"], d["cpi"], d["mui"], d["kpi"])
+    return euler_cosine_case(512, 256, modvis=1, kg=2, a1=1e-6, p0=2e6, T0=1500.0, Twall=-1.0, ktm=1, mix=mix,
+                             solver=solver, modtur=1, prt=0.9)
+
+
+def run_config3(args, local, warm=5, steps=20):
+    """Throughput of the turbulent 512x256 case over outer iterations
+    warm+1 .. warm+steps (FP64 MSI, and FP32 sweeps), device time of the
+    captured iterations, and the serial oracle on the same iterations."""
+    import torch
+
+    from mach2d_b200.simplec import Simplec
+    out = {"case": "C01 512x256 Navier-Stokes + MIXTURE air + Baldwin-Lomax (Pr_t 0.9), first cell 1e-6 m, "
+                   "p0 2 MPa, T0 1500 K, adiabatic wall", "iterations_timed": [warm + 1, warm + steps]}
+    cells = 512 * 256
+    for solver, key in ((0, "gpu_fp64"), (2, "gpu_fp32_sweeps")):
+        g = Simplec(config3_case(solver), device=local)
+        g.set_graph(True)
+        for _ in range(warm):
+            g.iterate()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            r = g.iterate()
+        torch.cuda.synchronize()
+        secs = time.perf_counter() - t0
+        out[key] = {"value": cells * steps / secs, "unit": "cell-updates/s", "ms_per_step": 1e3 * secs / steps,
+                    "normpl_last": r.normpl}
+        g.close()
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from _oracle import OracleCase
+    o = OracleCase(config3_case(0))
+    for _ in range(warm):
+        o.iterate()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        o.iterate()
+    secs = time.perf_counter() - t0
+    out["cpu_oracle_serial"] = {"value": cells * steps / secs, "unit": "cell-updates/s", "cores": 1,
+                                "ms_per_step": 1e3 * secs / steps}
+    out["note"] = ("host clock around iterations that each end in a read-back; the run stops with a NaN at "
+                   "iteration 982 in both implementations (tests/test_gpu_ns512.py), so no time to a residual "
+                   "of 1e-8 exists for this case")
     return out
 
 
@@ -690,6 +758,107 @@ def isolated_system9(nx, ny, seed=1, dominance=1.05):
     a[4] = np.where(inner, dominance * np.abs(a).sum(axis=0), 1.0)
     b = np.where(inner, rng.standard_normal((ny, nx)), 0.0)
     return a.reshape(-1).copy(), b.reshape(-1).copy()
+
+
+def isolated_system5(nx, ny, seed=1, dominance=1.05):
+    """The 5-diagonal analogue of the isolated system (the p' system's
+    stencil): the S, W, E, N couplings of isolated_system9 with aP = 1.05
+    sum|a_nb| of those four."""
+    import numpy as np
+    a9, b = isolated_system9(nx, ny, seed, dominance)
+    N = nx * ny
+    a = a9.reshape(9, N)[[1, 3, 4, 5, 7]].copy()
+    inner = np.zeros((ny, nx), bool)
+    inner[1:-1, 1:-1] = True
+    a[2] = np.where(inner.ravel(), dominance * np.abs(a[[0, 1, 3, 4]]).sum(axis=0), 1.0)
+    return a.reshape(-1).copy(), b
+
+
+def _timed(fn, reps=2):
+    """Host time of the last of `reps` calls of fn() (each synchronising)."""
+    import torch
+    out = None
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = fn()
+        torch.cuda.synchronize()
+        secs = time.perf_counter() - t0
+    return 1e3 * secs, out
+
+
+def run_krylov(local, nx=1026, ny=514, tol=1e-12, train_systems=48, train_steps=1000):
+    """Flexible GMRES (m2d_fgmres_solve) against MSI iterated alone on the
+    isolated systems at 1024x512 real cells: the 9-diagonal one with the MSI
+    factorisation as preconditioner (FP64, FP32), and the 5-diagonal one also
+    with the learned correction followed by one FP32 MSI step as the
+    preconditioner; the network is trained here, by the library's kernels,
+    on the MSI solutions of `train_systems` other seeds of the same system."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    from mach2d_b200 import unet
+    from mach2d_b200._lib import check, lib
+    from mach2d_b200.solvers import fgmres
+    dev = torch.device("cuda", local)
+    L = lib()
+    L.m2d_msi_workspace_doubles.restype = ctypes.c_long
+    L.m2d_msi_workspace_doubles.argtypes = [ctypes.c_int] * 3
+    for fn in ("m2d_msi_solve_device", "m2d_msi_solve_device_mixed"):
+        getattr(L, fn).argtypes = [ctypes.c_int] * 4 + [ctypes.c_double] + [ctypes.c_void_p] * 6
+    out = {"tolerance": tol, "metric": "host ms per solve to |b - A x| <= tol |b| from x = 0, restart 30"}
+    Jp = torch.ones(nx * ny, dtype=torch.float64, device=dev)
+    one = None
+    for nd in (9, 5):
+        a, b = isolated_system9(nx, ny) if nd == 9 else isolated_system5(nx, ny)
+        da, db = torch.from_numpy(a).to(dev), torch.from_numpy(b).to(dev)
+        ws = torch.empty(L.m2d_msi_workspace_doubles(nd, nx, ny), dtype=torch.float64, device=dev)
+        nit = torch.zeros(2, dtype=torch.int32, device=dev)
+        e = {"system": f"{nd}-diagonal {nx - 2}x{ny - 2}, aP = 1.05 sum|a_nb|, seed 1"}
+        for key, fn in (("msi_fp64", "m2d_msi_solve_device"), ("msi_fp32_refined", "m2d_msi_solve_device_mixed")):
+            def run(fn=fn):
+                x = torch.zeros(nx * ny, dtype=torch.float64, device=dev)
+                check(getattr(L, fn)(nd, nx, ny, 5000, tol, da.data_ptr(), db.data_ptr(), x.data_ptr(),
+                                     ws.data_ptr(), None, nit.data_ptr()))
+            ms, _ = _timed(run)
+            e[key] = {"ms": ms, "msi_iterations": int(nit[0].item())}
+        if nd == 5:
+            H, W = unet.image_shape(nx, ny)
+            systems = []
+            for sd in range(100, 100 + train_systems):
+                a_t, b_t = isolated_system5(nx, ny, sd)
+                systems.append((torch.from_numpy(a_t).to(dev), torch.from_numpy(b_t).to(dev)))
+            pairs = unet.PairSet(len(systems), H, W, device=local)
+            unet.harvest_systems(systems, nx, ny, Jp, pairs)
+            del systems
+            net = unet.UNet(8, H, W, device=local, seed=1)
+            t0 = time.perf_counter()
+            hist = unet.train(net, pairs, train_steps, batch=8, lr=2e-3, lr_final=1e-4)
+            torch.cuda.synchronize()
+            e["learned_training"] = {"systems": pairs.n, "steps": train_steps, "seconds": time.perf_counter() - t0,
+                                     "loss_first": hist[0], "loss_last50": float(np.mean(hist[-50:]))}
+            one = unet.UNet(1, H, W, device=local, params=net.params())
+            net.close()
+            del pairs
+        for key, prec in (("fgmres_msi_fp64", 0), ("fgmres_msi_fp32", 1), ("fgmres_learned_fp32", 2)):
+            if prec == 2 and nd != 5:
+                continue
+
+            def run(prec=prec):
+                x = torch.zeros(nx * ny, dtype=torch.float64, device=dev)
+                return fgmres(nd, nx, ny, da, db, x, tol, prec=prec, restart=30, net=one if prec == 2 else None,
+                              Jp=Jp if prec == 2 else None)
+            ms, r = _timed(run)
+            e[key] = {"ms": ms, "krylov_steps": r.iterations, "msi_applications": r.msi_applications,
+                      "learned_applications": r.learned_applications, "relative_residual": r.rel_residual}
+        base = e["msi_fp64"]["ms"]
+        e["speedup_vs_msi_fp64"] = {k: base / e[k]["ms"] for k in e if k.startswith("fgmres")}
+        out[f"nd{nd}"] = e
+    if one is not None:
+        one.close()
+    return out
 
 
 def run_isolated(local, nx=1026, ny=514, tol=1e-12):

@@ -149,7 +149,7 @@ int fail(int code, const char *msg)
 
 struct Layout {
     long long N;
-    double *V, *Z, *w, *ws, *part, *h;
+    double *V, *Z, *w, *t, *ws, *part, *h;
     size_t ws_doubles;
 };
 
@@ -164,6 +164,7 @@ Layout layout(int nd, int nx, int ny, int m, double *base)
     L.V = p; p += (size_t)(m + 1) * Na;
     L.Z = p; p += (size_t)m * Na;
     L.w = p; p += Na;
+    L.t = p; p += Na;
     L.ws_doubles = align32(msi_work_doubles(nd, nx, ny) + 4);
     L.ws = p; p += L.ws_doubles;
     L.part = p; p += align32((size_t)kMaxRestart * kBlocks);
@@ -174,7 +175,7 @@ Layout layout(int nd, int nx, int ny, int m, double *base)
 size_t workspace_doubles(int nd, int nx, int ny, int m)
 {
     const size_t Na = align32((size_t)nx * ny);
-    return (size_t)(2 * m + 2) * Na + align32(msi_work_doubles(nd, nx, ny) + 4) + align32((size_t)kMaxRestart * kBlocks)
+    return (size_t)(2 * m + 3) * Na + align32(msi_work_doubles(nd, nx, ny) + 4) + align32((size_t)kMaxRestart * kBlocks)
            + align32(2 * kMaxRestart + 8);
 }
 
@@ -221,23 +222,19 @@ extern "C" int m2d_fgmres_solve(int nd, int nx, int ny, int restart, int maxit, 
         if (ee == cudaSuccess) ee = cudaStreamSynchronize(st);
         return ee;
     };
-    // the preconditioner: z = P(v)
-    auto precondition = [&](const double *v, double *z) -> cudaError_t {
-        cudaError_t ee = cudaMemsetAsync(z, 0, (size_t)N * sizeof(double), st);
+    // one application of the factors: y = (LU)^-1 rhs, y zeroed here; the
+    // first call of a solve also factorises (and runs the full iteration
+    // step, which from y = 0 gives the same y)
+    auto apply_factors = [&](const double *rhs, double *y) -> cudaError_t {
+        cudaError_t ee = cudaMemsetAsync(y, 0, (size_t)N * sizeof(double), st);
         if (ee != cudaSuccess) return ee;
-        if (prec == 2) {
-            // z = N(v) from the zero guess (W.w is free here), then MSI from z
-            ee = cudaMemsetAsync(W.w, 0, (size_t)N * sizeof(double), st);
-            if (ee == cudaSuccess) ee = unet_correct(net, nx, ny, d_a, v, W.w, z, d_Jp, st);
-            if (ee != cudaSuccess) return ee;
-            net_apps++;
-        }
         MsiLaunch L;
         memset(&L, 0, sizeof L);
         L.nx = nx; L.ny = ny; L.nitm = 1; L.tol = 0.0;
         L.prec = (prec >= 1) ? 1 : 0;
         L.reuse_lu = factored ? 1 : 0;
-        L.s[0].a = d_a; L.s[0].b = v; L.s[0].x = z;
+        L.apply_only = factored ? 1 : 0;
+        L.s[0].a = d_a; L.s[0].b = rhs; L.s[0].x = y;
         L.s[0].ws = W.ws;
         L.s[0].rr = W.ws + (W.ws_doubles - 4);
         L.ws_cap = W.ws_doubles - 4;
@@ -245,6 +242,23 @@ extern "C" int m2d_fgmres_solve(int nd, int nx, int ny, int restart, int maxit, 
         factored = true;
         msi_apps++;
         return ee;
+    };
+    // the preconditioner: z = P(v)
+    auto precondition = [&](const double *v, double *z) -> cudaError_t {
+        if (prec != 2) return apply_factors(v, z);
+        // z = N(v) from the zero guess, then z += (LU)^-1 (v - A z)
+        cudaError_t ee = cudaMemsetAsync(W.w, 0, (size_t)N * sizeof(double), st);
+        if (ee == cudaSuccess) ee = unet_correct(net, nx, ny, d_a, v, W.w, z, d_Jp, st);
+        if (ee != cudaSuccess) return ee;
+        net_apps++;
+        apply_a(z, W.t, v, 1);
+        ee = apply_factors(W.t, W.w);
+        if (ee != cudaSuccess) return ee;
+        const double one = 1.0;
+        ee = cudaMemcpyAsync(W.h + 2 * kMaxRestart, &one, sizeof(double), cudaMemcpyHostToDevice, st);
+        if (ee != cudaSuccess) return ee;
+        k_multi_axpy<<<g, kThreads, 0, st>>>(1, N, (long long)Na, W.w, W.h + 2 * kMaxRestart, 1.0, z);
+        return cudaGetLastError();
     };
 
     e = cudaSuccess;

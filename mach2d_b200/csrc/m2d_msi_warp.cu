@@ -679,6 +679,43 @@ __global__ void __launch_bounds__(256) k_skew_a(MsiLaunch L)
     }
 }
 
+// An application of stored factors (MsiLaunch::apply_only): the residual
+// plane of the first forward sweep gets r = -b (the residual of x = 0) in
+// wavefront-major order, and afterwards x += z from the sweep-result plane,
+// each as one whole-GPU pass.  Grid: (cell blocks, systems).
+template <int ND, typename TS>
+__global__ void k_skew_rhs(MsiLaunch L)
+{
+    const MsiSys S = L.s[blockIdx.y];
+    const int nx = L.nx, ny = L.ny;
+    const int NL = (ND == 9) ? 5 : 4, NU = (ND == 9) ? 4 : 3;
+    const int SW = nx + kSkewPad;
+    const long long PS = (long long)((ny + 31) / 32) * SW * kLine;
+    TS *r = reinterpret_cast<TS *>(S.ws) + (long long)(NL + NU + 1) * PS;
+    const long long N = (long long)nx * ny;
+    for (long long np = blockIdx.x * (long long)blockDim.x + threadIdx.x; np < N;
+         np += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(np / nx), i = (int)(np - (long long)j * nx);
+        r[skew_slot(i, j, SW)] = (TS)(-S.b[np]);
+    }
+}
+template <int ND, typename TS>
+__global__ void k_unskew_add(MsiLaunch L)
+{
+    const MsiSys S = L.s[blockIdx.y];
+    const int nx = L.nx, ny = L.ny;
+    const int NL = (ND == 9) ? 5 : 4, NU = (ND == 9) ? 4 : 3;
+    const int SW = nx + kSkewPad;
+    const long long PS = (long long)((ny + 31) / 32) * SW * kLine;
+    const TS *z = reinterpret_cast<const TS *>(S.ws) + (long long)(NL + NU + 2) * PS;
+    const long long N = (long long)nx * ny;
+    for (long long np = blockIdx.x * (long long)blockDim.x + threadIdx.x; np < N;
+         np += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(np / nx), i = (int)(np - (long long)j * nx);
+        S.x[np] = (double)z[skew_slot(i, j, SW)] + S.x[np];
+    }
+}
+
 // TS = double: the reference's FP64 algorithm, bitwise.  TS = float: the
 // factors and both sweeps in FP32 inside the FP64 iteration (residual, x,
 // norm and stopping test stay FP64): iterative refinement preconditioned by
@@ -901,8 +938,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
     const int hw = (wl >> 2) * (4 - WPC) + ((wl & 3) - WPC);
     if (front) {
         if (!L.reuse_lu) run_lu(std::false_type{});
-    } else if (helper) {
-        // meanwhile the helper warps compute the initial residual
+    } else if (helper && !L.apply_only) {
+        // meanwhile the helper warps compute the initial residual (an
+        // application of the factors alone gets r = -b from k_skew_rhs)
         helper_residual<ND, TS>(cl, a, S.b, x, rp, nx, ny, SW, red, part, nhelp, hw);
     }
     if (!L.reuse_lu) up_base += nbatch - 1;
@@ -912,7 +950,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
     // ---- fb2d9 / fb2d5 (msi2d9-v03.f90:42-262, msi2d5-v03.f90:42-233)
     // (the barrier in cluster_total also makes every row's factors and the
     // residual final before the first forward sweep)
-    const double rr0 = cluster_total(cl, part);
+    const double rr0 = L.apply_only ? 0.0 : cluster_total(cl, part);
     stamp(L, rank, 2);
     const double gammarp = L.tol * sqrt(rr0);
     const int cap = (L.nitm > 0) ? L.nitm : kMaxIterUnbounded;
@@ -1138,6 +1176,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                 continue;
             }
         }
+        if (L.apply_only) break;   // x += z by k_unskew_add after the launch
         rr = cluster_residual<ND, TS>(cl, a, S.b, x, wp, rp, nx, ny, SW, red, part);
         if (nit == 1) stamp(L, rank, 5);
         if (sqrt(rr) < gammarp) break;
@@ -1154,7 +1193,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
         while (st.consumed < st.issued) (void)stage_wait(st, again);
     }
     if ((timed_out || hook_ran_out) && L.err) atomicOr(L.err, ERR_SPIN_TIMEOUT);
-    if (rank == 0 && threadIdx.x == 0) {
+    if (rank == 0 && threadIdx.x == 0 && !L.apply_only) {
         if (S.nit) *S.nit = nit;
         if (S.rr) { S.rr[0] = rr0; S.rr[1] = rr; }
     }
@@ -1214,14 +1253,25 @@ static cudaError_t launch_cluster(const MsiLaunch &L, int nsys, cudaStream_t st,
     *fits = true;
     // A into wavefront-major order first (all systems, whole GPU), unless the
     // factors (made from that copy) are reused
+    const bool apply = L.apply_only && L.reuse_lu && L.dev == nullptr && nsys <= 2;
+    const long long N = (long long)L.nx * L.ny;
+    const dim3 cg((unsigned)((N + 255) / 256 < 1184 ? (N + 255) / 256 : 1184), (unsigned)nsys);
     if (!L.reuse_lu) {
         const dim3 sg((unsigned)((L.nx + kSkewPad + kSkewTile - 1) / kSkewTile), (unsigned)nwarps,
                       (unsigned)(nsys * ND));
         k_skew_a<ND, TS><<<sg, 256, 0, st>>>(L);
-        e = cudaGetLastError();
-        if (e != cudaSuccess) return e;
+    } else if (apply) {
+        k_skew_rhs<ND, TS><<<cg, 256, 0, st>>>(L);
     }
-    return cudaLaunchKernelEx(&cfg, kern, L);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    MsiLaunch La = L;
+    La.apply_only = apply ? 1 : 0;
+    if (apply) La.nitm = 1;
+    e = cudaLaunchKernelEx(&cfg, kern, La);
+    if (e != cudaSuccess || !apply) return e;
+    k_unskew_add<ND, TS><<<cg, 256, 0, st>>>(La);
+    return cudaGetLastError();
 }
 
 template <int ND, typename TS>

@@ -48,6 +48,10 @@ struct MsiLaunch {
                                // workspace untouched since): the cluster kernel skips the transpose
                                // of A and the factorisation.  The one-CTA kernel always factorises;
                                // the results are the same either way.
+    int apply_only;            // with reuse_lu = 1 and nitm = 1 (cluster kernel): x += (LU)^-1 b,
+                               // the preconditioner application of a Krylov method -- the right
+                               // side enters the sweeps directly (r = -b, as for x = 0) and no
+                               // residual or norm is computed; S.nit and S.rr are not written
     int variant;               // wavefront schedule: 0 automatic (one wavefront warp per SM when the
                                // cluster fits, else two), 1 one warp per SM (4 staging stages),
                                // 2 two warps per SM (2 stages), 3 the one-CTA kernel (FP64 only);

@@ -1075,9 +1075,13 @@ __global__ void k_backup(Fields f)
     long long N = (long long)f.nx * f.ny;
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < N;
          k += (long long)gridDim.x * blockDim.x) {
-        f.roa[k] = f.ro[k]; f.Ta[k] = f.T[k]; f.pa[k] = f.p[k];
-        f.ua[k] = f.u[k]; f.va[k] = f.v[k];
-        f.uea[k] = f.ue[k]; f.vea[k] = f.ve[k]; f.una[k] = f.un[k]; f.vna[k] = f.vn[k];
+        // all nine loads before any store: the planes are distinct, and loads
+        // in flight together keep the copy bandwidth-bound
+        const double ro = __ldg(f.ro + k), T = __ldg(f.T + k), p = __ldg(f.p + k), u = __ldg(f.u + k);
+        const double v = __ldg(f.v + k), ue = __ldg(f.ue + k), ve = __ldg(f.ve + k), un = __ldg(f.un + k);
+        const double vn = __ldg(f.vn + k);
+        f.roa[k] = ro; f.Ta[k] = T; f.pa[k] = p; f.ua[k] = u; f.va[k] = v;
+        f.uea[k] = ue; f.vea[k] = ve; f.una[k] = un; f.vna[k] = vn;
     }
 }
 

@@ -233,6 +233,30 @@ def harvest(sim, pairs, iters_between=1, count=None, tight_nitm=400, tight_tol=1
     return pairs
 
 
+def harvest_systems(systems, nx, ny, Jp, pairs, tight_nitm=2000, tight_tol=1e-10):
+    """Training pairs from given 5-diagonal systems [(a, b)] (device
+    tensors): the features of each system's initial residual r = b (zero
+    guess) and, as the target, its MSI solution to tight_tol."""
+    import torch
+    dev = pairs.feat.device
+    L = _bind()
+    work = torch.empty(L.m2d_msi_workspace_doubles(5, nx, ny), dtype=torch.float64, device=dev)
+    nit = torch.zeros(2, dtype=torch.int32, device=dev)
+    delta = torch.zeros(nx * ny, dtype=torch.float64, device=dev)
+    stats = torch.zeros(16, dtype=torch.float64, device=dev)
+    for a, b in systems:
+        if pairs.n >= pairs.capacity:
+            break
+        delta.zero_()
+        msi5(nx, ny, tight_nitm, tight_tol, a, b, delta, work, nit)
+        k = pairs.n
+        features(nx, ny, pairs.H, pairs.W, a, b, Jp, pairs.feat[k], stats)
+        target(nx, ny, pairs.H, pairs.W, delta, stats, pairs.t[k], pairs.mask[k])
+        pairs.n += 1
+    torch.cuda.synchronize(dev)
+    return pairs
+
+
 def train(net, pairs, steps, batch=None, lr=1e-3, seed=0, lr_final=None, log=None):
     """Adam on random minibatches of the pairs; returns the loss history."""
     import torch

@@ -92,3 +92,23 @@ def tdma_lines_system(n, nlines, seed=0, dominance=1.05):
     ap[ap == 0] = 1.0
     d = rng.standard_normal((nlines, n))
     return aw, ap, ae, d
+
+
+def isolated5(nx, ny, seed=0, dominance=1.05):
+    """Vectorised 5-diagonal isolated system (plane-major S, W, P, E, N):
+    off-diagonals U[-1, 0] on couplings between real cells, aP = 1.05
+    sum|a_nb|, rhs N(0, 1) on real cells, zero-Dirichlet ghost ring."""
+    rng = np.random.default_rng(seed)
+    inner = np.zeros((ny, nx), bool)
+    inner[1:-1, 1:-1] = True
+    a = np.zeros((5, ny, nx))
+    for k, (di, dj) in enumerate(OFF5):
+        if k == 2:
+            continue
+        nb = np.zeros((ny, nx), bool)
+        nb[max(0, -dj):ny - max(0, dj), max(0, -di):nx - max(0, di)] = \
+            inner[max(0, dj):ny - max(0, -dj), max(0, di):nx - max(0, -di)]
+        a[k] = np.where(inner & nb, -rng.uniform(0.0, 1.0, (ny, nx)), 0.0)
+    a[2] = np.where(inner, dominance * np.abs(a).sum(axis=0), 1.0)
+    b = np.where(inner, rng.standard_normal((ny, nx)), 0.0)
+    return a.reshape(-1).copy(), b.reshape(-1).copy()
