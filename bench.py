@@ -702,7 +702,7 @@ def run_ttr512(local, net, cap_s, tol=1e-8):
            "cap_s": cap_s, "oracle_first_below_it": ref["it"] if ref else None}
     for key, solver in (("plain_fp64", 0), ("fp32_sweeps", 2), ("learned_fp32", 3)):
         g = Simplec(euler_cosine_case(512, 256, solver=solver, tolt=tol), device=local)
-        if solver == 3:
+        if solver >= 3:
             g.set_unet(net)
         else:
             g.set_graph(True)
@@ -718,9 +718,10 @@ def run_ttr512(local, net, cap_s, tol=1e-8):
         fmi, fme, Fd, Cd, pw = g.integrals()
         e = {"seconds": secs, "iterations": r.it, "reached": reached, "normpl": r.normpl, "Cd": Cd,
              "ms_per_iteration": 1e3 * secs / r.it}
-        if solver == 3:
+        if solver >= 3:
             e["learned_calls"] = g.scalar("learned_calls")
             e["learned_accepted"] = g.scalar("learned_accepted")
+            e["learned_alone"] = g.scalar("learned_alone")
         if ref and reached:
             pr = np.asarray(ref["pwall"])
             e["rel_err_vs_oracle"] = {"Cd": abs(Cd - ref["Cd"]) / abs(ref["Cd"]),

@@ -397,7 +397,9 @@ typedef struct m2d_case {
     double tolm, tolt;
     int solver;                             /* 0 MSI, 1 TDMA, 2 MSI with FP32 factors and sweeps,
                                                3 as 2 with the learned p' correction first
-                                               (m2d_ctx_set_unet) */
+                                               (m2d_ctx_set_unet), 4 as 3 with a kept correction
+                                               that already meets MSI's stopping test standing
+                                               alone (no MSI iteration for that p' solve) */
     int nitm_u, nitm_p;
     double tol_u, tol_p;
     int dtmodel;                            /* 0 RAMP, 1 SCARBOROUGH */
@@ -445,7 +447,8 @@ int m2d_get_fields(m2d_ctx *ctx, int count, const char *const *names, double *co
 /* named scalars: dt, norm, normpl, rmass, p_avg, Href, Cpref, fm1D, Fd1D,
  * Fpv1D, Sg, it, it_stop; and of the last iteration itp_used and the MSI
  * iterations nit_u, nit_v, nit_p (last p' cycle), nit_T; launches (kernels
- * started so far), learned_calls, learned_accepted, solver, msi_schedule */
+ * started so far), learned_calls, learned_accepted, learned_alone (p' solves
+ * the correction alone settled, solver 4), solver, msi_schedule */
 int m2d_get_scalar(const m2d_ctx *ctx, const char *name, double *out);
 /* post-processing integrals (src/user/internal_flow/mod_intflow.f90:1591-1643,
  * mod_intflow_postp.f90:1211 Cd = fme/fm1D, :430-445,1454-1465 wall pressure
@@ -573,9 +576,12 @@ int m2d_pprime_target(int nx, int ny, int H, int W, const double *d_delta, const
                       float *d_t, float *d_mask, void *stream);
 /* Flexible pressure-correction solve of the 5-diagonal p' system: the
  * network's correction is kept only when it lowers |b - A x|; the MSI
- * iteration (prec 0 FP64, 1 FP32 sweeps) then runs with its stopping test
- * relative to the residual before the correction; like plain MSI it runs at
- * least one iteration.  d_work: m2d_msi_workspace_doubles(5, nx, ny). */
+ * iteration (prec bit 0: 0 FP64, 1 FP32 sweeps) then runs with its stopping
+ * test relative to the residual before the correction; like plain MSI it
+ * runs at least one iteration, unless prec bit 1 is set and the corrected
+ * residual (FP64, every cell) already meets |r| < tol |r0|: then the
+ * correction is the solution and rep->nit = 0.
+ * d_work: m2d_msi_workspace_doubles(5, nx, ny). */
 typedef struct m2d_learned_report {
     int accepted;          /* 1: the network's correction was kept */
     double r0, r1;         /* |r| before and after the correction */

@@ -47,7 +47,7 @@ struct m2d_ctx {
     int *dint = nullptr;
     m2d_mixture *dmix = nullptr;   // device copy of c.mix (ktm = 1)
     m2d_unet *net = nullptr;       // learned p' correction (solver 3), not owned
-    long long learned_calls = 0, learned_accepted = 0;
+    long long learned_calls = 0, learned_accepted = 0, learned_alone = 0;
     // captured iteration (m2d_ctx_set_graph): the whole `it` body as one CUDA
     // graph, the p' loop a conditional WHILE node, dt and the loop exit on the
     // device
@@ -328,15 +328,18 @@ static int solve9(m2d_ctx *x, cudaStream_t s, int nsys, double *const *a, double
 static int solve5(m2d_ctx *x, cudaStream_t s)
 {
     const m2d_case &c = x->c;
-    if (c.solver == 3) {
-        // flexible p' solve: the network's correction, then MSI with FP32 sweeps
-        if (!x->net) return ctx_fail(M2D_ERR_ARG, "m2d_iterate: solver 3 needs a network (m2d_ctx_set_unet)");
+    if (c.solver == 3 || c.solver == 4) {
+        // flexible p' solve: the network's correction, then MSI with FP32
+        // sweeps; with solver 4 a kept correction that already meets MSI's
+        // stopping test is the whole solve
+        if (!x->net) return ctx_fail(M2D_ERR_ARG, "m2d_iterate: solvers 3 and 4 need a network (m2d_ctx_set_unet)");
         m2d_learned_report r;
         const int rc = m2d_pprime_solve_learned(x->net, x->nx, x->ny, c.nitm_p, c.tol_p, x->f.ap, x->f.bp, x->f.pl,
-                                                x->f.Jp, x->ws5, 1, s, &r);
+                                                x->f.Jp, x->ws5, c.solver == 4 ? 3 : 1, s, &r);
         if (rc) return rc;
         x->learned_calls++;
         x->learned_accepted += r.accepted;
+        if (r.accepted && r.nit == 0) x->learned_alone++;
         return M2D_OK;
     }
     if (c.solver != 1) {
@@ -683,8 +686,8 @@ extern "C" int m2d_ctx_set_msi_schedule(m2d_ctx *x, int variant)
 extern "C" int m2d_ctx_set_graph(m2d_ctx *x, int on)
 {
     if (!x) return ctx_fail(M2D_ERR_ARG, "m2d_ctx_set_graph: null context");
-    if (on && x->c.solver == 3)
-        return ctx_fail(M2D_ERR_ARG, "m2d_ctx_set_graph: solver 3 decides on the host and is not captured");
+    if (on && x->c.solver >= 3)
+        return ctx_fail(M2D_ERR_ARG, "m2d_ctx_set_graph: solvers 3 and 4 decide on the host and are not captured");
     TRY(cudaSetDevice(x->device));
     if (on && !x->graph_on) {
         // the device copies of dt and of the iteration counter start from the host's
@@ -855,6 +858,7 @@ extern "C" int m2d_get_scalar(const m2d_ctx *x, const char *name, double *out)
         {"launches", (double)x->launches}, {"nit_u", (double)x->hint[I_NIT_U]}, {"nit_v", (double)x->hint[I_NIT_V]},
         {"nit_p", (double)x->hint[I_NIT_P]}, {"nit_T", (double)x->hint[I_NIT_T]},
         {"learned_calls", (double)x->learned_calls}, {"learned_accepted", (double)x->learned_accepted},
+        {"learned_alone", (double)x->learned_alone},
         {"solver", (double)x->c.solver}, {"msi_schedule", (double)x->msi_variant}};
     for (auto &t : tab)
         if (!strcmp(name, t.nm)) { *out = t.v; return M2D_OK; }

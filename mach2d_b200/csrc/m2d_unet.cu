@@ -1444,6 +1444,10 @@ extern "C" int m2d_pprime_solve_learned(m2d_unet *n, int nx, int ny, int nitm, d
 {
     if (!n || !image_fits(nx, ny, n->H, n->W) || !d_a || !d_b || !d_x || !d_Jp || !d_work || nitm < 1)
         return unet_fail(M2D_ERR_ARG, "m2d_pprime_solve_learned: bad arguments");
+    // prec bit 0: FP32 factors and sweeps; bit 1: a kept correction that
+    // already meets the MSI stopping test |r| < tol |r0| stands alone
+    const bool alone = (prec & 2) != 0;
+    prec &= 1;
     cudaStream_t st = (cudaStream_t)stream;
     const int H = n->H, W = n->W;
     const long long N = (long long)nx * ny;
@@ -1471,12 +1475,18 @@ extern "C" int m2d_pprime_solve_learned(m2d_unet *n, int nx, int ny, int nitm, d
         tol_eff = r1 > 0.0 ? tol * r0 / r1 : 1.0;
     }
     int nit = 0;
-    if (e == cudaSuccess) {      // at least one MSI iteration, as the judge of the correction
+    // at least one MSI iteration, as the judge of the correction -- unless the
+    // corrected residual, measured in FP64, already passes MSI's own stopping
+    // test and the caller allows the correction to stand alone
+    const bool skip_msi = alone && accept && r1 < tol * r0;
+    if (e == cudaSuccess && !skip_msi) {
         const int rc = m2d_msi_solve_device_ws(5, nx, ny, nitm, tol_eff, d_a, d_b, d_x, d_work,
                                                m2d_msi_workspace_doubles(5, nx, ny), stream, n->nit, nullptr, prec);
         if (rc) return rc;
         e = cudaMemcpyAsync(&nit, n->nit, sizeof(int), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    } else if (e == cudaSuccess) {
+        e = cudaStreamSynchronize(st);   // the copy of the kept correction
     }
     if (e != cudaSuccess) { m2d_set_last_error(e, "m2d_pprime_solve_learned", __FILE__, __LINE__); return M2D_ERR_CUDA; }
     if (rep) { rep->accepted = accept ? 1 : 0; rep->r0 = r0; rep->r1 = r1; rep->nit = nit; }
