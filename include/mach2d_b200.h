@@ -89,6 +89,17 @@ int m2d_msi_solve_device_timed(int nd, int nx, int ny, int nitm, double tol,
                                const double *d_a, const double *d_b, double *d_x,
                                double *d_work, void *stream, int *d_nit,
                                unsigned long long *d_times);
+/* The device solve with its options spelled out: prec 0 (FP64, the
+ * reference's arithmetic) or 1 (FP32 factors and sweeps in the FP64
+ * iteration); reuse_factors = 1 when d_work already holds the factors of
+ * this same d_a from an earlier solve with the same prec and sizes, d_work
+ * untouched since (the cluster kernel then skips the transpose of A and the
+ * factorisation; the one-CTA kernel factorises anyway; the iterates are the
+ * same); d_times (may be null) as for m2d_msi_solve_device_timed, the
+ * factorisation phase empty when reused. */
+int m2d_msi_solve_device_ex(int nd, int nx, int ny, int nitm, double tol, const double *d_a, const double *d_b,
+                            double *d_x, double *d_work, void *stream, int *d_nit, int prec, int reuse_factors,
+                            unsigned long long *d_times);
 /* Diagnostics: the FP64 solves factorise with reciprocal-based (Markstein)
  * quotients and check every factor against IEEE division while the first
  * sweeps run; when one differs (operands near the subnormal or overflow
@@ -475,6 +486,15 @@ typedef struct m2d_case {
                                                arithmetic face means of mu_t and cp mu_t at the
                                                east and north faces, the wall faces laminar */
     double prt;                             /* turbulent Prandtl number (modtur = 1) */
+    int msi_lag;                            /* solvers 2-4, cluster MSI kernel: 0 factorises every
+                                               solve, as the reference; n > 0 lets a solve reuse
+                                               the FP32 factors its workspace holds for the same
+                                               equation from fewer than n solves ago while one
+                                               iteration still meets the tolerance (the FP64
+                                               residual and stopping test are unchanged; a stale
+                                               solve that needs a second iteration renews the
+                                               factors at the next one).  Not the reference's
+                                               algorithm: only the preconditioner ages. */
 } m2d_case;
 
 typedef struct m2d_report {

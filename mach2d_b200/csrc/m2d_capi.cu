@@ -249,6 +249,32 @@ int m2d_msi_solve_device_mixed(int nd, int nx, int ny, int nitm, double tol, con
                                    m2d_msi_workspace_doubles(nd, nx, ny), stream, d_nit, nullptr, 1);
 }
 
+int m2d_msi_solve_device_ex(int nd, int nx, int ny, int nitm, double tol, const double *d_a, const double *d_b,
+                            double *d_x, double *d_work, void *stream, int *d_nit, int prec, int reuse_factors,
+                            unsigned long long *d_times)
+{
+    if ((nd != 9 && nd != 5) || nx < 4 || ny < 4 || !d_a || !d_b || !d_x || !d_work || (prec != 0 && prec != 1) ||
+        (reuse_factors != 0 && reuse_factors != 1))
+        return fail(ST_ARG, "msi_solve_device_ex: bad arguments");
+    if (ny > msi_max_ny()) return fail(ST_TOO_LARGE, "msi_solve_device_ex: ny exceeds m2d_msi_max_ny()");
+    const long wd = m2d_msi_workspace_doubles(nd, nx, ny);
+    MsiLaunch L;
+    memset(&L, 0, sizeof L);
+    L.nx = nx; L.ny = ny; L.nitm = nitm; L.tol = tol;
+    L.prec = prec;
+    L.reuse_lu = reuse_factors;
+    MsiSys &S = L.s[0];
+    S.a = d_a; S.b = d_b; S.x = d_x;
+    S.ws = d_work;
+    S.rr = d_work + (wd - 4);
+    S.nit = d_nit;
+    L.ws_cap = (size_t)(wd - 4);
+    L.prof = d_times;
+    cudaError_t e = launch_msi(nd, L, 1, (cudaStream_t)stream);
+    if (e != cudaSuccess) { m2d_set_last_error(e, "msi_solve_device_ex launch", __FILE__, __LINE__); return ST_CUDA; }
+    return ST_OK;
+}
+
 int m2d_msi_solve_device_timed(int nd, int nx, int ny, int nitm, double tol, const double *d_a,
                                const double *d_b, double *d_x, double *d_work, void *stream,
                                int *d_nit, unsigned long long *d_times)

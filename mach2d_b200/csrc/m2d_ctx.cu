@@ -45,6 +45,7 @@ struct m2d_ctx {
     double *ws9[2], *ws5, *P, *Q, *part;
     double *dsc = nullptr;
     int *dint = nullptr;
+    int *dlag = nullptr;           // MSI factor records (MsiSys::lag), two ints per workspace
     m2d_mixture *dmix = nullptr;   // device copy of c.mix (ktm = 1)
     m2d_unet *net = nullptr;       // learned p' correction (solver 3), not owned
     long long learned_calls = 0, learned_accepted = 0, learned_alone = 0;
@@ -206,6 +207,7 @@ extern "C" int m2d_create(const m2d_case *c, int device, m2d_ctx **out)
     if (c->ktm != 0 && c->ktm != 1) return ctx_fail(M2D_ERR_ARG, "m2d_create: ktm must be 0 (CONSTANT) or 1 (MIXTURE)");
     if (c->modtur != 0 && !(c->modtur == 1 && c->modvis == 1 && c->prt > 0.0 && c->nyr >= 3))
         return ctx_fail(M2D_ERR_ARG, "m2d_create: modtur = 1 needs modvis = 1 and prt > 0");
+    if (c->msi_lag < 0) return ctx_fail(M2D_ERR_ARG, "m2d_create: msi_lag must be >= 0");
     if (c->ktm == 1 && (c->mix.ngs < 1 || c->mix.ngs > M2D_MAX_SPECIES || !(c->mix.Rg > 0.0)))
         return ctx_fail(M2D_ERR_ARG, "m2d_create: ktm = 1 needs a mixture from m2d_mixture_init");
     HostInstance h;
@@ -228,7 +230,7 @@ extern "C" int m2d_create(const m2d_case *c, int device, m2d_ctx **out)
     const size_t strips = (size_t)9 * h.ny + 2 * (size_t)h.nx + 64;
     const size_t solver = 2 * msi_work_doubles(9, h.nx, h.ny) + msi_work_doubles(5, h.nx, h.ny) + 4 + 2 * N + 3 * 32;
     const size_t mixd = (sizeof(m2d_mixture) + sizeof(double) - 1) / sizeof(double);
-    const size_t total = nplanes * N + 32 * N + strips + solver + (size_t)red_parts() + 64 + S_COUNT + mixd;
+    const size_t total = nplanes * N + 32 * N + strips + solver + (size_t)red_parts() + 72 + S_COUNT + mixd;
     e = cudaMalloc(&x->arena, total * sizeof(double));
     if (e != cudaSuccess) { cudaStreamDestroy(x->st); delete x; m2d_set_last_error(e, "cudaMalloc", __FILE__, __LINE__); return M2D_ERR_NOMEM; }
     cudaMemsetAsync(x->arena, 0, total * sizeof(double), x->st);
@@ -252,6 +254,7 @@ extern "C" int m2d_create(const m2d_case *c, int device, m2d_ctx **out)
     x->part = take((size_t)red_parts() + 8);
     x->dsc = take(S_COUNT);
     x->dint = (int *)take(I_COUNT);
+    x->dlag = (int *)take(4);   // factor records of ws9[0], ws9[1], ws5 (zeroed: no factors yet)
     x->dmix = (m2d_mixture *)take(mixd);
     if ((size_t)(cur - x->arena) > total) { m2d_destroy(x); return ctx_fail(M2D_ERR_NOMEM, "m2d_create: arena overflow"); }
     e = cudaMallocHost(&x->hsc, S_COUNT * sizeof(double));
@@ -312,10 +315,13 @@ static int solve9(m2d_ctx *x, cudaStream_t s, int nsys, double *const *a, double
         L.prec = (c.solver >= 2) ? 1 : 0;
         L.variant = x->msi_variant;
         L.err = x->dint + I_ERR;
+        L.lag_max = L.prec == 1 ? c.msi_lag : 0;
         for (int k = 0; k < nsys; k++) {
             L.s[k].a = a[k]; L.s[k].b = b[k]; L.s[k].x = v[k];
             L.s[k].ws = x->ws9[k];
             L.s[k].nit = x->dint + islot[k]; L.s[k].rr = x->dsc + rslot[k];
+            L.s[k].lag = x->dlag + 2 * k;
+            L.s[k].tag = 1 + islot[k];   // the equation (u, v or T) owns the factors
         }
         KL(launch_msi(9, L, nsys, s), 2);   // A transpose + solve
     } else {
@@ -352,6 +358,9 @@ static int solve5(m2d_ctx *x, cudaStream_t s)
         L.s[0].a = x->f.ap; L.s[0].b = x->f.bp; L.s[0].x = x->f.pl;
         L.s[0].ws = x->ws5;
         L.s[0].nit = x->dint + I_NIT_P; L.s[0].rr = x->dsc + S_RR + 4;
+        L.lag_max = L.prec == 1 ? c.msi_lag : 0;
+        L.s[0].lag = x->dlag + 4;
+        L.s[0].tag = 1 + I_NIT_P;
         KL(launch_msi(5, L, 1, s), 2);   // A transpose + solve
     } else {
         KL(launch_tdma(5, x->nx, x->ny, c.nitm_p, x->f.ap, x->f.bp, x->f.pl, x->P, x->Q, s), 4 * c.nitm_p);

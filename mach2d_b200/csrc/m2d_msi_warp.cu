@@ -356,8 +356,8 @@ __device__ __forceinline__ long long skew_slot(int i, int j, int sw)
 // r = A x - b for one cell, in-range neighbours in ascending diagonal order
 template <int ND>
 __device__ __forceinline__ double residual_cell(const double *__restrict__ a, const double *__restrict__ b,
-                                                const double *x, long long np, int i, int j, int nx, int ny,
-                                                long long N)
+                                                const double *__restrict__ x, long long np, int i, int j, int nx,
+                                                int ny, long long N)
 {
     const bool w = i > 0, e = i < nx - 1, s = j > 0, n = j < ny - 1;
     double v = -b[np];
@@ -395,8 +395,8 @@ __device__ __forceinline__ void named_bar(unsigned id, unsigned count)
 // the CTAs after the next cluster barrier.
 template <int ND, typename TS>
 __device__ void helper_residual(cg::cluster_group &cl, const double *__restrict__ a, const double *__restrict__ b,
-                                const double *x, TS *r, int nx, int ny, int sw, double *red, double *part,
-                                int nhelp, int hw)
+                                const double *__restrict__ x, TS *__restrict__ r, int nx, int ny, int sw,
+                                double *red, double *part, int nhelp, int hw)
 {
     const long long N = (long long)nx * ny;
     const int C = (int)cl.num_blocks(), rank = (int)cl.block_rank();
@@ -426,6 +426,42 @@ __device__ void helper_residual(cg::cluster_group &cl, const double *__restrict_
         double *p0 = cl.map_shared_rank(part, 0);
         p0[rank] = red[0];
     }
+}
+
+// r = A x - b over cells lo + threadIdx.x + kThreads k of [lo, hi), stored
+// wavefront-major; returns this thread's sum of r^2 in cell order.  Four
+// cells per round with their loads issued together.
+template <int ND, typename TS>
+__device__ __forceinline__ double residual_pass(const double *__restrict__ a, const double *__restrict__ b,
+                                                const double *__restrict__ x, TS *__restrict__ r, long long lo,
+                                                long long hi, int nx, int ny, int sw)
+{
+    const long long N = (long long)nx * ny;
+    double acc = 0.0;
+    long long np = lo + threadIdx.x;
+    for (; np + 3 * kThreads < hi; np += 4 * kThreads) {
+        double v[4];
+        int ii[4], jj[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const long long c = np + q * kThreads;
+            jj[q] = (int)((unsigned)c / (unsigned)nx);   // N < 2^31
+            ii[q] = (int)c - jj[q] * nx;
+            v[q] = residual_cell<ND>(a, b, x, c, ii[q], jj[q], nx, ny, N);
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            r[skew_slot(ii[q], jj[q], sw)] = (TS)v[q];
+            acc = acc + v[q] * v[q];
+        }
+    }
+    for (; np < hi; np += kThreads) {
+        const int j = (int)((unsigned)np / (unsigned)nx), i = (int)np - j * nx;
+        const double v = residual_cell<ND>(a, b, x, np, i, j, nx, ny, N);
+        r[skew_slot(i, j, sw)] = (TS)v;
+        acc = acc + v * v;
+    }
+    return acc;
 }
 
 // After a cluster barrier: the sum of the CTAs' part[] in rank order,
@@ -458,21 +494,17 @@ __device__ double cluster_residual(cg::cluster_group &cl, const double *__restri
     const long long per = (N + C - 1) / C;
     const long long lo = per * rank, hi = (lo + per < N) ? lo + per : N;
     if (z) {
+        double *__restrict__ xw = x;
+        const TS *__restrict__ zr = z;
 #pragma unroll 8
         for (long long np = lo + threadIdx.x; np < hi; np += kThreads) {
             const int j = (int)((unsigned)np / (unsigned)nx), i = (int)np - j * nx;   // N < 2^31
-            x[np] = (double)z[skew_slot(i, j, sw)] + x[np];
+            xw[np] = (double)zr[skew_slot(i, j, sw)] + xw[np];
         }
         cl.sync();
     }
-    double acc = 0.0;
-#pragma unroll 8
-    for (long long np = lo + threadIdx.x; np < hi; np += kThreads) {
-        const int j = (int)((unsigned)np / (unsigned)nx), i = (int)np - j * nx;   // N < 2^31
-        const double v = residual_cell<ND>(a, b, x, np, i, j, nx, ny, N);
-        r[skew_slot(i, j, sw)] = (TS)v;
-        acc = acc + v * v;
-    }
+    // x is final (read-only) from here on, and r is separate workspace
+    const double acc = residual_pass<ND, TS>(a, b, x, r, lo, hi, nx, ny, sw);
     fence_async_global();   // the forward sweep reads r with bulk copies
     red[threadIdx.x] = acc;
     __syncthreads();
@@ -653,12 +685,23 @@ __device__ void verify_factors(const double *asp, const double *dl, const double
 // (kSkewTile + 62) cells through shared memory into kSkewTile lines; cells
 // outside the grid become zeros.  Grid: (line tiles, row groups, systems x ND).
 constexpr int kSkewTile = 64;
+// lagged factorisation (MsiLaunch::lag_max): does this solve reuse the
+// factors in its workspace?  Read by the transpose and by every thread of
+// the solve before anything writes the record, so all agree.
+template <typename TS>
+__device__ __forceinline__ bool lag_reuse(const MsiLaunch &L, const MsiSys &S)
+{
+    if (std::is_same<TS, double>::value || L.lag_max <= 0 || !S.lag || L.reuse_lu || L.apply_only) return false;
+    return S.lag[0] == S.tag && S.lag[1] >= 1 && S.lag[1] < L.lag_max;
+}
+
 template <int ND, typename TS>
 __global__ void __launch_bounds__(256) k_skew_a(MsiLaunch L)
 {
     __shared__ double tile[32][kSkewTile + kSkewPad + 1];
     const int sys = blockIdx.z / ND, k = blockIdx.z - sys * ND;
     const MsiSys S = L.s[sys];
+    if (lag_reuse<TS>(L, S)) return;   // the factors are reused: A is not needed
     const int nx = L.nx, ny = L.ny;
     const long long N = (long long)nx * ny;
     const int NL = (ND == 9) ? 5 : 4, NU = (ND == 9) ? 4 : 3;
@@ -818,6 +861,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
         dn_full_dst = cluster_addr(&full_dn[pw][0], pr);
         up_empty_dst = cluster_addr(&empty_up[pw][0], pr);
     }
+    // lagged factorisation: reuse the workspace's factors (decided from the
+    // record as the launch found it; rank 0 rewrites it at the end)
+    const bool lagged = lag_reuse<TS>(L, S);
+    const int lag_age = lagged ? S.lag[1] : 0;
+    const bool reuse = L.reuse_lu || lagged;
     cl.sync();   // mbarriers initialised before any use; A staged by k_skew_a
     bool bad_pivot = false, timed_out = false, hook_ran_out = false;
     int up_base = 0, dn_base = 0;       // batches sent so far on each channel
@@ -936,21 +984,26 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
     const bool helper = (wl & 3) >= WPC;
     const int nhelp = (kThreads / 32 / 4) * (4 - WPC);
     const int hw = (wl >> 2) * (4 - WPC) + ((wl & 3) - WPC);
-    if (front) {
-        if (!L.reuse_lu) run_lu(std::false_type{});
-    } else if (helper && !L.apply_only) {
-        // meanwhile the helper warps compute the initial residual (an
-        // application of the factors alone gets r = -b from k_skew_rhs)
-        helper_residual<ND, TS>(cl, a, S.b, x, rp, nx, ny, SW, red, part, nhelp, hw);
+    // the initial residual: with a factorisation to run, the helper warps
+    // compute it meanwhile; with reused factors every warp takes part (the
+    // same per-thread sums and tree, so the same norm).  An application of
+    // the factors alone gets r = -b from k_skew_rhs.
+    double rr0 = 0.0;
+    if (!reuse) {
+        if (front) run_lu(std::false_type{});
+        else if (helper && !L.apply_only) helper_residual<ND, TS>(cl, a, S.b, x, rp, nx, ny, SW, red, part, nhelp, hw);
+        up_base += nbatch - 1;
     }
-    if (!L.reuse_lu) up_base += nbatch - 1;
     if (bad_pivot && L.err) atomicOr(L.err, ERR_NONFINITE_PIVOT);
     stamp(L, rank, 1);
 
     // ---- fb2d9 / fb2d5 (msi2d9-v03.f90:42-262, msi2d5-v03.f90:42-233)
-    // (the barrier in cluster_total also makes every row's factors and the
-    // residual final before the first forward sweep)
-    const double rr0 = L.apply_only ? 0.0 : cluster_total(cl, part);
+    // (the cluster barrier of the first residual pass or of cluster_total
+    // also makes every row's factors and the residual final before the
+    // first forward sweep)
+    if (L.apply_only) rr0 = 0.0;
+    else if (reuse) rr0 = cluster_residual<ND, TS>(cl, a, S.b, x, (const TS *)nullptr, rp, nx, ny, SW, red, part);
+    else rr0 = cluster_total(cl, part);
     stamp(L, rank, 2);
     const double gammarp = L.tol * sqrt(rr0);
     const int cap = (L.nitm > 0) ? L.nitm : kMaxIterUnbounded;
@@ -1196,6 +1249,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
     if (rank == 0 && threadIdx.x == 0 && !L.apply_only) {
         if (S.nit) *S.nit = nit;
         if (S.rr) { S.rr[0] = rr0; S.rr[1] = rr; }
+        if (!EXACT && L.lag_max > 0 && S.lag && !L.reuse_lu) {
+            // the record for the next solve: fresh factors are one solve old;
+            // reused ones age, and are renewed next time once they needed a
+            // second iteration (or anything went wrong)
+            const bool renew = timed_out || hook_ran_out || bad_pivot || (lagged && nit > 1);
+            S.lag[0] = S.tag;
+            S.lag[1] = renew ? L.lag_max : (lagged ? lag_age + 1 : 1);
+        }
     }
     cl.sync();   // no CTA leaves while another may still write into its shared memory
     stamp(L, rank, 6);

@@ -16,6 +16,10 @@ struct MsiSys {
     double *ws;
     int *nit;          // iterations performed (device int)
     double *rr;        // [0] = |r0|^2, [1] = |r_final|^2 (device doubles)
+    int *lag;          // MsiLaunch::lag_max > 0: the workspace's factor record (device ints):
+                       // [0] tag of the system whose factors ws holds, [1] solves since they were
+                       // made; may be null (factorise every solve)
+    int tag;           // this system's tag (nonzero)
 };
 
 // scratch doubles one system needs (the larger of the two kernels' layouts),
@@ -52,6 +56,13 @@ struct MsiLaunch {
                                // the preconditioner application of a Krylov method -- the right
                                // side enters the sweeps directly (r = -b, as for x = 0) and no
                                // residual or norm is computed; S.nit and S.rr are not written
+    int lag_max;               // > 0 (FP32 factors, cluster kernel): lagged factorisation.  A system
+                               // whose workspace holds its own factors from fewer than lag_max solves
+                               // ago, and whose last solve took one iteration, reuses them (no
+                               // transpose of A, no factorisation); the iteration, its FP64 residual
+                               // and stopping test are unchanged, so only the preconditioner is
+                               // older.  A stale solve that needs a second iteration marks the
+                               // factors for renewal at the next solve.  0: factorise every solve.
     int variant;               // wavefront schedule: 0 automatic (one wavefront warp per SM when the
                                // cluster fits, else two), 1 one warp per SM (4 staging stages),
                                // 2 two warps per SM (2 stages), 3 the one-CTA kernel (FP64 only);

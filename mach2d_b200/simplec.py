@@ -29,6 +29,7 @@ class Case(ctypes.Structure):
         ("it2", ctypes.c_int), ("h0", ctypes.c_double), ("mincc", ctypes.c_double),
         ("maxcc", ctypes.c_double), ("nan_policy", ctypes.c_int), ("ktm", ctypes.c_int),
         ("mix", Mixture), ("modtur", ctypes.c_int), ("prt", ctypes.c_double),
+        ("msi_lag", ctypes.c_int),
     ]
 
     @classmethod

@@ -250,6 +250,7 @@ typedef struct orc_case {
     orc_mixture mix;       /* ktm = 1 */
     int modtur;            /* 1: Baldwin-Lomax eddy viscosity in the transport coefficients (modvis = 1) */
     double prt;            /* turbulent Prandtl number (modtur = 1) */
+    int msi_lag;           /* device solver option (factor reuse); the oracle factorises every solve */
 } orc_case;
 
 typedef struct orc_report {
