@@ -323,7 +323,7 @@ static int solve9(m2d_ctx *x, cudaStream_t s, int nsys, double *const *a, double
             L.s[k].lag = x->dlag + 2 * k;
             L.s[k].tag = 1 + islot[k];   // the equation (u, v or T) owns the factors
         }
-        KL(launch_msi(9, L, nsys, s), 2);   // A transpose + solve
+        KL(launch_msi(9, L, nsys, s), msi_last_launch_count());
     } else {
         for (int k = 0; k < nsys; k++)
             KL(launch_tdma(9, x->nx, x->ny, c.nitm_u, a[k], b[k], v[k], x->P, x->Q, s), 4 * c.nitm_u);
@@ -361,7 +361,7 @@ static int solve5(m2d_ctx *x, cudaStream_t s)
         L.lag_max = L.prec == 1 ? c.msi_lag : 0;
         L.s[0].lag = x->dlag + 4;
         L.s[0].tag = 1 + I_NIT_P;
-        KL(launch_msi(5, L, 1, s), 2);   // A transpose + solve
+        KL(launch_msi(5, L, 1, s), msi_last_launch_count());
     } else {
         KL(launch_tdma(5, x->nx, x->ny, c.nitm_p, x->f.ap, x->f.bp, x->f.pl, x->P, x->Q, s), 4 * c.nitm_p);
     }

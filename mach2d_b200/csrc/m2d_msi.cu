@@ -49,8 +49,9 @@ size_t msi_generic_work_doubles(int nd, int nx, int ny)
 }
 size_t msi_cluster_work_doubles(int nd, int nx, int ny)
 {
-    // dl, du, 1/dl1, residual, correction and A, wavefront-major
-    return (size_t)(nd == 9 ? 21 : 15) * msi_skew_plane(nx, ny);
+    // dl, du, 1/dl1, residual, correction and A, wavefront-major, then the
+    // scratch of the whole-GPU residual passes
+    return (size_t)(nd == 9 ? 21 : 15) * msi_skew_plane(nx, ny) + kMsiExtScratch;
 }
 size_t msi_work_doubles(int nd, int nx, int ny)
 {
@@ -279,6 +280,10 @@ __global__ void __launch_bounds__(kMaxThreads) k_msi(MsiLaunch L)
     }
 }
 
+static thread_local int g_msi_launches = 0;
+void msi_note_launches(int n) { g_msi_launches = n; }
+int msi_last_launch_count() { return g_msi_launches; }
+
 cudaError_t launch_msi(int nd, const MsiLaunch &L, int nsys, cudaStream_t st)
 {
     if (L.ny > msi_max_ny() || L.nx < 3 || L.ny < 3) return cudaErrorInvalidValue;
@@ -301,6 +306,7 @@ cudaError_t launch_msi_generic(int nd, const MsiLaunch &L, int nsys, cudaStream_
         if (e != cudaSuccess) return e;
         k_msi<5><<<nsys, T, sm, st>>>(L);
     }
+    msi_note_launches(1);
     return cudaGetLastError();
 }
 

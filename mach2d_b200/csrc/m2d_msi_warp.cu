@@ -695,12 +695,43 @@ __device__ __forceinline__ bool lag_reuse(const MsiLaunch &L, const MsiSys &S)
     return S.lag[0] == S.tag && S.lag[1] >= 1 && S.lag[1] < L.lag_max;
 }
 
+constexpr int kExtBlocks = 296;
+constexpr long long kExtMinCells = 1LL << 16;
+constexpr int kExtTimedOut = 1, kExtLagged = 2, kExtBadPivot = 4;   // status bits of the first launch
+
+struct ExtWords {
+    double *partA, *partB;        // block sums of the initial / new residual
+    unsigned *cntA, *cntB;        // finished blocks of each reduction
+    int *status;                  // kExt* bits from the first launch
+    int *done;                    // the stopping test passed (or the solve must stop)
+};
+__device__ __forceinline__ ExtWords ext_words(const MsiSys &S, int nd, int nx, int ny)
+{
+    const long long PS = (long long)((ny + 31) / 32) * (nx + kSkewPad) * kLine;
+    double *e = S.ws + (long long)(nd == 9 ? 21 : 15) * PS;
+    ExtWords w;
+    w.partA = e;
+    w.partB = e + kExtBlocks;
+    w.cntA = reinterpret_cast<unsigned *>(e + 2 * kExtBlocks);
+    w.cntB = reinterpret_cast<unsigned *>(e + 2 * kExtBlocks + 1);
+    w.status = reinterpret_cast<int *>(e + 2 * kExtBlocks + 2);
+    w.done = reinterpret_cast<int *>(e + 2 * kExtBlocks + 3);
+    return w;
+}
+
 template <int ND, typename TS>
 __global__ void __launch_bounds__(256) k_skew_a(MsiLaunch L)
 {
     __shared__ double tile[32][kSkewTile + kSkewPad + 1];
     const int sys = blockIdx.z / ND, k = blockIdx.z - sys * ND;
     const MsiSys S = L.s[sys];
+    if (L.ext && k == 0 && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
+        // the whole-GPU passes start from a clean state
+        const ExtWords w = ext_words(S, ND, L.nx, L.ny);
+        *w.cntA = 0u;
+        *w.status = 0;
+        *w.done = 0;
+    }
     if (lag_reuse<TS>(L, S)) return;   // the factors are reused: A is not needed
     const int nx = L.nx, ny = L.ny;
     const long long N = (long long)nx * ny;
@@ -756,6 +787,127 @@ __global__ void k_unskew_add(MsiLaunch L)
          np += (long long)gridDim.x * blockDim.x) {
         const int j = (int)(np / nx), i = (int)(np - (long long)j * nx);
         S.x[np] = (double)z[skew_slot(i, j, SW)] + S.x[np];
+    }
+}
+
+// ---- whole-GPU residual passes (MsiLaunch::ext).  On a large grid the
+// passes over all cells (the initial residual of a solve with reused
+// factors, x += z and the new residual) run on the cluster's 9-16 SMs far
+// below what the whole GPU moves, and take a sixth to a quarter of a
+// one-iteration solve.  With ext the cluster kernel stops after the first
+// sweep pair, these kernels make the passes on every SM, and a
+// continuation launch of the cluster kernel iterates further only if the
+// stopping test asks for it.  Reductions are deterministic: kExtBlocks
+// blocks take fixed contiguous shares, a thread sums its cells in order, a
+// block adds its threads' sums by a fixed tree, and the last block to
+// finish adds the block sums in index order.
+// r = A x - b over block blockIdx.x's share into the wavefront-major plane
+// r, and the deterministic sum of r^2: returns the total in thread 0 of the
+// last block to finish (last = true there), after resetting the counter
+template <int ND, typename TS>
+__device__ double ext_residual(const MsiSys &S, int nx, int ny, TS *__restrict__ r, double *part, unsigned *cnt,
+                               bool &last)
+{
+    __shared__ double red[256];
+    __shared__ bool is_last;
+    const long long N = (long long)nx * ny;
+    const int SW = nx + kSkewPad;
+    const long long per = (N + kExtBlocks - 1) / kExtBlocks;
+    const long long lo = per * blockIdx.x, hi = (lo + per < N) ? lo + per : N;
+    double acc = 0.0;
+    for (long long np = lo + threadIdx.x; np < hi; np += blockDim.x) {
+        const int j = (int)((unsigned)np / (unsigned)nx), i = (int)np - j * nx;   // N < 2^31
+        const double v = residual_cell<ND>(S.a, S.b, S.x, np, i, j, nx, ny, N);
+        r[skew_slot(i, j, SW)] = (TS)v;
+        acc = acc + v * v;
+    }
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+        if (threadIdx.x < s) red[threadIdx.x] = red[threadIdx.x] + red[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        part[blockIdx.x] = red[0];
+        __threadfence();
+        is_last = atomicAdd(cnt, 1u) == (unsigned)gridDim.x - 1u;
+    }
+    __syncthreads();
+    last = is_last && threadIdx.x == 0;
+    double total = 0.0;
+    if (last) {
+        __threadfence();
+        for (int k = 0; k < (int)gridDim.x; k++) total = total + __ldcg(part + k);
+        *cnt = 0u;
+    }
+    return total;
+}
+
+// the initial residual of a solve that reuses its factors (lagged
+// factorisation); nothing when the factors are renewed (the helper warps
+// compute it behind the factorisation then).  Grid (kExtBlocks, systems).
+template <int ND, typename TS>
+__global__ void __launch_bounds__(256) k_ext_r0(MsiLaunch L)
+{
+    const MsiSys S = L.s[blockIdx.y];
+    if (!lag_reuse<TS>(L, S)) return;
+    const int nx = L.nx, ny = L.ny;
+    constexpr int NL = (ND == 9) ? 5 : 4, NU = (ND == 9) ? 4 : 3;
+    const long long PS = (long long)((ny + 31) / 32) * (nx + kSkewPad) * kLine;
+    TS *rp = reinterpret_cast<TS *>(S.ws) + (long long)(NL + NU + 1) * PS;
+    const ExtWords w = ext_words(S, ND, nx, ny);
+    bool last;
+    const double rr0 = ext_residual<ND, TS>(S, nx, ny, rp, w.partA, w.cntA, last);
+    if (last) S.rr[0] = rr0;
+}
+
+// x += z after the first sweep pair; zeroes the counter of the next pass.
+// Grid (blocks, systems).
+template <int ND, typename TS>
+__global__ void k_ext_update(MsiLaunch L)
+{
+    const MsiSys S = L.s[blockIdx.y];
+    const int nx = L.nx, ny = L.ny;
+    constexpr int NL = (ND == 9) ? 5 : 4, NU = (ND == 9) ? 4 : 3;
+    const int SW = nx + kSkewPad;
+    const long long PS = (long long)((ny + 31) / 32) * SW * kLine;
+    const TS *z = reinterpret_cast<const TS *>(S.ws) + (long long)(NL + NU + 2) * PS;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *ext_words(S, ND, nx, ny).cntB = 0u;
+    const long long N = (long long)nx * ny;
+    for (long long np = blockIdx.x * (long long)blockDim.x + threadIdx.x; np < N;
+         np += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(np / nx), i = (int)(np - (long long)j * nx);
+        S.x[np] = (double)z[skew_slot(i, j, SW)] + S.x[np];
+    }
+}
+
+// the new residual, its norm and the stopping test of the first iteration;
+// when the solve ends here the last block also writes the factor record.
+// Grid (kExtBlocks, systems).
+template <int ND, typename TS>
+__global__ void __launch_bounds__(256) k_ext_resid(MsiLaunch L)
+{
+    const MsiSys S = L.s[blockIdx.y];
+    const int nx = L.nx, ny = L.ny;
+    constexpr int NL = (ND == 9) ? 5 : 4, NU = (ND == 9) ? 4 : 3;
+    const long long PS = (long long)((ny + 31) / 32) * (nx + kSkewPad) * kLine;
+    TS *rp = reinterpret_cast<TS *>(S.ws) + (long long)(NL + NU + 1) * PS;
+    const ExtWords w = ext_words(S, ND, nx, ny);
+    bool last;
+    const double rr = ext_residual<ND, TS>(S, nx, ny, rp, w.partB, w.cntB, last);
+    if (!last) return;
+    const double rr0 = S.rr[0];
+    S.rr[1] = rr;
+    const int st = *w.status;
+    const int cap = (L.nitm > 0) ? L.nitm : kMaxIterUnbounded;
+    const bool done = (st & kExtTimedOut) || sqrt(rr) < L.tol * sqrt(rr0) || cap == 1;
+    *w.done = done ? 1 : 0;
+    if (done && !std::is_same<TS, double>::value && L.lag_max > 0 && S.lag) {
+        const bool lagged = (st & kExtLagged) != 0;
+        const bool renew = (st & (kExtTimedOut | kExtBadPivot)) != 0;
+        const int age = S.lag[1];
+        S.lag[0] = S.tag;
+        S.lag[1] = renew ? L.lag_max : (lagged ? age + 1 : 1);
     }
 }
 
@@ -823,6 +975,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
     const long long wbase = line0 * kLine + lane;
 #define SK(p, s) (p)[wbase + (long long)(s) * kLine]
 
+    // the continuation launch of a solve with whole-GPU passes: nothing to do
+    // when the first iteration already met the stopping test (every CTA of a
+    // cluster reads the same word, so all return before any cluster barrier)
+    const bool cont = L.ext == 2;
+    if (cont) {
+        stamp(L, rank, 5);
+        if (*ext_words(S, ND, nx, ny).done) {
+            stamp(L, rank, 6);
+            return;
+        }
+    }
     if (threadIdx.x == 0) {
         vbad = 0u;
         mbar_init(&idle_bar, 1);
@@ -865,7 +1028,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
     // record as the launch found it; rank 0 rewrites it at the end)
     const bool lagged = lag_reuse<TS>(L, S);
     const int lag_age = lagged ? S.lag[1] : 0;
-    const bool reuse = L.reuse_lu || lagged;
+    const bool reuse = L.reuse_lu || lagged || cont;
+    // with whole-GPU passes the initial residual of a lagged solve comes from
+    // k_ext_r0, and a continuation starts from the first iteration's state
+    const bool given_r0 = (L.ext == 1 && lagged) || cont;
     cl.sync();   // mbarriers initialised before any use; A staged by k_skew_a
     bool bad_pivot = false, timed_out = false, hook_ran_out = false;
     int up_base = 0, dn_base = 0;       // batches sent so far on each channel
@@ -1002,6 +1168,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
     // also makes every row's factors and the residual final before the
     // first forward sweep)
     if (L.apply_only) rr0 = 0.0;
+    else if (given_r0) rr0 = S.rr[0];
     else if (reuse) rr0 = cluster_residual<ND, TS>(cl, a, S.b, x, (const TS *)nullptr, rp, nx, ny, SW, red, part);
     else rr0 = cluster_total(cl, part);
     stamp(L, rank, 2);
@@ -1014,9 +1181,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
         if (helper && !L.reuse_lu)
             verify_factors<ND>(asp, dlp, dup, rl1, nx, ny, SW, PS, rank * WPC, WPC, nhelp, hw, &vbad);
     }
-    bool lu_redone = !EXACT || L.reuse_lu;   // reused factors were checked when they were made
-    int nit = 0;
-    double rr = rr0;
+    bool lu_redone = !EXACT || L.reuse_lu || cont;   // reused factors were checked when they were made
+    int nit = cont ? 1 : 0;
+    double rr = cont ? S.rr[1] : rr0;
     for (;;) {
         nit = nit + 1;
         // test hook: wavefront warp 0 waits, bounded by L.hook_ns, on a
@@ -1230,6 +1397,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
             }
         }
         if (L.apply_only) break;   // x += z by k_unskew_add after the launch
+        if (L.ext == 1) break;     // x += z, the residual and the test on the whole GPU
         rr = cluster_residual<ND, TS>(cl, a, S.b, x, wp, rp, nx, ny, SW, red, part);
         if (nit == 1) stamp(L, rank, 5);
         if (sqrt(rr) < gammarp) break;
@@ -1246,16 +1414,26 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
         while (st.consumed < st.issued) (void)stage_wait(st, again);
     }
     if ((timed_out || hook_ran_out) && L.err) atomicOr(L.err, ERR_SPIN_TIMEOUT);
+    if (L.ext == 1) {
+        // what the whole-GPU passes and the continuation need to know
+        int* status = ext_words(S, ND, nx, ny).status;
+        if (timed_out || hook_ran_out) atomicOr(status, kExtTimedOut);
+        if (bad_pivot) atomicOr(status, kExtBadPivot);
+        if (lagged && rank == 0 && threadIdx.x == 0) atomicOr(status, kExtLagged);
+    }
     if (rank == 0 && threadIdx.x == 0 && !L.apply_only) {
         if (S.nit) *S.nit = nit;
-        if (S.rr) { S.rr[0] = rr0; S.rr[1] = rr; }
-        if (!EXACT && L.lag_max > 0 && S.lag && !L.reuse_lu) {
+        if (S.rr) { S.rr[0] = rr0; if (L.ext != 1) S.rr[1] = rr; }
+        if (!EXACT && L.lag_max > 0 && S.lag && !L.reuse_lu && L.ext != 1) {
             // the record for the next solve: fresh factors are one solve old;
             // reused ones age, and are renewed next time once they needed a
             // second iteration (or anything went wrong)
-            const bool renew = timed_out || hook_ran_out || bad_pivot || (lagged && nit > 1);
+            const int st = cont ? *ext_words(S, ND, nx, ny).status : 0;
+            const bool lag_solve = cont ? (st & kExtLagged) != 0 : lagged;
+            const bool renew = timed_out || hook_ran_out || bad_pivot || (st & (kExtTimedOut | kExtBadPivot)) ||
+                               (lag_solve && nit > 1);
             S.lag[0] = S.tag;
-            S.lag[1] = renew ? L.lag_max : (lagged ? lag_age + 1 : 1);
+            S.lag[1] = renew ? L.lag_max : (lag_solve ? lag_age + 1 : 1);
         }
     }
     cl.sync();   // no CTA leaves while another may still write into its shared memory
@@ -1317,21 +1495,48 @@ static cudaError_t launch_cluster(const MsiLaunch &L, int nsys, cudaStream_t st,
     const bool apply = L.apply_only && L.reuse_lu && L.dev == nullptr && nsys <= 2;
     const long long N = (long long)L.nx * L.ny;
     const dim3 cg((unsigned)((N + 255) / 256 < 1184 ? (N + 255) / 256 : 1184), (unsigned)nsys);
-    if (!L.reuse_lu) {
-        const dim3 sg((unsigned)((L.nx + kSkewPad + kSkewTile - 1) / kSkewTile), (unsigned)nwarps,
-                      (unsigned)(nsys * ND));
-        k_skew_a<ND, TS><<<sg, 256, 0, st>>>(L);
-    } else if (apply) {
-        k_skew_rhs<ND, TS><<<cg, 256, 0, st>>>(L);
-    }
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
+    // the passes over all cells on the whole GPU (grids of kExtMinCells and
+    // more, where they outweigh three extra launches)
+    bool ext = !L.apply_only && !L.reuse_lu && L.dev == nullptr && nsys <= 2 && N >= kExtMinCells;
+    for (int k = 0; k < nsys && ext; k++) ext = L.s[k].rr != nullptr && L.s[k].nit != nullptr;
     MsiLaunch La = L;
     La.apply_only = apply ? 1 : 0;
     if (apply) La.nitm = 1;
+    La.ext = ext ? 1 : 0;
+    const bool lag_r0 = ext && L.lag_max > 0 && !std::is_same<TS, double>::value;
+    int launches = 1;
+    if (!L.reuse_lu) {
+        const dim3 sg((unsigned)((L.nx + kSkewPad + kSkewTile - 1) / kSkewTile), (unsigned)nwarps,
+                      (unsigned)(nsys * ND));
+        k_skew_a<ND, TS><<<sg, 256, 0, st>>>(La);
+        launches++;
+        if (lag_r0) {
+            k_ext_r0<ND, TS><<<dim3(kExtBlocks, (unsigned)nsys), 256, 0, st>>>(La);
+            launches++;
+        }
+    } else if (apply) {
+        k_skew_rhs<ND, TS><<<cg, 256, 0, st>>>(La);
+        launches++;
+    }
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
     e = cudaLaunchKernelEx(&cfg, kern, La);
-    if (e != cudaSuccess || !apply) return e;
-    k_unskew_add<ND, TS><<<cg, 256, 0, st>>>(La);
+    if (e != cudaSuccess) return e;
+    if (apply) {
+        k_unskew_add<ND, TS><<<cg, 256, 0, st>>>(La);
+        launches++;
+    } else if (ext) {
+        k_ext_update<ND, TS><<<cg, 256, 0, st>>>(La);
+        k_ext_resid<ND, TS><<<dim3(kExtBlocks, (unsigned)nsys), 256, 0, st>>>(La);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        MsiLaunch Lc = La;
+        Lc.ext = 2;
+        e = cudaLaunchKernelEx(&cfg, kern, Lc);
+        launches += 3;
+    }
+    msi_note_launches(launches);
+    if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
 

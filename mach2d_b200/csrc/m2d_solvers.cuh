@@ -33,6 +33,10 @@ size_t msi_cluster_work_doubles(int nd, int nx, int ny);
 // 32 rows a warp sweeps read and write one contiguous 256-byte line per step
 size_t msi_skew_plane(int nx, int ny);
 
+// doubles after the wavefront-major planes of a cluster-kernel workspace:
+// block partial sums, counters and flags of the whole-GPU residual passes
+constexpr int kMsiExtScratch = 1024;
+
 struct MsiLaunch {
     int nx, ny, nitm;
     double tol;
@@ -63,12 +67,21 @@ struct MsiLaunch {
                                // and stopping test are unchanged, so only the preconditioner is
                                // older.  A stale solve that needs a second iteration marks the
                                // factors for renewal at the next solve.  0: factorise every solve.
+    int ext;                   // set by the cluster launcher, not by callers: 0 the residual passes
+                               // run inside the cluster kernel; 1 the first launch of a solve whose
+                               // passes run on the whole GPU (it stops after the first sweep pair);
+                               // 2 the continuation launch (further iterations, if any are needed)
     int variant;               // wavefront schedule: 0 automatic (one wavefront warp per SM when the
                                // cluster fits, else two), 1 one warp per SM (4 staging stages),
                                // 2 two warps per SM (2 stages), 3 the one-CTA kernel (FP64 only);
                                // a schedule that cannot run falls back to the one-CTA kernel.  Every
                                // schedule gives the same iterates.
 };
+
+// kernels the last launch_msi on this host thread issued (transposes and
+// whole-GPU passes included)
+int msi_last_launch_count();
+void msi_note_launches(int n);
 
 // Largest ny the one-CTA wavefront kernel accepts (its shared-memory ring
 // holds 4 steps x 4 factor values per row).
