@@ -230,7 +230,8 @@ extern "C" int m2d_create(const m2d_case *c, int device, m2d_ctx **out)
     const size_t strips = (size_t)9 * h.ny + 2 * (size_t)h.nx + 64;
     const size_t solver = 2 * msi_work_doubles(9, h.nx, h.ny) + msi_work_doubles(5, h.nx, h.ny) + 4 + 2 * N + 3 * 32;
     const size_t mixd = (sizeof(m2d_mixture) + sizeof(double) - 1) / sizeof(double);
-    const size_t total = nplanes * N + 32 * N + strips + solver + (size_t)red_parts() + 72 + S_COUNT + mixd;
+    const size_t total = nplanes * N + 32 * N + strips + solver + (size_t)kMaxMultiReduce * red_parts() + 72 +
+                         S_COUNT + mixd;
     e = cudaMalloc(&x->arena, total * sizeof(double));
     if (e != cudaSuccess) { cudaStreamDestroy(x->st); delete x; m2d_set_last_error(e, "cudaMalloc", __FILE__, __LINE__); return M2D_ERR_NOMEM; }
     cudaMemsetAsync(x->arena, 0, total * sizeof(double), x->st);
@@ -251,7 +252,7 @@ extern "C" int m2d_create(const m2d_case *c, int device, m2d_ctx **out)
     for (int k = 0; k < 2; k++) x->ws9[k] = take_aligned(msi_work_doubles(9, h.nx, h.ny));
     x->ws5 = take_aligned(msi_work_doubles(5, h.nx, h.ny) + 4);   // + the rr words of m2d_msi_workspace_doubles
     x->P = take(N); x->Q = take(N);
-    x->part = take((size_t)red_parts() + 8);
+    x->part = take((size_t)kMaxMultiReduce * red_parts() + 8);
     x->dsc = take(S_COUNT);
     x->dint = (int *)take(I_COUNT);
     x->dlag = (int *)take(4);   // factor records of ws9[0], ws9[1], ws5 (zeroed: no factors yet)
@@ -563,14 +564,14 @@ static int issue_iteration(m2d_ctx *x, bool capture, int *itp_used_out)
             if (rc) return rc;
         }
         {
-            RedArgs r = red(x, RED_NORM_L1_9D); r.a = f.au; r.b = f.bu; r.x = f.u;
-            KL(launch_reduce(r, x->part, x->dsc + S_NU_A, st), 1);
-            r.kind = RED_SUM_ABS_B;
-            KL(launch_reduce(r, x->part, x->dsc + S_NU_B, st), 1);
-            r = red(x, RED_NORM_L1_9D); r.a = f.av; r.b = f.bv; r.x = f.v;
-            KL(launch_reduce(r, x->part, x->dsc + S_NV_A, st), 1);
-            r.kind = RED_SUM_ABS_B;
-            KL(launch_reduce(r, x->part, x->dsc + S_NV_B, st), 1);
+            // the u and v norms (norm_l1_9d, norm_l1_b) in one launch
+            RedArgs r[4];
+            r[0] = red(x, RED_NORM_L1_9D); r[0].a = f.au; r[0].b = f.bu; r[0].x = f.u;
+            r[1] = r[0]; r[1].kind = RED_SUM_ABS_B;
+            r[2] = red(x, RED_NORM_L1_9D); r[2].a = f.av; r[2].b = f.bv; r[2].x = f.v;
+            r[3] = r[2]; r[3].kind = RED_SUM_ABS_B;
+            double *out[4] = {x->dsc + S_NU_A, x->dsc + S_NU_B, x->dsc + S_NV_A, x->dsc + S_NV_B};
+            KL(launch_reduce_multi(r, out, 4, x->part, st), 1);
         }
         KL(launch_velocities_at_internal_faces(f, q.dt, st, q.dtp), 1);
         KL(launch_velocities_at_boundary_faces(f, c.modvis, st), 1);
@@ -620,22 +621,23 @@ static int issue_iteration(m2d_ctx *x, bool capture, int *itp_used_out)
         int is[1] = {I_NIT_T}, rs[1] = {S_RR + 6};
         int rc = solve9(x, st, 1, a, b, v, is, rs);
         if (rc) return rc;
-        RedArgs r = red(x, RED_NORM_L1_9D); r.a = f.at; r.b = f.bt; r.x = f.T;
-        KL(launch_reduce(r, x->part, x->dsc + S_NT_A, st), 1);
-        r.kind = RED_SUM_ABS_B;
-        KL(launch_reduce(r, x->part, x->dsc + S_NT_B, st), 1);
+        RedArgs r[2];
+        r[0] = red(x, RED_NORM_L1_9D); r[0].a = f.at; r[0].b = f.bt; r[0].x = f.T;
+        r[1] = r[0]; r[1].kind = RED_SUM_ABS_B;
+        double *out[2] = {x->dsc + S_NT_A, x->dsc + S_NT_B};
+        KL(launch_reduce_multi(r, out, 2, x->part, st), 1);
     }
     KL(launch_density_at_nodes(f, q.Rg, st), 1);
     KL(launch_density_at_faces(f, c.beta, st), 1);
     if (c.dtmodel == 1) {
-        RedArgs r = red(x, RED_MEAN_CC_9D); r.a = f.au;
-        KL(launch_reduce(r, x->part, x->dsc + S_CC_U, st), 1);
-        r.a = f.av;
-        KL(launch_reduce(r, x->part, x->dsc + S_CC_V, st), 1);
-        r.a = f.at;
-        KL(launch_reduce(r, x->part, x->dsc + S_CC_T, st), 1);
-        r = red(x, RED_MEAN_CC_5D); r.a = f.ap;
-        KL(launch_reduce(r, x->part, x->dsc + S_CC_P, st), 1);
+        // the four mean convergence coefficients (get_mean_cc_9d/5d) in one launch
+        RedArgs r[4];
+        r[0] = red(x, RED_MEAN_CC_9D); r[0].a = f.au;
+        r[1] = r[0]; r[1].a = f.av;
+        r[2] = r[0]; r[2].a = f.at;
+        r[3] = red(x, RED_MEAN_CC_5D); r[3].a = f.ap;
+        double *out[4] = {x->dsc + S_CC_U, x->dsc + S_CC_V, x->dsc + S_CC_T, x->dsc + S_CC_P};
+        KL(launch_reduce_multi(r, out, 4, x->part, st), 1);
     }
     KL(launch_mass_flow_thrust(f, x->dsc + S_FMI, st), 1);
     if (capture) {

@@ -97,6 +97,10 @@ struct RedArgs {
     const double *dtp;     // when set, dt is read from this device word
 };
 cudaError_t launch_reduce(const RedArgs &r, double *part, double *out, cudaStream_t st);
+// n (<= kMaxMultiReduce) reductions in one launch, each bitwise what
+// launch_reduce gives; part holds n x red_parts() doubles
+constexpr int kMaxMultiReduce = 4;
+cudaError_t launch_reduce_multi(const RedArgs *r, double *const *out, int n, double *part, cudaStream_t st);
 
 // inlet/outlet strip integrals of get_mass_flow_rate_and_thrust: out[0..2] = fmi, fme, Fd
 cudaError_t launch_mass_flow_thrust(const Fields &f, double *out, cudaStream_t st);

@@ -107,7 +107,7 @@ __device__ __forceinline__ double block_reduce(double v, int c)
 // block to finish (a counter in part[kParts], back to zero afterwards)
 // combines the kParts partials in index order with the same tree, so the
 // result does not depend on which block finishes last.
-__global__ void __launch_bounds__(kThreads) k_reduce(RedArgs r, double *part, double *out)
+__device__ __forceinline__ void reduce_one(const RedArgs &r, double *part, double *out)
 {
     const int c = combine_of(r.kind);
     double acc = ident(c);
@@ -144,9 +144,40 @@ __global__ void __launch_bounds__(kThreads) k_reduce(RedArgs r, double *part, do
     }
 }
 
+__global__ void __launch_bounds__(kThreads) k_reduce(RedArgs r, double *part, double *out)
+{
+    reduce_one(r, part, out);
+}
+
 cudaError_t launch_reduce(const RedArgs &r, double *part, double *out, cudaStream_t st)
 {
     k_reduce<<<kParts, kThreads, 0, st>>>(r, part, out);
+    return cudaGetLastError();
+}
+
+// up to kMaxMultiReduce independent reductions in one launch: blockIdx.y
+// picks one, which runs exactly as k_reduce would (same shares, trees and
+// final combine, its own partials), so each result is bitwise that of its
+// own launch
+struct RedMulti {
+    RedArgs r[kMaxMultiReduce];
+    double *out[kMaxMultiReduce];
+};
+__global__ void __launch_bounds__(kThreads) k_reduce_multi(RedMulti m, double *part)
+{
+    const int y = blockIdx.y;
+    reduce_one(m.r[y], part + (long long)y * (kParts + 1), m.out[y]);
+}
+
+cudaError_t launch_reduce_multi(const RedArgs *r, double *const *out, int n, double *part, cudaStream_t st)
+{
+    if (n < 1 || n > kMaxMultiReduce) return cudaErrorInvalidValue;
+    RedMulti m;
+    for (int k = 0; k < n; k++) {
+        m.r[k] = r[k];
+        m.out[k] = out[k];
+    }
+    k_reduce_multi<<<dim3(kParts, (unsigned)n), kThreads, 0, st>>>(m, part);
     return cudaGetLastError();
 }
 
