@@ -462,9 +462,7 @@ static int issue_p_cycle(m2d_ctx *x, const Params &q, cudaStream_t s)
     Fields &f = x->f;
     Params qc = q;
     qc.maxpl = x->dsc + S_MAXPL;    // zeroed by the coefficient pass, maximised by the update
-    KL(launch_p_assembly(f, qc, ASM_COEF, s), 1);
-    KL(launch_set_bcpl(f, s), 1);
-    KL(launch_p_assembly(f, q, ASM_SRC, s), 1);
+    KL(launch_p_assembly_bc(f, qc, s), 1);   // coefficients, boundary rows and source
     int rc = solve5(x, s);
     if (rc) return rc;
     // face corrections, boundary faces, p and rho corrections and max|p'|
@@ -551,10 +549,8 @@ static int issue_iteration(m2d_ctx *x, bool capture, int *itp_used_out)
     bool have_pavg = false;
     int itp_used = 0;
     for (int itm = 1; itm <= c.itmmax; itm++) {
-        KL(launch_u_assembly(f, q, ASM_COEF | ASM_SRC, st), 1);
-        KL(launch_set_bcu(f, c.modvis, st), 1);
-        KL(launch_v_assembly(f, q, ASM_COEF | ASM_SRC, st), 1);
-        KL(launch_set_bcv(f, c.modvis, st), 1);
+        // u and v coefficients, sources and boundary rows in one launch
+        KL(launch_uv_assembly_bc(f, q, c.modvis, st), 1);
         KL(launch_internal_simplec(f, st), 1);
         KL(launch_boundary_simplec(f, st), 1);
         {
@@ -573,8 +569,7 @@ static int issue_iteration(m2d_ctx *x, bool capture, int *itp_used_out)
             double *out[4] = {x->dsc + S_NU_A, x->dsc + S_NU_B, x->dsc + S_NV_A, x->dsc + S_NV_B};
             KL(launch_reduce_multi(r, out, 4, x->part, st), 1);
         }
-        KL(launch_velocities_at_internal_faces(f, q.dt, st, q.dtp), 1);
-        KL(launch_velocities_at_boundary_faces(f, c.modvis, st), 1);
+        KL(launch_faces_all(f, q.dt, c.modvis, st, q.dtp), 1);   // internal and boundary faces
         TRY(cudaMemsetAsync(f.pl, 0, x->N * sizeof(double), st));
         if (capture) {
             k_ctx_itp_reset<<<1, 1, 0, st>>>(x->dint);

@@ -44,6 +44,12 @@ enum { ASM_COEF = 1, ASM_SRC = 2 };
 cudaError_t launch_density_at_nodes(const Fields &f, double Rg, cudaStream_t st);
 cudaError_t launch_density_at_faces(const Fields &f, double beta, cudaStream_t st);
 cudaError_t launch_u_assembly(const Fields &f, const Params &q, int what, cudaStream_t st);
+// fused launches of the iteration (bitwise the separate kernels): u and v
+// assembly with their boundary rows; internal and boundary face
+// velocities; the p' coefficients, source and boundary rows of one cycle
+cudaError_t launch_uv_assembly_bc(const Fields &f, const Params &q, int modvis, cudaStream_t st);
+cudaError_t launch_faces_all(const Fields &f, double dt, int modvis, cudaStream_t st, const double *dtp);
+cudaError_t launch_p_assembly_bc(const Fields &f, const Params &q, cudaStream_t st);
 cudaError_t launch_v_assembly(const Fields &f, const Params &q, int what, cudaStream_t st);
 cudaError_t launch_T_assembly(const Fields &f, const Params &q, cudaStream_t st);
 cudaError_t launch_p_assembly(const Fields &f, const Params &q, int what, cudaStream_t st);

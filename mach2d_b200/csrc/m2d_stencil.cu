@@ -53,11 +53,10 @@ __global__ void k_density_faces(Fields f, double beta)
 
 // ---------------------------------------------------------------------------
 // get_u_coefficients + get_u_source  src/equations/mach2d_coef.f90:63-451
-__global__ void k_u_assembly(Fields f, Params q, int what)
+__device__ __forceinline__ void u_assembly_cell(const Fields &f, const Params &q, int what, int i, int j)
 {
     const int nx = f.nx, ny = f.ny;
     const long long N = (long long)nx * ny;
-    CELL_IJ
     if (i < 2 || i > nx - 1 || j < 2 || j > ny - 1) return;
     const long long np = IDX(i, j), nps = np - nx, npn = np + nx, npw = np - 1, npe = np + 1;
     const double *roe = f.roe, *ron = f.ron, *re = f.re, *rn = f.rn, *Uce = f.Uce, *Vcn = f.Vcn;
@@ -149,13 +148,17 @@ __global__ void k_u_assembly(Fields f, Params q, int what)
     }
     f.bu[np] = b;
 }
+__global__ void k_u_assembly(Fields f, Params q, int what)
+{
+    CELL_IJ
+    u_assembly_cell(f, q, what, i, j);
+}
 
 // get_v_coefficients + get_v_source  src/equations/mach2d_coef.f90:454-783
-__global__ void k_v_assembly(Fields f, Params q, int what)
+__device__ __forceinline__ void v_assembly_cell(const Fields &f, const Params &q, int what, int i, int j)
 {
     const int nx = f.nx, ny = f.ny;
     const long long N = (long long)nx * ny;
-    CELL_IJ
     if (i < 2 || i > nx - 1 || j < 2 || j > ny - 1) return;
     const long long np = IDX(i, j), nps = np - nx, npn = np + nx, npw = np - 1, npe = np + 1;
     const double *roe = f.roe, *ron = f.ron, *re = f.re, *rn = f.rn, *Uce = f.Uce, *Vcn = f.Vcn;
@@ -234,6 +237,11 @@ __global__ void k_v_assembly(Fields f, Params q, int what)
         b = b + svp;
     }
     f.bv[np] = b;
+}
+__global__ void k_v_assembly(Fields f, Params q, int what)
+{
+    CELL_IJ
+    v_assembly_cell(f, q, what, i, j);
 }
 
 // get_T_coefficients_and_source  src/equations/mach2d_coef.f90:787-1203
@@ -374,11 +382,10 @@ __global__ void k_T_assembly(Fields f, Params q)
 }
 
 // get_p_coefficients + get_p_source  src/equations/mach2d_coef.f90:1207-1348
-__global__ void k_p_assembly(Fields f, Params q, int what)
+__device__ __forceinline__ void p_assembly_cell(const Fields &f, const Params &q, int what, int i, int j)
 {
     const int nx = f.nx, ny = f.ny;
     const long long N = (long long)nx * ny;
-    CELL_IJ
     if (q.maxpl && (what & ASM_COEF) && i == 1 && j == 1) *q.maxpl = 0.0;   // k_p_cycle_update's max|p'|
     if (i < 2 || i > nx - 1 || j < 2 || j > ny - 1) return;
     const long long np = IDX(i, j), nps = np - nx, npn = np + nx, npw = np - 1, npe = np + 1;
@@ -417,14 +424,18 @@ __global__ void k_p_assembly(Fields f, Params q, int what)
                  - ronl * rn[np] * Vcnl + rosl * rn[nps] * Vcsl;
     }
 }
+__global__ void k_p_assembly(Fields f, Params q, int what)
+{
+    CELL_IJ
+    p_assembly_cell(f, q, what, i, j);
+}
 
 // get_velocities_at_internal_faces  src/equations/mach2d_coef.f90:1350-1501
-__global__ void k_faces_internal(Fields f, double dt, const double *dtp)
+__device__ __forceinline__ void faces_internal_cell(const Fields &f, double dt, const double *dtp, int i, int j)
 {
     if (dtp) dt = *dtp;
     const int nx = f.nx, ny = f.ny;
     const long long N = (long long)nx * ny;
-    CELL_IJ
     if (i < 2 || i > nx - 1 || j < 2 || j > ny - 1) return;
     const long long np = IDX(i, j), nps = np - nx, npn = np + nx, npw = np - 1, npe = np + 1;
     const long long npsw = nps - 1, npse = nps + 1, npnw = npn - 1, npne = npn + 1;
@@ -476,6 +487,11 @@ __global__ void k_faces_internal(Fields f, double dt, const double *dtp)
         f.vn[np] = vn;
         f.Vcn[np] = vn * f.xk[np] - un * f.yk[np];
     }
+}
+__global__ void k_faces_internal(Fields f, double dt, const double *dtp)
+{
+    CELL_IJ
+    faces_internal_cell(f, dt, dtp, i, j);
 }
 
 __device__ __forceinline__ double sum9(const double *a, long long N, long long np)
@@ -702,6 +718,10 @@ __device__ __forceinline__ bool strip_of(int q, int nx, int ny, int &side, int &
     if (q < nx) { side = 3; idx = q + 1; return true; }
     return false;
 }
+#define STRIP_VARS                                              \
+    const int nx = f.nx, ny = f.ny;                             \
+    const long long N = (long long)nx * ny;                     \
+    (void)N;
 #define STRIP_HEAD                                              \
     const int nx = f.nx, ny = f.ny;                             \
     const long long N = (long long)nx * ny;                     \
@@ -719,9 +739,9 @@ __device__ __forceinline__ void set_row9(double *a, long long N, long long np, i
 }
 
 // intflow_set_bcu  mod_intflow.f90:214-301
-__global__ void k_set_bcu(Fields f, int modvis)
+__device__ __forceinline__ void set_bcu_strip(const Fields &f, int modvis, int side, int idx)
 {
-    STRIP_HEAD
+    STRIP_VARS
     const double *x = f.x, *xp = f.xp, *u = f.u;
     if (side == 0) {
         int j = idx; if (j < 2 || j > ny - 1) return;
@@ -744,11 +764,17 @@ __global__ void k_set_bcu(Fields f, int modvis)
         else { double ub, vb; north_slip(f, idx, ub, vb); f.bu[np] = 2.0 * ub; }
     }
 }
+__global__ void k_set_bcu(Fields f, int modvis)
+{
+    int side, idx;
+    if (!strip_of(blockIdx.x * blockDim.x + threadIdx.x, f.nx, f.ny, side, idx)) return;
+    set_bcu_strip(f, modvis, side, idx);
+}
 
 // intflow_set_bcv  mod_intflow.f90:305-392
-__global__ void k_set_bcv(Fields f, int modvis)
+__device__ __forceinline__ void set_bcv_strip(const Fields &f, int modvis, int side, int idx)
 {
-    STRIP_HEAD
+    STRIP_VARS
     const double *x = f.x, *xp = f.xp, *v = f.v;
     if (side == 0) {
         int j = idx; if (j < 2 || j > ny - 1) return;
@@ -771,6 +797,12 @@ __global__ void k_set_bcv(Fields f, int modvis)
         else { double ub, vb; north_slip(f, idx, ub, vb); f.bv[np] = 2.0 * vb; }
     }
 }
+__global__ void k_set_bcv(Fields f, int modvis)
+{
+    int side, idx;
+    if (!strip_of(blockIdx.x * blockDim.x + threadIdx.x, f.nx, f.ny, side, idx)) return;
+    set_bcv_strip(f, modvis, side, idx);
+}
 
 __device__ __forceinline__ void set_row5(double *a, long long N, long long np, int k1, double v1)
 {
@@ -781,9 +813,9 @@ __device__ __forceinline__ void set_row5(double *a, long long N, long long np, i
 }
 
 // intflow_set_bcpl  mod_intflow.f90:396-459 (corner rows untouched)
-__global__ void k_set_bcpl(Fields f)
+__device__ __forceinline__ void set_bcpl_strip(const Fields &f, int side, int idx)
 {
-    STRIP_HEAD
+    STRIP_VARS
     if (side == 0) {
         int j = idx; if (j < 2 || j > ny - 1) return;
         long long np = IDX(1, j);
@@ -805,6 +837,12 @@ __global__ void k_set_bcpl(Fields f)
         set_row5(f.ap, N, np, 1, -1.0);
         f.bp[np] = 0.0;
     }
+}
+__global__ void k_set_bcpl(Fields f)
+{
+    int side, idx;
+    if (!strip_of(blockIdx.x * blockDim.x + threadIdx.x, f.nx, f.ny, side, idx)) return;
+    set_bcpl_strip(f, side, idx);
 }
 
 // intflow_set_bcT  mod_intflow.f90:464-550
@@ -833,9 +871,9 @@ __global__ void k_set_bcT(Fields f, double Twall)
 }
 
 // intflow_velocities_at_boundary_faces  mod_intflow.f90:692-787
-__global__ void k_faces_boundary(Fields f, int modvis)
+__device__ __forceinline__ void faces_boundary_strip(const Fields &f, int modvis, int side, int idx)
 {
-    STRIP_HEAD
+    STRIP_VARS
     const double *u = f.u, *v = f.v;
     if (side == 0) {
         int j = idx; if (j < 2 || j > ny - 1) return;
@@ -862,6 +900,12 @@ __global__ void k_faces_boundary(Fields f, int modvis)
         if (modvis == 0) north_slip_inner(f, i, ub, vb);
         f.un[np] = ub; f.vn[np] = vb; f.Vcn[np] = 0.0;
     }
+}
+__global__ void k_faces_boundary(Fields f, int modvis)
+{
+    int side, idx;
+    if (!strip_of(blockIdx.x * blockDim.x + threadIdx.x, f.nx, f.ny, side, idx)) return;
+    faces_boundary_strip(f, modvis, side, idx);
 }
 
 // intflow_boundary_simplec  mod_intflow.f90:791-877
@@ -1085,6 +1129,62 @@ __global__ void k_backup(Fields f)
     }
 }
 
+// ---- fused launches: kernels whose cells are disjoint and that read none of
+// each other's outputs run as one launch, every cell computed by the same
+// device function as in its own kernel (bitwise the separate launches)
+
+// ring cell (i, j) -> the strip entry of the boundary kernels that covers it
+// (the corners belong to the south and north strips; the west and east
+// strips skip them)
+__device__ __forceinline__ bool ring_strip(int i, int j, int nx, int ny, int &side, int &idx)
+{
+    if (j == 1) { side = 2; idx = i; return true; }
+    if (j == ny) { side = 3; idx = i; return true; }
+    if (i == 1) { side = 0; idx = j; return true; }
+    if (i == nx) { side = 1; idx = j; return true; }
+    return false;
+}
+
+// u and v coefficients and sources on the real cells, intflow_set_bcu/bcv on
+// the ring
+__global__ void k_uv_assembly_bc(Fields f, Params q, int modvis)
+{
+    CELL_IJ
+    if (i > f.nx || j > f.ny) return;
+    int side, idx;
+    if (ring_strip(i, j, f.nx, f.ny, side, idx)) {
+        set_bcu_strip(f, modvis, side, idx);
+        set_bcv_strip(f, modvis, side, idx);
+    } else {
+        u_assembly_cell(f, q, ASM_COEF | ASM_SRC, i, j);
+        v_assembly_cell(f, q, ASM_COEF | ASM_SRC, i, j);
+    }
+}
+
+// the internal face velocities and the boundary faces
+__global__ void k_faces_all(Fields f, double dt, const double *dtp, int modvis)
+{
+    CELL_IJ
+    if (i > f.nx || j > f.ny) return;
+    int side, idx;
+    if (ring_strip(i, j, f.nx, f.ny, side, idx)) faces_boundary_strip(f, modvis, side, idx);
+    else faces_internal_cell(f, dt, dtp, i, j);
+}
+
+// the p' coefficients and source of one cycle and intflow_set_bcpl
+__global__ void k_p_assembly_bc(Fields f, Params q)
+{
+    CELL_IJ
+    if (i > f.nx || j > f.ny) return;
+    int side, idx;
+    if (ring_strip(i, j, f.nx, f.ny, side, idx)) {
+        if (i == 1 && j == 1 && q.maxpl) *q.maxpl = 0.0;   // as p_assembly_cell does at (1, 1)
+        set_bcpl_strip(f, side, idx);
+    } else {
+        p_assembly_cell(f, q, ASM_COEF | ASM_SRC, i, j);
+    }
+}
+
 // ---------------------------------------------------------------------------
 static inline dim3 grid1d(long long N)
 {
@@ -1098,6 +1198,12 @@ static inline dim3 grid_strip(int nx, int ny)
     return dim3((unsigned)((2 * nx + 2 * ny + 127) / 128));
 }
 
+cudaError_t launch_uv_assembly_bc(const Fields &f, const Params &q, int modvis, cudaStream_t st)
+{ k_uv_assembly_bc<<<grid2d(f.nx, f.ny), kBlock2d, 0, st>>>(f, q, modvis); return cudaGetLastError(); }
+cudaError_t launch_faces_all(const Fields &f, double dt, int modvis, cudaStream_t st, const double *dtp)
+{ k_faces_all<<<grid2d(f.nx, f.ny), kBlock2d, 0, st>>>(f, dt, dtp, modvis); return cudaGetLastError(); }
+cudaError_t launch_p_assembly_bc(const Fields &f, const Params &q, cudaStream_t st)
+{ k_p_assembly_bc<<<grid2d(f.nx, f.ny), kBlock2d, 0, st>>>(f, q); return cudaGetLastError(); }
 cudaError_t launch_density_at_nodes(const Fields &f, double Rg, cudaStream_t st)
 { k_density_nodes<<<grid1d((long long)f.nx * f.ny), 256, 0, st>>>(f, Rg); return cudaGetLastError(); }
 cudaError_t launch_density_at_faces(const Fields &f, double beta, cudaStream_t st)
