@@ -38,6 +38,12 @@ def _gpu_msi(nd, nx, ny, nitm, tol, a, b, x):
     (66, 34, 20, 1e-2, 2),
     (130, 70, 30, 1e-6, 3),
     (40, 300, 4, 1e-30, 4),      # ny > nx: long wavefront, several rows per thread pass
+    # 2^16 cells and more: the residual passes run on the whole GPU and a
+    # continuation launch iterates; stopped by the tolerance, by a cap of
+    # one iteration (the first launch's state alone) and of two
+    (300, 240, 40, 1e-8, 5),
+    (260, 256, 1, 1e-30, 6),
+    (260, 256, 2, 1e-30, 7),
 ])
 def test_msi_bitwise(nd, nx, ny, nitm, tol, seed):
     a, b = random_dominant_planes(nd, nx, ny, seed=seed)
