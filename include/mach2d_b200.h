@@ -152,8 +152,8 @@ int m2d_msi_solve_device_mixed(int nd, int nx, int ny, int nitm, double tol, con
  * device reset between calls leaves no stale address; the first call on a
  * device also loads the device code there, so make it before any stream
  * capture.  The fast cluster kernel runs only while its wavefront-major
- * layout fits in the array (32*ceil(ny/32) * (nx + 62) <= 74898 for nd = 9,
- * <= 104857 for nd = 5); other grids under the cell limit, 514 x 258 with
+ * layout fits in the array (32*ceil(ny/32) * (nx + 62) <= 74849 for nd = 9,
+ * <= 104789 for nd = 5); other grids under the cell limit, 514 x 258 with
  * nd = 9 among them, run the bitwise-equal but slower one-CTA kernel.  All
  * calls share the array: calls that overlap on the GPU race and must be
  * serialised by the caller. */

@@ -23,8 +23,8 @@
 // norms), so nothing needs clearing, but calls that overlap on the GPU (two
 // streams, or two host threads) race on it and must be serialised by the
 // caller.  The cluster kernel runs only while its wavefront-major layout fits
-// in the array, that is while 32*ceil(ny/32) * (nx + 62) is at most 74,898
-// (9 diagonals) or 104,857 (5 diagonals); otherwise the one-CTA kernel,
+// in the array, that is while 32*ceil(ny/32) * (nx + 62) is at most 74,849
+// (9 diagonals) or 104,789 (5 diagonals); otherwise the one-CTA kernel,
 // bitwise equal but slower, runs.  At 514 x 258 (512 x 256 real cells) the
 // 9-diagonal solve therefore takes the one-CTA kernel.
 #include "m2d_solvers.cuh"
