@@ -54,14 +54,20 @@ namespace cg = cooperative_groups;
 namespace m2d {
 
 namespace {
-constexpr int kLag = 16;          // steps per batch = per-warp time lag
-constexpr int kRing = 128;        // ring slots; a producer may lead its consumer by 5 batches
+constexpr int kRing = 128;        // ring entries per channel (kSlots batches)
 constexpr int kThreads = 256;     // threads per CTA (wavefront warps + helpers)
 constexpr int kMaxCluster = 16;
 constexpr int kSkewPad = 62;      // slots per warp = nx + 62 (slot s = i + 2 lane)
-constexpr int kLine = 32;         // doubles per slot line, one per lane
-constexpr int kBlock = kLag * kLine;   // doubles of one plane for one batch (4 KB)
-constexpr int kSlots = kRing / kLag;    // ring slots, one batch each
+constexpr int kLine = 32;         // values per slot line, one per lane
+// Steps per batch = the per-warp time lag.  FP64: 16.  FP32: 32, whose
+// shorter steps made the per-batch hand-off and staging show (measured at
+// 514x258: forward sweeps 11-12 % and backward sweeps 22-24 % faster with
+// 32-step batches; the FP64 factorisation runs slower with them).
+template <typename TS> struct Batch {
+    static constexpr int kLag = std::is_same<TS, float>::value ? 32 : 16;
+    static constexpr int kBlock = kLag * kLine;   // elements of one plane for one batch
+    static constexpr int kSlots = kRing / kLag;   // ring slots, one batch each
+};
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kMaxIterUnbounded = 10000;
 constexpr unsigned long long kWaitLimitNs = 4000000000ull;   // bound of every wait (4 s of %globaltimer)
@@ -277,7 +283,7 @@ struct Stager {
     int base;                    // this warp's area in it (elements)
     unsigned long long *bar;
     int issued, consumed;
-    __device__ int block(int q) const { return base + q * PMAX * kBlock; }
+    __device__ int block(int q) const { return base + q * PMAX * Batch<TS>::kBlock; }
 };
 
 // stage slot lines [s_lo, s_lo + kLag) of NP wavefront-major planes (lines
@@ -289,14 +295,14 @@ __device__ __forceinline__ void stage_issue(Stager<TS, NSTAGE, PMAX> &st, TS *co
     const int q = st.issued % NSTAGE;
     if ((threadIdx.x & 31) == 0) {
         fence_async_shared();   // earlier reads of this block precede the copies into it
-        const int lo = max(s_lo, 0), hi = min(s_lo + kLag, sw);
+        const int lo = max(s_lo, 0), hi = min(s_lo + Batch<TS>::kLag, sw);
         const unsigned bytes = hi > lo ? (unsigned)(hi - lo) * kLine * (unsigned)sizeof(TS) : 0u;
         mbar_arrive_tx(&st.bar[q], bytes * NP);
         if (bytes) {
             TS *dst = st.mem + st.block(q) + (lo - s_lo) * kLine;
 #pragma unroll
             for (int p = 0; p < NP; p++)
-                bulk_g2s(dst + p * kBlock, planes[p] + (line0 + lo) * kLine, bytes, &st.bar[q]);
+                bulk_g2s(dst + p * Batch<TS>::kBlock, planes[p] + (line0 + lo) * kLine, bytes, &st.bar[q]);
         }
     }
     st.issued++;
@@ -321,30 +327,35 @@ __device__ __forceinline__ int stage_wait(Stager<TS, NSTAGE, PMAX> &st, bool &ti
 // slot.  The consumer frees the slot by arriving on the producer's "empty"
 // barrier.  Batch numbers n count over all phases of a channel, so the k-th
 // use of a slot is phase k of its barriers.
+template <typename TS>
 __device__ __forceinline__ void chan_recv(unsigned long long *full, int n, unsigned bytes, bool &timed_out)
 {
+    constexpr int kSlots = Batch<TS>::kSlots;
     unsigned long long *bar = &full[n & (kSlots - 1)];
     if ((threadIdx.x & 31) == 0) mbar_arrive_tx(bar, bytes);
     __syncwarp();
     mbar_wait(bar, (unsigned)(n / kSlots) & 1u, timed_out);
 }
 // producer, before staging batch n: the consumer has released batch n - kSlots
+template <typename TS>
 __device__ __forceinline__ void chan_slot_free(unsigned long long *empty, int n, bool &timed_out)
 {
+    constexpr int kSlots = Batch<TS>::kSlots;
     if (n >= kSlots) mbar_wait(&empty[n & (kSlots - 1)], (unsigned)(n / kSlots - 1) & 1u, timed_out);
 }
 // producer lane that staged the values: ship batch n (vals elements)
 template <typename TS>
 __device__ __forceinline__ void chan_send(unsigned ring_dst, unsigned full_dst, const TS *out, int n, int vals)
 {
-    const int slot = n & (kSlots - 1);
+    const int slot = n & (Batch<TS>::kSlots - 1);
     fence_async_shared();   // the staged values become visible to the bulk copy
     bulk_s2s(ring_dst + (unsigned)(slot * vals) * (unsigned)sizeof(TS), out + slot * vals,
              (unsigned)vals * (unsigned)sizeof(TS), full_dst + (unsigned)slot * 8u);
 }
+template <typename TS>
 __device__ __forceinline__ void chan_release(unsigned empty_dst, int n)
 {
-    mbar_remote_arrive(empty_dst + (unsigned)(n & (kSlots - 1)) * 8u);
+    mbar_remote_arrive(empty_dst + (unsigned)(n & (Batch<TS>::kSlots - 1)) * 8u);
 }
 
 // wavefront-major slot of cell (i, j): warp j/32, step offset i + 2 (j%32), lane j%32
@@ -924,6 +935,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
     constexpr int PMAX = (ND > NL + 2) ? ND : NL + 2;   // planes staged per batch
     constexpr int DIAG = (ND == 9) ? 4 : 2;      // index of the main diagonal in a row of A
     constexpr unsigned ES = sizeof(TS);
+    constexpr int kLag = Batch<TS>::kLag, kBlock = Batch<TS>::kBlock, kSlots = Batch<TS>::kSlots;
     // per wavefront warp of this CTA.  Consumer side: rings of values from the
     // neighbour warps and their "full" barriers; producer side: staging of the
     // values for the neighbours and the "empty" barriers the neighbours release.
@@ -1055,8 +1067,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
             const int tb = b * kLag;
             const int n = up_base + b;                          // global batch number on the channel
             const bool send = has_above && b <= nbatch - 2;   // the last batch is never read
-            if (has_below && b >= 1) chan_recv(&full_up[fw][0], n - 1, kLag * NU * ES, timed_out);
-            if (send) chan_slot_free(&empty_up[fw][0], n, timed_out);
+            if (has_below && b >= 1) chan_recv<TS>(&full_up[fw][0], n - 1, kLag * NU * ES, timed_out);
+            if (send) chan_slot_free<TS>(&empty_up[fw][0], n, timed_out);
             const int bo = stage_wait(st, timed_out) + lane;
             if (b + NSTAGE - 1 < nbatch) stage_issue<ND>(st, ap, line0, (b + NSTAGE - 1) * kLag - soff, SW);
             const unsigned rbase = (unsigned)up_base * kLag;
@@ -1137,9 +1149,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
             }
             store_prev();
             if (lane == 31 && send) chan_send(up_ring_dst, up_full_dst, &out_up[fw][0], n, kLag * NU);
-            if (lane == 0 && has_below && b >= 2) chan_release(up_empty_dst, n - 2);
+            if (lane == 0 && has_below && b >= 2) chan_release<TS>(up_empty_dst, n - 2);
         }
-        if (lane == 0 && has_below && nbatch >= 2) chan_release(up_empty_dst, up_base + nbatch - 2);
+        if (lane == 0 && has_below && nbatch >= 2) chan_release<TS>(up_empty_dst, up_base + nbatch - 2);
         if (piv) bad_pivot = true;
         fence_async_global();   // the sweeps read the factors with bulk copies
     };
@@ -1208,8 +1220,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                 const int tb = b * kLag;
                 const int n = up_base + b;
                 const bool send = has_above && b <= nbatch - 2;
-                if (has_below && b >= 1) chan_recv(&full_up[fw][0], n - 1, kLag * ES, timed_out);
-                if (send) chan_slot_free(&empty_up[fw][0], n, timed_out);
+                if (has_below && b >= 1) chan_recv<TS>(&full_up[fw][0], n - 1, kLag * ES, timed_out);
+                if (send) chan_slot_free<TS>(&empty_up[fw][0], n, timed_out);
                 const int bo = stage_wait(st, timed_out) + lane;
                 if (b + NSTAGE - 1 < nbatch) stage_issue<NL + 2>(st, fp, line0, (b + NSTAGE - 1) * kLag - soff, SW);
                 const TS m0 = mine, b1 = a1, b2 = a2, b3 = a3;   // state at batch start
@@ -1287,9 +1299,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                     }
                 }
                 if (lane == 31 && send) chan_send(up_ring_dst, up_full_dst, &out_up[fw][0], n, kLag);
-                if (lane == 0 && has_below && b >= 2) chan_release(up_empty_dst, n - 2);
+                if (lane == 0 && has_below && b >= 2) chan_release<TS>(up_empty_dst, n - 2);
             }
-            if (lane == 0 && has_below && nbatch >= 2) chan_release(up_empty_dst, up_base + nbatch - 2);
+            if (lane == 0 && has_below && nbatch >= 2) chan_release<TS>(up_empty_dst, up_base + nbatch - 2);
             fence_async_global();   // the backward sweep reads w with bulk copies
             __syncwarp();
         }
@@ -1311,8 +1323,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                 const int tb = b * kLag;
                 const int n = dn_base + b;
                 const bool send = has_below && b <= nbatch - 2;
-                if (has_above && b >= 1) chan_recv(&full_dn[fw][0], n - 1, kLag * ES, timed_out);
-                if (send) chan_slot_free(&empty_dn[fw][0], n, timed_out);
+                if (has_above && b >= 1) chan_recv<TS>(&full_dn[fw][0], n - 1, kLag * ES, timed_out);
+                if (send) chan_slot_free<TS>(&empty_dn[fw][0], n, timed_out);
                 const int bo = stage_wait(st, timed_out) + lane;
                 if (b + NSTAGE - 1 < nbatch)
                     stage_issue<NU + 1>(st, bp, line0, Tmax - ((b + NSTAGE - 1) * kLag + kLag - 1) - soff, SW);
@@ -1370,9 +1382,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                     stg_if(wp + wbase + (long long)sl * kLine, pz, has_rows && sl >= 0 && sl < SW);
                 }
                 if (lane == 0 && send) chan_send(dn_ring_dst, dn_full_dst, &out_dn[fw][0], n, kLag);
-                if (lane == 31 && has_above && b >= 2) chan_release(dn_empty_dst, n - 2);
+                if (lane == 31 && has_above && b >= 2) chan_release<TS>(dn_empty_dst, n - 2);
             }
-            if (lane == 31 && has_above && nbatch >= 2) chan_release(dn_empty_dst, dn_base + nbatch - 2);
+            if (lane == 31 && has_above && nbatch >= 2) chan_release<TS>(dn_empty_dst, dn_base + nbatch - 2);
         }
         dn_base += nbatch - 1;
         if (nit == 1) stamp(L, rank, 4);
@@ -1454,7 +1466,7 @@ static size_t stage_bytes()
 {
     constexpr int NL = (ND == 9) ? 5 : 4;
     constexpr int PMAX = (ND > NL + 2) ? ND : NL + 2;
-    return (size_t)WPC * NSTAGE * PMAX * kBlock * sizeof(TS);
+    return (size_t)WPC * NSTAGE * PMAX * Batch<TS>::kBlock * sizeof(TS);
 }
 
 // launches one cluster per system if the cluster shape can be scheduled;
