@@ -1187,7 +1187,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
     const double gammarp = L.tol * sqrt(rr0);
     const int cap = (L.nitm > 0) ? L.nitm : kMaxIterUnbounded;
     // while the first sweeps run, the helper warps check that every stored
-    // factor is the IEEE result of its stored inputs; the verdict is read
+    // factor is the IEEE result of its stored inputs; their finding is read
     // before the first correction of x
     if constexpr (EXACT) {
         if (helper && !L.reuse_lu)
@@ -1390,7 +1390,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
         if (nit == 1) stamp(L, rank, 4);
         // var = z + var, then the new residual
         if (!lu_redone) {
-            // the helpers' verdict on the Markstein factorisation: if any
+            // the helpers' finding on the Markstein factorisation: if any
             // factor differs from IEEE division, factorise again with IEEE
             // division and repeat the first iteration (x is still untouched)
             cl.sync();
@@ -1399,7 +1399,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
             lu_redone = true;
             if (any) {
                 if (rank == 0 && threadIdx.x == 0) atomicAdd(&g_lu_redo, 1ull);
-                cl.sync();   // every CTA has read the verdicts
+                cl.sync();   // every CTA has read the findings
                 if (front) run_lu(std::true_type{});
                 up_base += nbatch - 1;
                 if (bad_pivot && L.err) atomicOr(L.err, ERR_NONFINITE_PIVOT);

@@ -4,7 +4,7 @@
 // No counterpart in the reference: it maps (p' residual, the nine
 // coefficient planes, the Jacobian) to a p' correction that the flexible
 // pressure-correction solve (m2d_pprime_solve_learned) tries before the MSI
-// iteration, keeping plain MSI as the fallback and the judge.
+// iteration, keeping plain MSI as the fallback and the arbiter.
 //
 // Layout: activations are pixel-major (NHWC), a pixel's channels contiguous,
 // so the K slice of one 3x3 tap is one 32-byte row per 16 channels.  Images
@@ -1475,7 +1475,7 @@ extern "C" int m2d_pprime_solve_learned(m2d_unet *n, int nx, int ny, int nitm, d
         tol_eff = r1 > 0.0 ? tol * r0 / r1 : 1.0;
     }
     int nit = 0;
-    // at least one MSI iteration, as the judge of the correction -- unless the
+    // at least one MSI iteration, as the arbiter of the correction -- unless the
     // corrected residual, measured in FP64, already passes MSI's own stopping
     // test and the caller allows the correction to stand alone
     const bool skip_msi = alone && accept && r1 < tol * r0;
