@@ -292,18 +292,22 @@ template <int NP, typename TS, int NSTAGE, int PMAX>
 __device__ __forceinline__ void stage_issue(Stager<TS, NSTAGE, PMAX> &st, TS *const *planes,
                                             long long line0, int s_lo, int sw)
 {
+    static_assert(NP <= 32, "one staged plane per lane");
     const int q = st.issued % NSTAGE;
-    if ((threadIdx.x & 31) == 0) {
+    const int lane = threadIdx.x & 31;
+    const int lo = max(s_lo, 0), hi = min(s_lo + Batch<TS>::kLag, sw);
+    const unsigned bytes = hi > lo ? (unsigned)(hi - lo) * kLine * (unsigned)sizeof(TS) : 0u;
+    if (lane == 0) {
         fence_async_shared();   // earlier reads of this block precede the copies into it
-        const int lo = max(s_lo, 0), hi = min(s_lo + Batch<TS>::kLag, sw);
-        const unsigned bytes = hi > lo ? (unsigned)(hi - lo) * kLine * (unsigned)sizeof(TS) : 0u;
         mbar_arrive_tx(&st.bar[q], bytes * NP);
-        if (bytes) {
-            TS *dst = st.mem + st.block(q) + (lo - s_lo) * kLine;
-#pragma unroll
-            for (int p = 0; p < NP; p++)
-                bulk_g2s(dst + p * Batch<TS>::kBlock, planes[p] + (line0 + lo) * kLine, bytes, &st.bar[q]);
-        }
+    }
+    __syncwarp();
+    // one plane per lane: the copies go out in one warp instruction instead of
+    // NP single-lane ones on the wavefront warp's path
+    if (bytes && lane < NP) {
+        fence_async_shared();
+        TS *dst = st.mem + st.block(q) + (lo - s_lo) * kLine + lane * Batch<TS>::kBlock;
+        bulk_g2s(dst, planes[lane] + (line0 + lo) * kLine, bytes, &st.bar[q]);
     }
     st.issued++;
 }
