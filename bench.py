@@ -534,8 +534,8 @@ def run_extras(args, local):
     ttr = {"case": "C01 Euler 80x40, tolt 1e-10, SCARBOROUGH", "metric": "seconds to the stopping iteration"}
     fin = json.load(open(os.path.join(ROOT, "tests", "golden", "bench_workloads.json")))["c01_euler_80x40_converged"][
         "final"]
-    for solver, key in ((0, "gpu_fp64"), (2, "gpu_fp32_sweeps")):
-        g = Simplec(euler_cosine_case(80, 40, solver=solver), device=local)
+    for solver, key, lag in ((0, "gpu_fp64", 0), (2, "gpu_fp32_sweeps", 0), (2, "gpu_fp32_lagged_factors", 32)):
+        g = Simplec(euler_cosine_case(80, 40, solver=solver, msi_lag=lag), device=local)
         g.set_graph(True)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -544,6 +544,7 @@ def run_extras(args, local):
         fmi, fme, Fd, Cd, pw = g.integrals()
         pr = np.asarray(fin["pwall"])
         ttr[key] = {"seconds": time.perf_counter() - t0, "iterations": rep.it, "normpl": rep.normpl, "Cd": Cd,
+                    "msi_lag": lag,
                     "rel_err_vs_oracle": {"Cd": abs(Cd - fin["Cd"]) / abs(fin["Cd"]),
                                           "fmi": abs(fmi - fin["fmi"]) / abs(fin["fmi"]),
                                           "fme": abs(fme - fin["fme"]) / abs(fin["fme"]),
