@@ -59,12 +59,15 @@ constexpr int kThreads = 256;     // threads per CTA (wavefront warps + helpers)
 constexpr int kMaxCluster = 16;
 constexpr int kSkewPad = 62;      // slots per warp = nx + 62 (slot s = i + 2 lane)
 constexpr int kLine = 32;         // values per slot line, one per lane
-// Steps per batch = the per-warp time lag.  FP64: 16.  FP32: 32, whose
-// shorter steps made the per-batch hand-off and staging show (measured at
-// 514x258: forward sweeps 11-12 % and backward sweeps 22-24 % faster with
-// 32-step batches; the FP64 factorisation runs slower with them).
-template <typename TS> struct Batch {
-    static constexpr int kLag = std::is_same<TS, float>::value ? 32 : 16;
+// Steps per batch = the per-warp time lag (LAG).  FP64: 16.  FP32: 32 on
+// grids of kLongLagCells and more, whose short steps and long sweeps made
+// the per-batch hand-off and staging show (measured at 514x258: forward
+// sweeps 11-12 % and backward sweeps 22-24 % faster with 32-step batches);
+// 16 below, where the longer pipeline fill of 32-step batches costs more
+// (a sweep of 256 nozzles of 64..512 x 32..128 cells: 7 % slower with 32);
+// the FP64 factorisation runs slower with 32-step batches.
+template <int LAG> struct Batch {
+    static constexpr int kLag = LAG;
     static constexpr int kBlock = kLag * kLine;   // elements of one plane for one batch
     static constexpr int kSlots = kRing / kLag;   // ring slots, one batch each
 };
@@ -277,25 +280,25 @@ __device__ __forceinline__ void fence_async_shared() { asm volatile("fence.proxy
 // Per wavefront warp: NSTAGE staging blocks of NP planes x kLag lines, one
 // mbarrier each.  issued/consumed count staged batches over all phases, so
 // block = count % NSTAGE and the mbarrier parity = (count / NSTAGE) & 1.
-template <typename TS, int NSTAGE, int PMAX>
+template <typename TS, int NSTAGE, int PMAX, int LAG>
 struct Stager {
     TS *mem;                     // the CTA's staging memory
     int base;                    // this warp's area in it (elements)
     unsigned long long *bar;
     int issued, consumed;
-    __device__ int block(int q) const { return base + q * PMAX * Batch<TS>::kBlock; }
+    __device__ int block(int q) const { return base + q * PMAX * Batch<LAG>::kBlock; }
 };
 
 // stage slot lines [s_lo, s_lo + kLag) of NP wavefront-major planes (lines
 // outside [0, sw) are not copied: every cell on them is invalid)
-template <int NP, typename TS, int NSTAGE, int PMAX>
-__device__ __forceinline__ void stage_issue(Stager<TS, NSTAGE, PMAX> &st, TS *const *planes,
+template <int NP, typename TS, int NSTAGE, int PMAX, int LAG>
+__device__ __forceinline__ void stage_issue(Stager<TS, NSTAGE, PMAX, LAG> &st, TS *const *planes,
                                             long long line0, int s_lo, int sw)
 {
     static_assert(NP <= 32, "one staged plane per lane");
     const int q = st.issued % NSTAGE;
     const int lane = threadIdx.x & 31;
-    const int lo = max(s_lo, 0), hi = min(s_lo + Batch<TS>::kLag, sw);
+    const int lo = max(s_lo, 0), hi = min(s_lo + Batch<LAG>::kLag, sw);
     const unsigned bytes = hi > lo ? (unsigned)(hi - lo) * kLine * (unsigned)sizeof(TS) : 0u;
     if (lane == 0) {
         fence_async_shared();   // earlier reads of this block precede the copies into it
@@ -306,14 +309,14 @@ __device__ __forceinline__ void stage_issue(Stager<TS, NSTAGE, PMAX> &st, TS *co
     // NP single-lane ones on the wavefront warp's path
     if (bytes && lane < NP) {
         fence_async_shared();
-        TS *dst = st.mem + st.block(q) + (lo - s_lo) * kLine + lane * Batch<TS>::kBlock;
+        TS *dst = st.mem + st.block(q) + (lo - s_lo) * kLine + lane * Batch<LAG>::kBlock;
         bulk_g2s(dst, planes[lane] + (line0 + lo) * kLine, bytes, &st.bar[q]);
     }
     st.issued++;
 }
 // waits for the next staged batch; returns its block's offset in st.mem
-template <typename TS, int NSTAGE, int PMAX>
-__device__ __forceinline__ int stage_wait(Stager<TS, NSTAGE, PMAX> &st, bool &timed_out)
+template <typename TS, int NSTAGE, int PMAX, int LAG>
+__device__ __forceinline__ int stage_wait(Stager<TS, NSTAGE, PMAX, LAG> &st, bool &timed_out)
 {
     const int q = st.consumed % NSTAGE;
     const unsigned parity = (unsigned)(st.consumed / NSTAGE) & 1u;
@@ -331,35 +334,35 @@ __device__ __forceinline__ int stage_wait(Stager<TS, NSTAGE, PMAX> &st, bool &ti
 // slot.  The consumer frees the slot by arriving on the producer's "empty"
 // barrier.  Batch numbers n count over all phases of a channel, so the k-th
 // use of a slot is phase k of its barriers.
-template <typename TS>
+template <int LAG>
 __device__ __forceinline__ void chan_recv(unsigned long long *full, int n, unsigned bytes, bool &timed_out)
 {
-    constexpr int kSlots = Batch<TS>::kSlots;
+    constexpr int kSlots = Batch<LAG>::kSlots;
     unsigned long long *bar = &full[n & (kSlots - 1)];
     if ((threadIdx.x & 31) == 0) mbar_arrive_tx(bar, bytes);
     __syncwarp();
     mbar_wait(bar, (unsigned)(n / kSlots) & 1u, timed_out);
 }
 // producer, before staging batch n: the consumer has released batch n - kSlots
-template <typename TS>
+template <int LAG>
 __device__ __forceinline__ void chan_slot_free(unsigned long long *empty, int n, bool &timed_out)
 {
-    constexpr int kSlots = Batch<TS>::kSlots;
+    constexpr int kSlots = Batch<LAG>::kSlots;
     if (n >= kSlots) mbar_wait(&empty[n & (kSlots - 1)], (unsigned)(n / kSlots - 1) & 1u, timed_out);
 }
 // producer lane that staged the values: ship batch n (vals elements)
-template <typename TS>
+template <typename TS, int LAG>
 __device__ __forceinline__ void chan_send(unsigned ring_dst, unsigned full_dst, const TS *out, int n, int vals)
 {
-    const int slot = n & (Batch<TS>::kSlots - 1);
+    const int slot = n & (Batch<LAG>::kSlots - 1);
     fence_async_shared();   // the staged values become visible to the bulk copy
     bulk_s2s(ring_dst + (unsigned)(slot * vals) * (unsigned)sizeof(TS), out + slot * vals,
              (unsigned)vals * (unsigned)sizeof(TS), full_dst + (unsigned)slot * 8u);
 }
-template <typename TS>
+template <int LAG>
 __device__ __forceinline__ void chan_release(unsigned empty_dst, int n)
 {
-    mbar_remote_arrive(empty_dst + (unsigned)(n & (Batch<TS>::kSlots - 1)) * 8u);
+    mbar_remote_arrive(empty_dst + (unsigned)(n & (Batch<LAG>::kSlots - 1)) * 8u);
 }
 
 // wavefront-major slot of cell (i, j): warp j/32, step offset i + 2 (j%32), lane j%32
@@ -712,6 +715,7 @@ __device__ __forceinline__ bool lag_reuse(const MsiLaunch &L, const MsiSys &S)
 
 constexpr int kExtBlocks = 296;
 constexpr long long kExtMinCells = 1LL << 16;
+constexpr long long kLongLagCells = 1LL << 16;   // FP32 grids from here on use 32-step batches
 constexpr int kExtTimedOut = 1, kExtLagged = 2, kExtBadPivot = 4;   // status bits of the first launch
 
 struct ExtWords {
@@ -930,7 +934,7 @@ __global__ void __launch_bounds__(256) k_ext_resid(MsiLaunch L)
 // factors and both sweeps in FP32 inside the FP64 iteration (residual, x,
 // norm and stopping test stay FP64): iterative refinement preconditioned by
 // the FP32 factorisation.
-template <int ND, int WPC, int NSTAGE, typename TS>
+template <int ND, int WPC, int NSTAGE, typename TS, int LAG>
 __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
 {
     constexpr bool EXACT = std::is_same<TS, double>::value;
@@ -939,7 +943,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
     constexpr int PMAX = (ND > NL + 2) ? ND : NL + 2;   // planes staged per batch
     constexpr int DIAG = (ND == 9) ? 4 : 2;      // index of the main diagonal in a row of A
     constexpr unsigned ES = sizeof(TS);
-    constexpr int kLag = Batch<TS>::kLag, kBlock = Batch<TS>::kBlock, kSlots = Batch<TS>::kSlots;
+    constexpr int kLag = LAG, kBlock = Batch<LAG>::kBlock, kSlots = Batch<LAG>::kSlots;
     // per wavefront warp of this CTA.  Consumer side: rings of values from the
     // neighbour warps and their "full" barriers; producer side: staging of the
     // values for the neighbours and the "empty" barriers the neighbours release.
@@ -1017,7 +1021,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
     const unsigned sbase = smem_u32(stage_mem);
     const unsigned rup = smem_u32(&ring_up[fw][0]), rdn = smem_u32(&ring_dn[fw][0]);
     const unsigned oup1 = smem_u32(&out_up[fw][0]), odn1 = smem_u32(&out_dn[fw][0]);   // sweeps: one value per slot
-    Stager<TS, NSTAGE, PMAX> st;
+    Stager<TS, NSTAGE, PMAX, LAG> st;
     st.mem = stage_mem;
     st.base = fw * NSTAGE * PMAX * kBlock;
     st.bar = &stage_bar[fw][0];
@@ -1071,8 +1075,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
             const int tb = b * kLag;
             const int n = up_base + b;                          // global batch number on the channel
             const bool send = has_above && b <= nbatch - 2;   // the last batch is never read
-            if (has_below && b >= 1) chan_recv<TS>(&full_up[fw][0], n - 1, kLag * NU * ES, timed_out);
-            if (send) chan_slot_free<TS>(&empty_up[fw][0], n, timed_out);
+            if (has_below && b >= 1) chan_recv<LAG>(&full_up[fw][0], n - 1, kLag * NU * ES, timed_out);
+            if (send) chan_slot_free<LAG>(&empty_up[fw][0], n, timed_out);
             const int bo = stage_wait(st, timed_out) + lane;
             if (b + NSTAGE - 1 < nbatch) stage_issue<ND>(st, ap, line0, (b + NSTAGE - 1) * kLag - soff, SW);
             const unsigned rbase = (unsigned)up_base * kLag;
@@ -1152,10 +1156,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                 for (int q = 0; q < NU; q++) mw[q] = u[q];
             }
             store_prev();
-            if (lane == 31 && send) chan_send(up_ring_dst, up_full_dst, &out_up[fw][0], n, kLag * NU);
-            if (lane == 0 && has_below && b >= 2) chan_release<TS>(up_empty_dst, n - 2);
+            if (lane == 31 && send) chan_send<TS, LAG>(up_ring_dst, up_full_dst, &out_up[fw][0], n, kLag * NU);
+            if (lane == 0 && has_below && b >= 2) chan_release<LAG>(up_empty_dst, n - 2);
         }
-        if (lane == 0 && has_below && nbatch >= 2) chan_release<TS>(up_empty_dst, up_base + nbatch - 2);
+        if (lane == 0 && has_below && nbatch >= 2) chan_release<LAG>(up_empty_dst, up_base + nbatch - 2);
         if (piv) bad_pivot = true;
         fence_async_global();   // the sweeps read the factors with bulk copies
     };
@@ -1224,8 +1228,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                 const int tb = b * kLag;
                 const int n = up_base + b;
                 const bool send = has_above && b <= nbatch - 2;
-                if (has_below && b >= 1) chan_recv<TS>(&full_up[fw][0], n - 1, kLag * ES, timed_out);
-                if (send) chan_slot_free<TS>(&empty_up[fw][0], n, timed_out);
+                if (has_below && b >= 1) chan_recv<LAG>(&full_up[fw][0], n - 1, kLag * ES, timed_out);
+                if (send) chan_slot_free<LAG>(&empty_up[fw][0], n, timed_out);
                 const int bo = stage_wait(st, timed_out) + lane;
                 if (b + NSTAGE - 1 < nbatch) stage_issue<NL + 2>(st, fp, line0, (b + NSTAGE - 1) * kLag - soff, SW);
                 const TS m0 = mine, b1 = a1, b2 = a2, b3 = a3;   // state at batch start
@@ -1302,10 +1306,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                         stg_if(wp + wbase + (long long)sl * kLine, pw, has_rows && sl >= 0 && sl < SW);
                     }
                 }
-                if (lane == 31 && send) chan_send(up_ring_dst, up_full_dst, &out_up[fw][0], n, kLag);
-                if (lane == 0 && has_below && b >= 2) chan_release<TS>(up_empty_dst, n - 2);
+                if (lane == 31 && send) chan_send<TS, LAG>(up_ring_dst, up_full_dst, &out_up[fw][0], n, kLag);
+                if (lane == 0 && has_below && b >= 2) chan_release<LAG>(up_empty_dst, n - 2);
             }
-            if (lane == 0 && has_below && nbatch >= 2) chan_release<TS>(up_empty_dst, up_base + nbatch - 2);
+            if (lane == 0 && has_below && nbatch >= 2) chan_release<LAG>(up_empty_dst, up_base + nbatch - 2);
             fence_async_global();   // the backward sweep reads w with bulk copies
             __syncwarp();
         }
@@ -1327,8 +1331,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                 const int tb = b * kLag;
                 const int n = dn_base + b;
                 const bool send = has_below && b <= nbatch - 2;
-                if (has_above && b >= 1) chan_recv<TS>(&full_dn[fw][0], n - 1, kLag * ES, timed_out);
-                if (send) chan_slot_free<TS>(&empty_dn[fw][0], n, timed_out);
+                if (has_above && b >= 1) chan_recv<LAG>(&full_dn[fw][0], n - 1, kLag * ES, timed_out);
+                if (send) chan_slot_free<LAG>(&empty_dn[fw][0], n, timed_out);
                 const int bo = stage_wait(st, timed_out) + lane;
                 if (b + NSTAGE - 1 < nbatch)
                     stage_issue<NU + 1>(st, bp, line0, Tmax - ((b + NSTAGE - 1) * kLag + kLag - 1) - soff, SW);
@@ -1385,10 +1389,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_msi_c(MsiLaunch L)
                     const int sl = Tmax - (tb + kLag - 1) - soff;
                     stg_if(wp + wbase + (long long)sl * kLine, pz, has_rows && sl >= 0 && sl < SW);
                 }
-                if (lane == 0 && send) chan_send(dn_ring_dst, dn_full_dst, &out_dn[fw][0], n, kLag);
-                if (lane == 31 && has_above && b >= 2) chan_release<TS>(dn_empty_dst, n - 2);
+                if (lane == 0 && send) chan_send<TS, LAG>(dn_ring_dst, dn_full_dst, &out_dn[fw][0], n, kLag);
+                if (lane == 31 && has_above && b >= 2) chan_release<LAG>(dn_empty_dst, n - 2);
             }
-            if (lane == 31 && has_above && nbatch >= 2) chan_release<TS>(dn_empty_dst, dn_base + nbatch - 2);
+            if (lane == 31 && has_above && nbatch >= 2) chan_release<LAG>(dn_empty_dst, dn_base + nbatch - 2);
         }
         dn_base += nbatch - 1;
         if (nit == 1) stamp(L, rank, 4);
@@ -1465,25 +1469,25 @@ long long msi_lu_redo_count()
     return (long long)v;
 }
 
-template <int ND, int WPC, int NSTAGE, typename TS>
+template <int ND, int WPC, int NSTAGE, typename TS, int LAG>
 static size_t stage_bytes()
 {
     constexpr int NL = (ND == 9) ? 5 : 4;
     constexpr int PMAX = (ND > NL + 2) ? ND : NL + 2;
-    return (size_t)WPC * NSTAGE * PMAX * Batch<TS>::kBlock * sizeof(TS);
+    return (size_t)WPC * NSTAGE * PMAX * Batch<LAG>::kBlock * sizeof(TS);
 }
 
 // launches one cluster per system if the cluster shape can be scheduled;
 // *fits = false (and nothing launched) otherwise
-template <int ND, int WPC, int NSTAGE, typename TS>
+template <int ND, int WPC, int NSTAGE, typename TS, int LAG>
 static cudaError_t launch_cluster(const MsiLaunch &L, int nsys, cudaStream_t st, bool *fits)
 {
     *fits = false;
     const int nwarps = (L.ny + 31) / 32;
     const int C = (nwarps + WPC - 1) / WPC;
     if (C > kMaxCluster) return cudaSuccess;
-    auto kern = k_msi_c<ND, WPC, NSTAGE, TS>;
-    const size_t smem = stage_bytes<ND, WPC, NSTAGE, TS>();
+    auto kern = k_msi_c<ND, WPC, NSTAGE, TS, LAG>;
+    const size_t smem = stage_bytes<ND, WPC, NSTAGE, TS, LAG>();
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -1556,6 +1560,19 @@ static cudaError_t launch_cluster(const MsiLaunch &L, int nsys, cudaStream_t st,
     return cudaGetLastError();
 }
 
+// fewest wavefront warps per CTA (one SM per warp) whose cluster fits,
+// unless the caller asked for one schedule
+template <int ND, typename TS, int LAG>
+static cudaError_t launch_schedules(const MsiLaunch &L, int nsys, cudaStream_t st, bool *done)
+{
+    cudaError_t e = cudaSuccess;
+    if (L.variant != 2) {
+        e = launch_cluster<ND, 1, 4, TS, LAG>(L, nsys, st, done);
+        if (e != cudaSuccess || *done || L.variant == 1) return e;
+    }
+    return launch_cluster<ND, 2, 2, TS, LAG>(L, nsys, st, done);
+}
+
 template <int ND, typename TS>
 static cudaError_t launch_nd(const MsiLaunch &L, int nsys, cudaStream_t st, bool *done)
 {
@@ -1568,14 +1585,10 @@ static cudaError_t launch_nd(const MsiLaunch &L, int nsys, cudaStream_t st, bool
     const bool room = L.ws_cap == 0 || L.ws_cap >= msi_cluster_work_doubles(ND, L.nx, L.ny);
     const bool small = (long long)L.nx * L.ny < (1LL << 31);   // 32-bit cell indices in the passes
     if (!(aligned && room && small)) return cudaSuccess;
-    // fewest wavefront warps per CTA (one SM per warp) whose cluster fits,
-    // unless the caller asked for one schedule
-    cudaError_t e = cudaSuccess;
-    if (L.variant != 2) {
-        e = launch_cluster<ND, 1, 4, TS>(L, nsys, st, done);
-        if (e != cudaSuccess || *done || L.variant == 1) return e;
+    if constexpr (std::is_same<TS, float>::value) {
+        if ((long long)L.nx * L.ny >= kLongLagCells) return launch_schedules<ND, TS, 32>(L, nsys, st, done);
     }
-    return launch_cluster<ND, 2, 2, TS>(L, nsys, st, done);
+    return launch_schedules<ND, TS, 16>(L, nsys, st, done);
 }
 
 // m2d_test_wait_hook's setting for the cluster kernel (0: off)
