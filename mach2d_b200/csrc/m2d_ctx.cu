@@ -42,7 +42,7 @@ struct m2d_ctx {
     Fields f;
     Params q;
     double *arena = nullptr;
-    double *ws9[2], *ws5, *P, *Q, *part;
+    double *ws9[3], *ws5, *P, *Q, *part;   // ws9: u, v and (energy equation) T
     double *dsc = nullptr;
     int *dint = nullptr;
     int *dlag = nullptr;           // MSI factor records (MsiSys::lag), two ints per workspace
@@ -228,7 +228,11 @@ extern "C" int m2d_create(const m2d_case *c, int device, m2d_ctx **out)
     const size_t nplanes = 0 M2D_PLANES(M2D_COUNT);
 #undef M2D_COUNT
     const size_t strips = (size_t)9 * h.ny + 2 * (size_t)h.nx + 64;
-    const size_t solver = 2 * msi_work_doubles(9, h.nx, h.ny) + msi_work_doubles(5, h.nx, h.ny) + 4 + 2 * N + 3 * 32;
+    // a third 9-diagonal workspace when the energy equation is solved, so
+    // that T keeps its own factors (lagged factorisation)
+    const int n9 = (c->modvis == 0 && c->ktm == 0) ? 2 : 3;
+    const size_t solver = (size_t)n9 * msi_work_doubles(9, h.nx, h.ny) + msi_work_doubles(5, h.nx, h.ny) + 4 +
+                          2 * N + 4 * 32;
     const size_t mixd = (sizeof(m2d_mixture) + sizeof(double) - 1) / sizeof(double);
     const size_t total = nplanes * N + 32 * N + strips + solver + (size_t)kMaxMultiReduce * red_parts() + 72 +
                          S_COUNT + mixd;
@@ -249,13 +253,14 @@ extern "C" int m2d_create(const m2d_case *c, int device, m2d_ctx **out)
     f.Tbn = take(h.nx); f.Tbs = take(h.nx);
     // MSI scratch starts on 256-byte boundaries (one line per warp step)
     auto take_aligned = [&](size_t n) { cur = x->arena + (((size_t)(cur - x->arena) + 31) / 32) * 32; return take(n); };
-    for (int k = 0; k < 2; k++) x->ws9[k] = take_aligned(msi_work_doubles(9, h.nx, h.ny));
+    x->ws9[2] = nullptr;
+    for (int k = 0; k < n9; k++) x->ws9[k] = take_aligned(msi_work_doubles(9, h.nx, h.ny));
     x->ws5 = take_aligned(msi_work_doubles(5, h.nx, h.ny) + 4);   // + the rr words of m2d_msi_workspace_doubles
     x->P = take(N); x->Q = take(N);
     x->part = take((size_t)kMaxMultiReduce * red_parts() + 8);
     x->dsc = take(S_COUNT);
     x->dint = (int *)take(I_COUNT);
-    x->dlag = (int *)take(4);   // factor records of ws9[0], ws9[1], ws5 (zeroed: no factors yet)
+    x->dlag = (int *)take(4);   // factor records of ws9[0], ws9[1], ws5, ws9[2] (zeroed: no factors yet)
     x->dmix = (m2d_mixture *)take(mixd);
     if ((size_t)(cur - x->arena) > total) { m2d_destroy(x); return ctx_fail(M2D_ERR_NOMEM, "m2d_create: arena overflow"); }
     e = cudaMallocHost(&x->hsc, S_COUNT * sizeof(double));
@@ -319,9 +324,10 @@ static int solve9(m2d_ctx *x, cudaStream_t s, int nsys, double *const *a, double
         L.lag_max = L.prec == 1 ? c.msi_lag : 0;
         for (int k = 0; k < nsys; k++) {
             L.s[k].a = a[k]; L.s[k].b = b[k]; L.s[k].x = v[k];
-            L.s[k].ws = x->ws9[k];
+            const bool t_eq = islot[k] == I_NIT_T && x->ws9[2];
+            L.s[k].ws = t_eq ? x->ws9[2] : x->ws9[k];
             L.s[k].nit = x->dint + islot[k]; L.s[k].rr = x->dsc + rslot[k];
-            L.s[k].lag = x->dlag + 2 * k;
+            L.s[k].lag = x->dlag + (t_eq ? 6 : 2 * k);
             L.s[k].tag = 1 + islot[k];   // the equation (u, v or T) owns the factors
         }
         KL(launch_msi(9, L, nsys, s), msi_last_launch_count());
