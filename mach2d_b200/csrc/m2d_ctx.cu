@@ -59,6 +59,9 @@ struct m2d_ctx {
     long long launches_fixed = 0, launches_body = 0;
     double *hsc = nullptr;   // pinned mirror of dsc
     int *hint = nullptr;     // pinned mirror of dint
+    double *hsc_b = nullptr; // second mirrors and their events: m2d_run keeps two
+    int *hint_b = nullptr;   // captured iterations in flight
+    cudaEvent_t ev[2] = {nullptr, nullptr};
     double dt = 0, norm = 0, normpl = 0, rmass = 0, p_avg = 0;
     double Href = 0, Cpref = 0, fm1D = 0, Fd1D = 0, Fpv1D = 0, Sg = 0;
     int it = 0, it_stop = -1, itp_used = 0;
@@ -288,6 +291,10 @@ extern "C" int m2d_destroy(m2d_ctx *x)
     if (x->arena) cudaFree(x->arena);
     if (x->hsc) cudaFreeHost(x->hsc);
     if (x->hint) cudaFreeHost(x->hint);
+    if (x->hsc_b) cudaFreeHost(x->hsc_b);
+    if (x->hint_b) cudaFreeHost(x->hint_b);
+    for (cudaEvent_t e : x->ev)
+        if (e) cudaEventDestroy(e);
     if (x->st) cudaStreamDestroy(x->st);
     delete x;
     return M2D_OK;
@@ -795,9 +802,74 @@ extern "C" int m2d_iterate(m2d_ctx *x, m2d_report *rep)
     return finish_iteration(x, it, itp_used, rep);
 }
 
+// m2d_run with captured iterations: two iterations in flight, so that the GPU
+// does not wait for the host's turn between them.  Iteration k+1 is queued
+// before iteration k's scalars are read; the stop rule's iteration (it_stop
+// = 2 it of the first iteration below tolt) is always known an iteration
+// ahead, so no iteration past the stop or past itmax starts, and every
+// report is the one m2d_iterate gives.  When an iteration fails, the one
+// queued behind it still runs before the error returns (the context then
+// counts both).
+static int run_pipelined(m2d_ctx *x, int itmax, m2d_report *last)
+{
+    TRY(cudaSetDevice(x->device));
+    if (!x->hsc_b) TRY(cudaMallocHost(&x->hsc_b, S_COUNT * sizeof(double)));
+    if (!x->hint_b) TRY(cudaMallocHost(&x->hint_b, I_COUNT * sizeof(int)));
+    for (cudaEvent_t &e : x->ev)
+        if (!e) TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    if (!x->exec) {
+        const int rc = build_graph(x);
+        if (rc) return rc;
+    }
+    double *hs[2] = {x->hsc, x->hsc_b};
+    int *hi[2] = {x->hint, x->hint_b};
+    cudaStream_t st = x->st;
+    auto queue = [&](int slot) -> cudaError_t {
+        cudaError_t e = cudaGraphLaunch(x->exec, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(hs[slot], x->dsc, S_COUNT * sizeof(double), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(hi[slot], x->dint, I_COUNT * sizeof(int), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaEventRecord(x->ev[slot], st);
+        return e;
+    };
+    const int it0 = x->it;
+    TRY(queue(0));
+    for (int k = 1; k <= itmax; k++) {
+        const int slot = (k - 1) & 1, itk = it0 + k;
+        const bool more = k < itmax && !(x->it_stop >= 0 && itk >= x->it_stop);
+        if (more) {
+            const cudaError_t e = queue(slot ^ 1);
+            if (e != cudaSuccess) {
+                cudaStreamSynchronize(st);
+                x->it = itk;
+                m2d_set_last_error(e, "m2d_run: queue an iteration", __FILE__, __LINE__);
+                return M2D_ERR_CUDA;
+            }
+        }
+        TRY(cudaEventSynchronize(x->ev[slot]));
+        x->hsc = hs[slot]; x->hint = hi[slot];
+        x->hsc_b = hs[slot ^ 1]; x->hint_b = hi[slot ^ 1];
+        x->it = itk;
+        const int itp_used = x->hint[I_ITP];
+        x->launches += x->launches_fixed + x->launches_body * x->hint[I_ITP_TOTAL];
+        x->p_avg = x->hsc[S_PAVG];
+        x->normpl = x->hsc[S_NORMPL];
+        x->norm = x->hsc[S_NORM];
+        x->dt = x->hsc[S_DT];
+        const int rc = finish_iteration(x, itk, itp_used, last);
+        if (rc) {
+            cudaStreamSynchronize(st);
+            if (more) x->it = itk + 1;   // the device ran the queued iteration too
+            return rc;
+        }
+        if (!more || x->it_stop == itk) break;
+    }
+    return M2D_OK;
+}
+
 extern "C" int m2d_run(m2d_ctx *x, int itmax, m2d_report *last)
 {
     if (!x) return ctx_fail(M2D_ERR_ARG, "m2d_run: null context");
+    if (x->graph_on) return itmax > 0 ? run_pipelined(x, itmax, last) : M2D_OK;
     for (int k = 0; k < itmax; k++) {
         int rc = m2d_iterate(x, last);
         if (rc) return rc;

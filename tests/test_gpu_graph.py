@@ -64,3 +64,41 @@ def test_graph_run_stops_where_the_default_run_stops():
     assert ra.it == rb.it and ra.normpl == rb.normpl
     assert a.integrals()[3] == b.integrals()[3]
     a.close(), b.close()
+
+
+def test_run_with_two_iterations_in_flight_equals_single_iterations():
+    """m2d_run in graph mode queues each captured iteration before the
+    previous one's scalars come back; its reports, fields and stopping
+    iteration are those of one m2d_iterate at a time."""
+    a = Simplec(euler_cosine_case(30, 14))
+    b = Simplec(euler_cosine_case(30, 14))
+    a.set_graph(True)
+    b.set_graph(True)
+    for _ in range(3):              # the two modes mix
+        a.iterate(), b.iterate()
+    ra = [a.iterate() for _ in range(37)]
+    rb = b.run(37)
+    assert rb.it == ra[-1].it == 40
+    for c in ("dt", "norm", "normpl", "rmass", "fmi", "fme", "Fd", "itp_used"):
+        assert getattr(rb, c) == getattr(ra[-1], c), c
+    for f in ("u", "v", "p", "T", "ro"):
+        assert np.array_equal(a.field(f), b.field(f)), f
+    assert b.iterate().normpl == a.iterate().normpl
+    assert a.scalar("launches") == b.scalar("launches")
+    a.close(), b.close()
+
+
+def test_run_stops_at_the_reference_stopping_iteration_in_graph_mode():
+    c = euler_cosine_case(20, 10, tolt=1e-6)
+    a, b = Simplec(c), Simplec(c)
+    a.set_graph(True)
+    b.set_graph(True)
+    for _ in range(100000):
+        r = a.iterate()
+        if a.scalar("it_stop") == r.it:
+            break
+    assert a.scalar("it_stop") == r.it
+    rb = b.run(100000)
+    assert rb.it == r.it and rb.normpl == r.normpl
+    assert np.array_equal(a.field("p"), b.field("p"))
+    a.close(), b.close()
