@@ -354,8 +354,9 @@ static int solve5(m2d_ctx *x, cudaStream_t s)
         // stopping test is the whole solve
         if (!x->net) return ctx_fail(M2D_ERR_ARG, "m2d_iterate: solvers 3 and 4 need a network (m2d_ctx_set_unet)");
         m2d_learned_report r;
-        const int rc = m2d_pprime_solve_learned(x->net, x->nx, x->ny, c.nitm_p, c.tol_p, x->f.ap, x->f.bp, x->f.pl,
-                                                x->f.Jp, x->ws5, c.solver == 4 ? 3 : 1, s, &r);
+        const int rc = pprime_solve_learned_lagged(x->net, x->nx, x->ny, c.nitm_p, c.tol_p, x->f.ap, x->f.bp,
+                                                   x->f.pl, x->f.Jp, x->ws5, c.solver == 4 ? 3 : 1, s, &r,
+                                                   x->dlag + 4, 1 + I_NIT_P, c.msi_lag);
         if (rc) return rc;
         x->learned_calls++;
         x->learned_accepted += r.accepted;

@@ -78,6 +78,16 @@ struct MsiLaunch {
                                // schedule gives the same iterates.
 };
 
+}  // namespace m2d
+struct m2d_unet;
+struct m2d_learned_report;
+namespace m2d {
+// the learned p' solve (m2d_pprime_solve_learned) whose MSI iteration may
+// reuse lagged FP32 factors (m2d_unet.cu)
+int pprime_solve_learned_lagged(::m2d_unet *n, int nx, int ny, int nitm, double tol, const double *d_a,
+                                const double *d_b, double *d_x, const double *d_Jp, double *d_work, int prec,
+                                void *stream, ::m2d_learned_report *rep, int *lag_rec, int lag_tag, int lag_max);
+
 // kernels the last launch_msi on this host thread issued (transposes and
 // whole-GPU passes included)
 int msi_last_launch_count();

@@ -21,6 +21,7 @@
 #include <cstring>
 #include <vector>
 #include "m2d_common.cuh"
+#include "m2d_solvers.cuh"
 #include "../../include/mach2d_b200.h"
 
 using bf16 = __nv_bfloat16;
@@ -1438,9 +1439,13 @@ cudaError_t unet_correct(m2d_unet *n, int nx, int ny, const double *d_a, const d
 }
 }  // namespace m2d
 
-extern "C" int m2d_pprime_solve_learned(m2d_unet *n, int nx, int ny, int nitm, double tol, const double *d_a,
-                                        const double *d_b, double *d_x, const double *d_Jp, double *d_work, int prec,
-                                        void *stream, m2d_learned_report *rep)
+// m2d_pprime_solve_learned, and for the context's p' solve with lagged FP32
+// factors (lag_max > 0, prec bit 0): the MSI iteration after the correction
+// reuses the workspace's factors as MsiLaunch::lag_max describes, with the
+// factor record lag_rec and the equation's tag
+int m2d::pprime_solve_learned_lagged(m2d_unet *n, int nx, int ny, int nitm, double tol, const double *d_a,
+                                     const double *d_b, double *d_x, const double *d_Jp, double *d_work, int prec,
+                                     void *stream, m2d_learned_report *rep, int *lag_rec, int lag_tag, int lag_max)
 {
     if (!n || !image_fits(nx, ny, n->H, n->W) || !d_a || !d_b || !d_x || !d_Jp || !d_work || nitm < 1)
         return unet_fail(M2D_ERR_ARG, "m2d_pprime_solve_learned: bad arguments");
@@ -1480,9 +1485,28 @@ extern "C" int m2d_pprime_solve_learned(m2d_unet *n, int nx, int ny, int nitm, d
     // test and the caller allows the correction to stand alone
     const bool skip_msi = alone && accept && r1 < tol * r0;
     if (e == cudaSuccess && !skip_msi) {
-        const int rc = m2d_msi_solve_device_ws(5, nx, ny, nitm, tol_eff, d_a, d_b, d_x, d_work,
-                                               m2d_msi_workspace_doubles(5, nx, ny), stream, n->nit, nullptr, prec);
-        if (rc) return rc;
+        const long wd = m2d_msi_workspace_doubles(5, nx, ny);
+        if (lag_rec && lag_max > 0 && prec == 1) {
+            MsiLaunch L;
+            memset(&L, 0, sizeof L);
+            L.nx = nx; L.ny = ny; L.nitm = nitm; L.tol = tol_eff;
+            L.prec = 1;
+            L.lag_max = lag_max;
+            L.ws_cap = (size_t)(wd - 4);
+            MsiSys &S = L.s[0];
+            S.a = d_a; S.b = d_b; S.x = d_x;
+            S.ws = d_work;
+            S.rr = d_work + (wd - 4);
+            S.nit = n->nit;
+            S.lag = lag_rec;
+            S.tag = lag_tag;
+            e = launch_msi(5, L, 1, st);
+            if (e != cudaSuccess) { m2d_set_last_error(e, "m2d_pprime_solve_learned: MSI", __FILE__, __LINE__); return M2D_ERR_CUDA; }
+        } else {
+            const int rc = m2d_msi_solve_device_ws(5, nx, ny, nitm, tol_eff, d_a, d_b, d_x, d_work, wd, stream,
+                                                   n->nit, nullptr, prec);
+            if (rc) return rc;
+        }
         e = cudaMemcpyAsync(&nit, n->nit, sizeof(int), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     } else if (e == cudaSuccess) {
@@ -1491,6 +1515,14 @@ extern "C" int m2d_pprime_solve_learned(m2d_unet *n, int nx, int ny, int nitm, d
     if (e != cudaSuccess) { m2d_set_last_error(e, "m2d_pprime_solve_learned", __FILE__, __LINE__); return M2D_ERR_CUDA; }
     if (rep) { rep->accepted = accept ? 1 : 0; rep->r0 = r0; rep->r1 = r1; rep->nit = nit; }
     return M2D_OK;
+}
+
+extern "C" int m2d_pprime_solve_learned(m2d_unet *n, int nx, int ny, int nitm, double tol, const double *d_a,
+                                        const double *d_b, double *d_x, const double *d_Jp, double *d_work, int prec,
+                                        void *stream, m2d_learned_report *rep)
+{
+    return m2d::pprime_solve_learned_lagged(n, nx, ny, nitm, tol, d_a, d_b, d_x, d_Jp, d_work, prec, stream, rep,
+                                            nullptr, 0, 0);
 }
 
 // Two-level cycles: the network's correction (kept only if it lowers |r|)

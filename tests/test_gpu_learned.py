@@ -155,3 +155,29 @@ def test_solver4_lets_a_sufficient_correction_stand_alone(trained):
     assert g4.scalar("learned_alone") > 0
     assert g4.scalar("learned_alone") <= g4.scalar("learned_accepted") <= g4.scalar("learned_calls")
     g2.close(), g4.close(), small.close()
+
+
+def test_solver3_with_lagged_factors_stays_on_track(trained):
+    """Solver 3 with msi_lag = 16: the MSI iteration after the network's
+    correction may reuse FP32 factors of an earlier p' matrix (and the u, v
+    solves theirs); every solve still passes the FP64 stopping test, so the
+    run stays on the track of solver 3 with fresh factors, and it is
+    deterministic."""
+    net, _, _, _ = trained
+    small = unet.UNet(1, net.H, net.W, params=net.params())
+    runs = []
+    for lag in (16, 16, 0):
+        g = Simplec(_case(64, solver=3, msi_lag=lag))
+        g.set_unet(small)
+        reps = [g.iterate() for _ in range(40)]
+        runs.append((reps, {f: g.field(f) for f in ("u", "v", "p", "T")}, g.scalar("learned_accepted")))
+        g.close()
+    (ra, fa, acc), (rb, fb, _), (r0, f0, _) = runs
+    assert [r.normpl for r in ra] == [r.normpl for r in rb]
+    assert acc > 0
+    ratios = [x.normpl / y.normpl for x, y in zip(ra, r0)]
+    assert 0.5 < float(np.exp(np.mean(np.log(ratios)))) < 2.0
+    for f in fa:
+        assert np.array_equal(fa[f], fb[f]), f
+        assert np.max(np.abs(fa[f] - f0[f])) <= 1e-2 * np.max(np.abs(f0[f])), f
+    small.close()
